@@ -1,0 +1,310 @@
+"""Benchmark: sampled edges per second (SEPS) on one B200 (or N replicas).
+
+Workload (one step): the mid-size power-law graph -- a seeded synthetic
+directed graph with 875,713 vertices and 5,105,039 edges, out-degree power
+law exponent 2.1 capped at 460, int32 CSR, lognormal(0,1) weights -- run with
+  (a) degree-biased neighbor sampling: 4000 samples, FrontierSize 4,
+      NeighborSize 20, Depth 3;
+  (b) degree-biased random walks: 4000 walks of length 64.
+value = (edges of a + edges of b) / device time of the step.  Inputs are
+resident in HBM; between timed steps a 256 MiB buffer is written to flush L2.
+e2e = the same metric through csaw_sample_host: host seeds in, host edge list
+(src, dst, sample) out, copies inside the timed region.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl csaw|reference]
+
+--impl reference times the CPU oracle (a port of the reference's sampling
+semantics; the reference itself has no CPU implementation and its CUDA
+kernels read out of bounds, so they are not run) on all host threads, on a
+bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "c-saw_b200")]
+
+GRAPH = dict(n_vertices=875_713, n_edges=5_105_039, gamma=2.1, max_degree=460, seed=20, weight="lognormal")
+WORK_A = dict(mode=0, bias=1, n_samples=4000, frontier_size=4, neighbor_size=20, depth=3)
+WORK_B = dict(mode=1, bias=1, n_samples=4000, frontier_size=1, neighbor_size=1, depth=64)
+SEED_A, SEED_B = 0xC5A0, 0xC5A1
+FLUSH_BYTES = 256 << 20
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.idx = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.2)
+        self.proc.terminate()
+        self.proc.wait()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    return int(os.environ.get("RANK", "0")), ws, int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def build_graph():
+    from csaw import graphgen
+    return graphgen.powerlaw_directed(**GRAPH)
+
+
+def workload_desc():
+    return {"workload": "powerlaw_v875713_e5105039: (a) degree-biased neighbor sampling 4000 samples F4 N20 D3 "
+                        "+ (b) degree-biased random walks 4000 x 64",
+            "graph": GRAPH, "a": WORK_A, "b": WORK_B, "l2": "flushed between timed steps (256 MiB write)"}
+
+
+def run_reference(args):
+    """CPU oracle on all host threads, bounded sample of the workload per step."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    g = build_graph()
+    threads = os.cpu_count() or 1
+    na, nb = 1000, 1000   # a quarter of each workload per step
+    seeds_a = oracle.make_seeds(g.rowptr, na * WORK_A["frontier_size"], SEED_A)
+    seeds_b = oracle.make_seeds(g.rowptr, nb, SEED_B)
+
+    def step():
+        ea = oracle.run(g.rowptr, g.col, g.weight, seeds_a, 0, 1, na, 4, 3, [20, 20, 20], seed=SEED_A,
+                        n_threads=threads)
+        eb = oracle.run(g.rowptr, g.col, g.weight, seeds_b, 1, 1, nb, 1, 64, seed=SEED_B, n_threads=threads)
+        return len(ea[0]) + len(eb[0])
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    edges = sum(step() for _ in range(args.steps))
+    dt = time.perf_counter() - t0
+    v = edges / dt
+    desc = workload_desc()
+    desc["sample"] = f"{na} of 4000 samples of (a) and {nb} of 4000 walks of (b) per step"
+    line = {"impl": "reference", "metric": "sampled_edges_per_sec", "value": v, "unit": "edges/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+int32", "data": "synthetic", "config": desc,
+            "cpu_baseline": {"value": v, "unit": "edges/s", "cores": threads, "kind": "port",
+                             "sample": desc["sample"]},
+            "e2e": {"value": v, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def cpu_baseline(g):
+    """Oracle timed on the host cores on a bounded sample (reported baseline only)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    threads = os.cpu_count() or 1
+    na, nb = 1000, 1000
+    sa = oracle.make_seeds(g.rowptr, na * 4, SEED_A)
+    sb = oracle.make_seeds(g.rowptr, nb, SEED_B)
+    edges, t0, reps = 0, time.perf_counter(), 0
+    while True:
+        ea = oracle.run(g.rowptr, g.col, g.weight, sa, 0, 1, na, 4, 3, [20, 20, 20], seed=SEED_A, n_threads=threads)
+        eb = oracle.run(g.rowptr, g.col, g.weight, sb, 1, 1, nb, 1, 64, seed=SEED_B, n_threads=threads)
+        edges += len(ea[0]) + len(eb[0])
+        reps += 1
+        if time.perf_counter() - t0 > 10.0 or reps >= 200:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": edges / dt, "unit": "edges/s", "cores": threads, "kind": "port",
+            "sample": f"{reps} x ({na} of 4000 samples of (a) + {nb} of 4000 walks of (b)), {dt:.1f} s"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="csaw", choices=["csaw", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import csaw
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    g = build_graph()
+    G = csaw.Graph(g)                       # plain residency (gathered degrees)
+    stream = torch.cuda.current_stream()
+    pa = csaw.make_params(**WORK_A, seed=SEED_A + 7919 * rank)
+    pb = csaw.make_params(**WORK_B, seed=SEED_B + 7919 * rank)
+    seeds_a = G.make_seeds(4000 * 4, SEED_A + 7919 * rank)
+    seeds_b = G.make_seeds(4000, SEED_B + 7919 * rank)
+    cap_a, cap_b = csaw.edge_bound(pa), csaw.edge_bound(pb)
+    out_a = torch.empty((3, cap_a), dtype=torch.int32, device="cuda")
+    out_b = torch.empty((3, cap_b), dtype=torch.int32, device="cuda")
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.int32, device="cuda")
+
+    def step():
+        a = G.sample(pa, seeds_a, capacity=cap_a, out=out_a, with_depth=False)
+        b = G.sample(pb, seeds_b, capacity=cap_b, out=out_b, with_depth=False)
+        return a[0].numel() + b[0].numel()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-timed steps (L2 flushed before each)
+    G.profile(True)
+    launches0 = G.stats()["kernel_launches"]
+    clocks = Clocks(local)
+    clocks.start()
+    barrier()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    edges = 0
+    for i in range(args.steps):
+        flush.zero_()
+        evs[i][0].record(stream)
+        edges += step()
+        evs[i][1].record(stream)
+    barrier()
+    clk = clocks.stop()
+    launches = G.stats()["kernel_launches"] - launches0
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    kstats = {k: G.kernel_stats(k) for k in ("expand", "heavy", "walk", "setup")}
+    G.profile(False)
+
+    # ---- end to end through the host-buffer entry point
+    seeds_a_h = seeds_a.cpu().numpy()
+    seeds_b_h = seeds_b.cpu().numpy()
+    host_a = torch.empty((3, cap_a), dtype=torch.int32).pin_memory().numpy()
+    host_b = torch.empty((3, cap_b), dtype=torch.int32).pin_memory().numpy()
+    sa_pin = torch.from_numpy(seeds_a_h).pin_memory().numpy()
+    sb_pin = torch.from_numpy(seeds_b_h).pin_memory().numpy()
+    e2e_steps = max(3, args.steps // 2)
+    G.sample_host(pa, sa_pin, capacity=cap_a, out=host_a, with_depth=False)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    e2e_edges = 0
+    for _ in range(e2e_steps):
+        ra = G.sample_host(pa, sa_pin, capacity=cap_a, out=host_a, with_depth=False, stream=stream.cuda_stream)
+        rb = G.sample_host(pb, sb_pin, capacity=cap_b, out=host_b, with_depth=False, stream=stream.cuda_stream)
+        e2e_edges += ra[0].size + rb[0].size
+    e1.record(stream)
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+
+    # ---- max over ranks
+    t_s = ms / 1e3
+    tot = torch.tensor([float(edges), t_s, float(e2e_edges), e2e_ms / 1e3], dtype=torch.float64, device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+        s = tot.clone()
+        dist.all_reduce(s[0:1])
+        dist.all_reduce(s[2:3])
+        m = tot.clone()
+        dist.all_reduce(m[1:2], op=dist.ReduceOp.MAX)
+        dist.all_reduce(m[3:4], op=dist.ReduceOp.MAX)
+        tot = torch.stack([s[0], m[1], s[2], m[3]])
+    all_edges, t_max, e2e_all, e2e_t = (float(x) for x in tot.cpu())
+    value = all_edges / t_max
+    e2e_value = e2e_all / e2e_t
+
+    peak, peak_kind = load_peaks()
+    ke = kstats["expand"]
+    achieved = ke["bytes"] / (ke["ms"] * 1e-3) / 1e9 if ke["ms"] > 0 else None
+    per_launch_bytes = ke["bytes"] / ke["launches"] if ke["launches"] else None
+    roofline = {"bound": "hbm", "kernel": "k_expand_warp (level expansion)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+                "traffic": None, "algorithmic_bytes_per_launch": per_launch_bytes,
+                "launch_ms": ke["ms"] / ke["launches"] if ke["launches"] else None}
+
+    if rank == 0:
+        line = {"metric": "sampled_edges_per_sec", "value": value, "unit": "edges/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+int32",
+                "data": "synthetic", "config": workload_desc(),
+                "e2e": {"value": e2e_value, "unit": "edges/s",
+                        "h2d_bytes_per_step": 4 * (seeds_a_h.size + seeds_b_h.size),
+                        "d2h_bytes_per_step": int(12 * e2e_edges / e2e_steps)},
+                "gpu_launches": int(launches), "clocks": clk, "roofline": roofline,
+                "kernels": {k: v for k, v in kstats.items() if v["launches"]},
+                "edges_per_step": all_edges / args.steps / world}
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(g)
+        print(json.dumps(line))
+    G.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,90 @@
+"""ctypes binding of libcsaw_b200.so (the C ABI declared in include/csaw.h).
+
+There is no fallback: if the library is missing or fails to load, every call
+raises.  Build it with `make -C c-saw_b200` (or __graft_entry__.build()).
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libcsaw_b200.so")
+
+OK, ERR_INVALID, ERR_CUDA, ERR_CAPACITY, ERR_NOMEM, ERR_DEVICE = range(6)
+MODE_NEIGHBOR, MODE_WALK, MODE_MDRW = 0, 1, 2
+BIAS_UNBIASED, BIAS_DEGREE, BIAS_EDGE_WEIGHT, BIAS_HOOK = 0, 1, 2, 3
+SCHED_PLAIN, SCHED_BATCHED, SCHED_LEARNED = 0, 1, 2
+GRAPH_DEGREE_BIAS, GRAPH_CDF_CACHE = 1, 2
+MAX_DEPTH = 64
+KERNEL_KINDS = {"expand": 0, "heavy": 1, "walk": 2, "mdrw": 3, "setup": 4}
+
+# Every symbol include/csaw.h declares (tests check the library exports them).
+EXPORTS = [
+    "csaw_last_error", "csaw_version", "csaw_graph_create", "csaw_graph_destroy",
+    "csaw_graph_stats", "csaw_graph_profile", "csaw_graph_kernel_stats", "csaw_make_seeds",
+    "csaw_sample", "csaw_sample_host", "csaw_sampler_compat",
+]
+
+
+class CsawError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"csaw error {code}: {msg}")
+        self.code = code
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("mode", ctypes.c_int32),
+        ("bias", ctypes.c_int32),
+        ("schedule", ctypes.c_int32),
+        ("n_samples", ctypes.c_int32),
+        ("frontier_size", ctypes.c_int32),
+        ("neighbor_size", ctypes.c_int32),
+        ("depth", ctypes.c_int32),
+        ("fanout", ctypes.c_int32 * MAX_DEPTH),
+        ("seed", ctypes.c_uint64),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in (
+        "n_vertices", "n_edges", "max_degree", "device_bytes", "workspace_bytes",
+        "kernel_launches", "last_edges", "last_items", "last_bytes")]
+
+
+_L = None
+
+
+def lib():
+    """Load the library (raises if it is not built)."""
+    global _L
+    if _L is not None:
+        return _L
+    if not os.path.exists(LIB_PATH):
+        raise CsawError(ERR_CUDA, f"{LIB_PATH} is not built: run `make -C c-saw_b200`")
+    L = ctypes.CDLL(LIB_PATH)
+    p, i32, i64, u64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_uint64
+    P64 = ctypes.POINTER(ctypes.c_int64)
+    L.csaw_last_error.restype = ctypes.c_char_p
+    L.csaw_version.restype = ctypes.c_char_p
+    L.csaw_graph_create.argtypes = [p, i32, p, p, i64, i64, i32, ctypes.POINTER(p)]
+    L.csaw_graph_destroy.argtypes = [p]
+    L.csaw_graph_stats.argtypes = [p, ctypes.POINTER(Stats)]
+    L.csaw_graph_profile.argtypes = [p, i32]
+    L.csaw_graph_kernel_stats.argtypes = [p, i32, ctypes.POINTER(ctypes.c_double), P64, P64, P64]
+    L.csaw_make_seeds.argtypes = [p, i64, u64, p, p]
+    sig = [p, ctypes.POINTER(Params), p, p, p, p, p, i64, P64, p]
+    L.csaw_sample.argtypes = sig
+    L.csaw_sample_host.argtypes = sig
+    L.csaw_sampler_compat.argtypes = [ctypes.c_char_p, ctypes.c_char_p, i32, i32, i32, i32, i32, i32,
+                                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
+    for name in EXPORTS:
+        if name not in ("csaw_last_error", "csaw_version"):
+            getattr(L, name).restype = ctypes.c_int
+    _L = L
+    return L
+
+
+def check(rc):
+    if rc != OK:
+        raise CsawError(rc, lib().csaw_last_error().decode())
+    return rc

@@ -1,0 +1,158 @@
+"""Deterministic synthetic graph generators (CSR, int32 col, float32 weights).
+
+The reference's example graph (web-Google, SNAP) is not shipped with it, so
+the workloads use seeded synthetic graphs with the stated shapes:
+  - R-MAT (Chakrabarti, Zhan, Faloutsos, SDM 2004) with (a, b, c, d), scale
+    and edge factor, optionally symmetrised, self-loops and duplicate edges
+    removed;
+  - a directed graph with a power-law out-degree sequence (exponent gamma,
+    capped at max_degree, summing exactly to n_edges) whose destinations follow
+    a Zipf popularity, so in-degrees are skewed too.
+Weights: uniform (0, 1], lognormal(0, 1) or Pareto(alpha) (numpy PCG64).
+"""
+import numpy as np
+
+
+class CSR:
+    """Host CSR: rowptr int64[V+1], col int32[E], weight float32[E] or None."""
+
+    def __init__(self, rowptr, col, weight=None, name=""):
+        self.rowptr = np.ascontiguousarray(rowptr, dtype=np.int64)
+        self.col = np.ascontiguousarray(col, dtype=np.int32)
+        self.weight = None if weight is None else np.ascontiguousarray(weight, dtype=np.float32)
+        self.name = name
+
+    @property
+    def n_vertices(self):
+        return self.rowptr.size - 1
+
+    @property
+    def n_edges(self):
+        return self.col.size
+
+    def degrees(self):
+        return np.diff(self.rowptr)
+
+    def rowptr32(self):
+        if self.n_edges >= 2**31:
+            raise ValueError("E >= 2^31 needs int64 rowptr")
+        return self.rowptr.astype(np.int32)
+
+
+def _csr_from_edges(src, dst, V):
+    order = np.lexsort((dst, src))
+    src, dst = src[order], dst[order]
+    counts = np.bincount(src, minlength=V).astype(np.int64)
+    rowptr = np.zeros(V + 1, dtype=np.int64)
+    np.cumsum(counts, out=rowptr[1:])
+    return rowptr, dst.astype(np.int32)
+
+
+def weights(kind, n, seed):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    if kind == "uniform":
+        return (1.0 - rng.random(n, dtype=np.float32)).astype(np.float32)  # (0, 1]
+    if kind == "lognormal":
+        return rng.lognormal(0.0, 1.0, n).astype(np.float32)
+    if kind.startswith("pareto"):
+        alpha = float(kind.split(":")[1]) if ":" in kind else 1.5
+        return (1.0 + rng.pareto(alpha, n)).astype(np.float32)
+    if kind == "none":
+        return None
+    raise ValueError(kind)
+
+
+def rmat(scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=0, symmetrize=True, weight="uniform",
+         chunk=1 << 22):
+    """R-MAT graph with 2^scale vertices and edge_factor * 2^scale generated edges."""
+    V = 1 << scale
+    E = edge_factor * V
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ab, abc = a + b, a + b + c
+    srcs, dsts = [], []
+    for off in range(0, E, chunk):
+        n = min(chunk, E - off)
+        s = np.zeros(n, dtype=np.int64)
+        d = np.zeros(n, dtype=np.int64)
+        for bit in range(scale):
+            r = rng.random(n, dtype=np.float32)
+            sbit = r >= ab                      # quadrants c, d
+            dbit = ((r >= a) & (r < ab)) | (r >= abc)  # quadrants b, d
+            s |= sbit.astype(np.int64) << bit
+            d |= dbit.astype(np.int64) << bit
+        srcs.append(s)
+        dsts.append(d)
+    s = np.concatenate(srcs)
+    d = np.concatenate(dsts)
+    if symmetrize:
+        s, d = np.concatenate([s, d]), np.concatenate([d, s])
+    keep = s != d
+    s, d = s[keep], d[keep]
+    key = np.unique(s * V + d)
+    s, d = key // V, key % V
+    rowptr, col = _csr_from_edges(s, d, V)
+    w = weights(weight, col.size, seed + 1)
+    return CSR(rowptr, col, w, name=f"rmat{scale}_ef{edge_factor}")
+
+
+def powerlaw_directed(n_vertices=875_713, n_edges=5_105_039, gamma=2.1, max_degree=460, zipf=0.6,
+                      seed=0, weight="lognormal"):
+    """Directed graph whose out-degrees follow P(d) ~ d^-gamma on [1, max_degree]."""
+    V, E = n_vertices, n_edges
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ds = np.arange(1, max_degree + 1, dtype=np.float64)
+    pmf = ds ** (-gamma)
+    pmf /= pmf.sum()
+    deg = rng.choice(ds.astype(np.int64), size=V, p=pmf)
+    # rescale the sequence to sum to E (keeps the power-law shape), cap, then fix the remainder
+    deg = np.minimum(np.floor(deg * (E / deg.sum())).astype(np.int64), max_degree)
+    deg[np.argmax(deg)] = max_degree
+    diff = E - int(deg.sum())
+    while diff != 0:
+        idx = rng.integers(0, V, size=abs(diff) * 2)
+        for v in idx:
+            if diff > 0 and deg[v] < max_degree:
+                deg[v] += 1
+                diff -= 1
+            elif diff < 0 and deg[v] > 0 and deg[v] != max_degree:
+                deg[v] -= 1
+                diff += 1
+            if diff == 0:
+                break
+    # destinations: Zipf popularity over a random permutation of the vertices
+    perm = rng.permutation(V)
+    pop = (np.arange(1, V + 1, dtype=np.float64)) ** (-zipf)
+    cdf = np.cumsum(pop)
+    cdf /= cdf[-1]
+    src = np.repeat(np.arange(V, dtype=np.int64), deg)
+    dst = perm[np.searchsorted(cdf, rng.random(src.size))]
+    for _ in range(64):  # redraw self loops and duplicate (src, dst) pairs
+        key = src * V + dst
+        order = np.argsort(key, kind="stable")
+        ks = key[order]
+        dup = np.zeros(ks.size, dtype=bool)
+        dup[1:] = ks[1:] == ks[:-1]
+        bad = np.zeros(src.size, dtype=bool)
+        bad[order[dup]] = True
+        bad |= src == dst
+        nb = int(bad.sum())
+        if nb == 0:
+            break
+        dst[bad] = perm[np.searchsorted(cdf, rng.random(nb))]
+    else:
+        raise RuntimeError("could not remove duplicate edges")
+    rowptr, col = _csr_from_edges(src, dst, V)
+    w = weights(weight, col.size, seed + 1)
+    return CSR(rowptr, col, w, name=f"powerlaw_v{V}_e{E}")
+
+
+def write_reference_format(g, beg_path, csr_path):
+    """beg.bin = int64[V+1], csr.bin = int64[E] (reference graph.hpp:18-34)."""
+    g.rowptr.astype(np.int64).tofile(beg_path)
+    g.col.astype(np.int64).tofile(csr_path)
+
+
+def read_reference_format(beg_path, csr_path):
+    rowptr = np.fromfile(beg_path, dtype=np.int64)
+    col = np.fromfile(csr_path, dtype=np.int64)[: rowptr[-1]]
+    return CSR(rowptr, col.astype(np.int32), None, name="file")

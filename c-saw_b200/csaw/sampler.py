@@ -1,0 +1,172 @@
+"""Host-side mirror of C-SAW's sampler interface over the csaw-b200 C ABI.
+
+C-SAW's user surface is its positional run parameters -- #samples
+(n_subgraph), FrontierSize, NeighborSize, Depth/Length (mpi_main.cpp:19-28,
+README.md:30) -- the api.cuh hooks, a CSR input and a per-sample edge list
+output (Si, sample_class.cuh:76-90).  `Graph.sample` takes the same
+parameters and returns the edge list as (src, dst, sample, depth) tensors;
+`Sampler` keeps the reference's host entry point (non-stream/main.cu:196).
+PyTorch only provides device buffers and the current stream here.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import (BIAS_DEGREE, BIAS_EDGE_WEIGHT, BIAS_HOOK, BIAS_UNBIASED, MODE_MDRW, MODE_NEIGHBOR,
+                   MODE_WALK, SCHED_PLAIN, CsawError, check, lib)
+
+BIAS_NAMES = {"unbiased": BIAS_UNBIASED, "degree": BIAS_DEGREE, "weight": BIAS_EDGE_WEIGHT,
+              "hook": BIAS_HOOK}
+MODE_NAMES = {"neighbor": MODE_NEIGHBOR, "walk": MODE_WALK, "mdrw": MODE_MDRW}
+
+
+def make_params(mode, bias, n_samples, frontier_size=1, neighbor_size=1, depth=1, fanout=None, seed=0,
+                schedule=SCHED_PLAIN):
+    p = _lib.Params()
+    p.mode = MODE_NAMES.get(mode, mode)
+    p.bias = BIAS_NAMES.get(bias, bias)
+    p.schedule = schedule
+    p.n_samples = n_samples
+    p.frontier_size = frontier_size
+    p.neighbor_size = neighbor_size
+    p.depth = depth
+    for i, n in enumerate(fanout or []):
+        p.fanout[i] = n
+    p.seed = seed
+    return p
+
+
+def fanouts(p):
+    return [p.fanout[i] or p.neighbor_size for i in range(p.depth)]
+
+
+def edge_bound(p):
+    """Largest possible number of output edges for params p."""
+    if p.mode == MODE_NEIGHBOR:
+        tot, lvl = 0, p.frontier_size
+        for n in fanouts(p):
+            lvl *= n
+            tot += lvl
+        return p.n_samples * tot
+    return p.n_samples * p.depth
+
+
+def _torch():
+    import torch
+    return torch
+
+
+class Graph:
+    """A CSR resident on the current CUDA device (csaw_graph_create)."""
+
+    def __init__(self, csr, rowptr64=None, degree_bias=False, cdf_cache=False):
+        L = lib()
+        if rowptr64 is None:
+            rowptr64 = csr.n_edges >= 2**31
+        self.rowptr_host = csr.rowptr if rowptr64 else csr.rowptr32()
+        self.csr = csr
+        flags = (_lib.GRAPH_DEGREE_BIAS if degree_bias else 0) | (_lib.GRAPH_CDF_CACHE if cdf_cache else 0)
+        h = ctypes.c_void_p()
+        w = None if csr.weight is None else csr.weight.ctypes.data_as(ctypes.c_void_p)
+        check(L.csaw_graph_create(self.rowptr_host.ctypes.data_as(ctypes.c_void_p), int(rowptr64),
+                                  csr.col.ctypes.data_as(ctypes.c_void_p), w, csr.n_vertices,
+                                  csr.n_edges, flags, ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().csaw_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def stats(self):
+        s = _lib.Stats()
+        check(lib().csaw_graph_stats(self.h, ctypes.byref(s)))
+        return {f: getattr(s, f) for f, _ in _lib.Stats._fields_}
+
+    def profile(self, enable=True):
+        check(lib().csaw_graph_profile(self.h, int(enable)))
+
+    def kernel_stats(self, kind):
+        ms = ctypes.c_double()
+        n, b, it = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        check(lib().csaw_graph_kernel_stats(self.h, _lib.KERNEL_KINDS.get(kind, kind), ctypes.byref(ms),
+                                            ctypes.byref(n), ctypes.byref(b), ctypes.byref(it)))
+        return {"ms": ms.value, "launches": n.value, "bytes": b.value, "items": it.value}
+
+    def make_seeds(self, n, seed, stream=None):
+        torch = _torch()
+        out = torch.empty(max(n, 1), dtype=torch.int32, device="cuda")
+        st = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        check(lib().csaw_make_seeds(self.h, n, seed, ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(st)))
+        return out[:n]
+
+    def sample(self, params, seeds, capacity=None, out=None, with_sample=True, with_depth=True, stream=None):
+        """Run one job on device seeds; returns (src, dst, sample, depth) device tensors."""
+        torch = _torch()
+        if capacity is None:
+            capacity = edge_bound(params)
+        if out is None:
+            out = torch.empty((2 + with_sample + with_depth, max(capacity, 1)), dtype=torch.int32, device="cuda")
+        ptrs = [ctypes.c_void_p(out[i].data_ptr()) for i in range(out.shape[0])]
+        src, dst = ptrs[0], ptrs[1]
+        smp = ptrs[2] if with_sample else None
+        dep = ptrs[2 + with_sample] if with_depth else None
+        n = ctypes.c_int64()
+        st = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        seeds = seeds.to(device="cuda", dtype=torch.int32).contiguous()
+        check(lib().csaw_sample(self.h, ctypes.byref(params), ctypes.c_void_p(seeds.data_ptr()), src, dst, smp,
+                                dep, capacity, ctypes.byref(n), ctypes.c_void_p(st)))
+        k = n.value
+        res = [out[0, :k], out[1, :k]]
+        res.append(out[2, :k] if with_sample else None)
+        res.append(out[2 + with_sample, :k] if with_depth else None)
+        return tuple(res)
+
+    def sample_host(self, params, seeds, capacity=None, with_sample=True, with_depth=True, out=None,
+                    stream=None):
+        """Host seeds in, host edge list out (copies inside the call)."""
+        if capacity is None:
+            capacity = edge_bound(params)
+        seeds = np.ascontiguousarray(seeds, dtype=np.int32)
+        if out is None:
+            out = np.empty((2 + with_sample + with_depth, max(capacity, 1)), dtype=np.int32)
+        ptr = lambda i: out[i].ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+        n = ctypes.c_int64()
+        st = ctypes.c_void_p(stream) if stream is not None else None
+        check(lib().csaw_sample_host(self.h, ctypes.byref(params), seeds.ctypes.data_as(ctypes.c_void_p), ptr(0),
+                                     ptr(1), ptr(2) if with_sample else None,
+                                     ptr(2 + with_sample) if with_depth else None, capacity, ctypes.byref(n), st))
+        k = n.value
+        return (out[0, :k], out[1, :k], out[2, :k] if with_sample else None,
+                out[2 + with_sample, :k] if with_depth else None)
+
+
+class Arguments:
+    """struct arguments of the reference (sampler.cuh:3-6)."""
+
+    def __init__(self, sampled_edges=0, time=0.0):
+        self.sampled_edges = sampled_edges
+        self.time = time
+
+
+def Sampler(beg, csr, n_blocks, n_threads, n_subgraph, FrontierSize, NeighborSize, Depth, args=None, rank=0):
+    """Reference host entry (non-stream/main.cu:196): loads int64 beg/csr files,
+    samples (FrontierSize == 1) or runs MDRW (FrontierSize > 1), returns
+    Arguments(sampled_edges, time)."""
+    e = ctypes.c_int()
+    t = ctypes.c_double()
+    check(lib().csaw_sampler_compat(str(beg).encode(), str(csr).encode(), n_blocks, n_threads, n_subgraph,
+                                    FrontierSize, NeighborSize, Depth, ctypes.byref(e), ctypes.byref(t)))
+    out = args if args is not None else Arguments()
+    out.sampled_edges, out.time = e.value, t.value
+    return out
+
+
+__all__ = ["Graph", "Sampler", "Arguments", "make_params", "edge_bound", "CsawError"]

@@ -1,0 +1,370 @@
+// csaw_device.cuh -- device primitives of the csaw-b200 sampler (sm_100a).
+//
+// Every float operation here is one IEEE round-to-nearest add, multiply or
+// max, in the canonical order documented in csaw_internal.h, so the CUDA path
+// is bit-identical to the CPU restatement of the same semantics.  The library
+// is built with --fmad=false as a second guard against FMA contraction.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "csaw.h"
+#include "csaw_api.cuh"
+#include "csaw_internal.h"
+
+namespace csaw {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// --------------------------------------------------------------- graph view
+struct DevGraph {
+    csaw_graph_view v;     // what the user hooks see
+    const float *ebias;    // materialised neighbor degree per edge, or null
+    const float *cdf;      // canonical per-vertex prefix of cdf_bias, or null
+    int cdf_bias;          // bias kind the cdf was built for
+};
+
+template <typename I>
+__device__ __forceinline__ int64_t row_begin(const DevGraph &g, int64_t v) {
+    return (int64_t)__ldg(((const I *)g.v.rowptr) + v);
+}
+
+template <typename I>
+__device__ __forceinline__ float degree_f(const DevGraph &g, int32_t u) {
+    const I *r = (const I *)g.v.rowptr;
+    return __ll2float_rn((long long)(__ldg(r + u + 1) - __ldg(r + u)));
+}
+
+// Bias of edge e (neighbor col[e]) for the bias kind BIAS.
+template <typename I, int BIAS>
+__device__ __forceinline__ float edge_bias(const DevGraph &g, int64_t e) {
+    if constexpr (BIAS == CSAW_BIAS_EDGE_WEIGHT) {
+        return __ldg(g.v.weight + e);
+    } else if constexpr (BIAS == CSAW_BIAS_DEGREE) {
+        if (g.ebias) return __ldg(g.ebias + e);
+        return degree_f<I>(g, __ldg(g.v.col + e));
+    } else {
+        return EdgeBias(__ldg(g.v.col + e), e, &g.v);
+    }
+}
+
+// ------------------------------------------------------------------- Philox
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC11).
+__device__ __forceinline__ uint4 philox(uint4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+__device__ __forceinline__ uint32_t word_of(uint4 b, int w) {
+    return w == 0 ? b.x : (w == 1 ? b.y : (w == 2 ? b.z : b.w));
+}
+
+__device__ __forceinline__ float unit24(uint32_t x) {
+    return __fmul_rn(__uint2float_rn(x >> 8), 5.9604644775390625e-8f);
+}
+
+__device__ __forceinline__ uint32_t mulhi(uint32_t x, uint32_t n) { return __umulhi(x, n); }
+
+// t = unit(x) * T, kept strictly below T.
+__device__ __forceinline__ float its_target(uint32_t x, float T) {
+    float t = __fmul_rn(unit24(x), T);
+    if (!(t < T)) t = __int_as_float(__float_as_int(T) - 1);
+    return t;
+}
+
+// First i in [0, d) with P[i] > t (P monotone, P[d-1] > t).
+__device__ __forceinline__ int64_t search_upper(const float *P, int64_t d, float t) {
+    int64_t lo = 0, hi = d - 1;
+    while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        if (P[mid] > t) hi = mid; else lo = mid + 1;
+    }
+    return lo;
+}
+
+// ------------------------------------------------------------ warp scans
+__device__ __forceinline__ float warp_ks_sum(float v, int lane) {
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        float up = __shfl_up_sync(FULL, v, off);
+        if (lane >= off) v = __fadd_rn(v, up);
+    }
+    return v;
+}
+
+__device__ __forceinline__ float warp_max_scan(float v, int lane) {
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        float up = __shfl_up_sync(FULL, v, off);
+        if (lane >= off) v = fmaxf(v, up);
+    }
+    return v;
+}
+
+// Canonical prefix of wfn(0..d) into P[0..d) computed by one warp; elements
+// whose bit is set in zmask (if given) count as 0.  Returns T = P[d-1] on
+// every lane.  P may live in shared or global memory.
+template <typename WFn>
+__device__ float warp_canon_prefix(WFn wfn, int64_t d, float *P, const uint32_t *zmask, int lane) {
+    const int64_t ntiles = (d + 31) >> 5;
+    float C = 0.f, runmax = 0.f;
+    for (int64_t g0 = 0; g0 < ntiles; g0 += 32) {
+        const int gt = (ntiles - g0) < 32 ? (int)(ntiles - g0) : 32;
+        float my_tsum = 0.f;
+        for (int tt = 0; tt < gt; ++tt) {
+            int64_t i = ((g0 + tt) << 5) + lane;
+            float w = 0.f;
+            if (i < d) {
+                w = wfn(i);
+                if (zmask && ((zmask[i >> 5] >> (i & 31)) & 1u)) w = 0.f;
+            }
+            float v = warp_ks_sum(w, lane);
+            if (i < d) P[i] = v;
+            float s = __shfl_sync(FULL, v, 31);
+            if (lane == tt) my_tsum = s;
+        }
+        float q = warp_ks_sum(my_tsum, lane);
+        float qex = __shfl_up_sync(FULL, q, 1);
+        if (lane == 0) qex = 0.f;
+        float gtot = __shfl_sync(FULL, q, 31);
+        __syncwarp();
+        for (int tt = 0; tt < gt; ++tt) {
+            int64_t i = ((g0 + tt) << 5) + lane;
+            float qx = __shfl_sync(FULL, qex, tt);
+            float p = 0.f;
+            if (i < d) p = __fadd_rn(C, __fadd_rn(qx, P[i]));
+            p = fmaxf(warp_max_scan(p, lane), runmax);
+            if (i < d) P[i] = p;
+            runmax = __shfl_sync(FULL, p, 31);
+        }
+        C = __fadd_rn(C, gtot);
+    }
+    __syncwarp();
+    return runmax;
+}
+
+// Same canonical prefix computed by a whole CTA (all threads must call).
+// Scratch: tsum[ntiles], gcar[ngroups] (shared or global).
+template <typename WFn>
+__device__ float cta_canon_prefix(WFn wfn, int64_t d, float *P, float *tsum, float *gcar,
+                                  const uint32_t *zmask) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int64_t ntiles = (d + 31) >> 5, ngroups = (ntiles + 31) >> 5;
+    for (int64_t t = warp; t < ntiles; t += nw) {
+        int64_t i = (t << 5) + lane;
+        float w = 0.f;
+        if (i < d) {
+            w = wfn(i);
+            if (zmask && ((zmask[i >> 5] >> (i & 31)) & 1u)) w = 0.f;
+        }
+        float v = warp_ks_sum(w, lane);
+        if (i < d) P[i] = v;
+        if (lane == 31) tsum[t] = v;
+    }
+    __syncthreads();
+    for (int64_t gg = warp; gg < ngroups; gg += nw) {
+        int64_t t = (gg << 5) + lane;
+        float s = t < ntiles ? tsum[t] : 0.f;
+        float q = warp_ks_sum(s, lane);
+        float qex = __shfl_up_sync(FULL, q, 1);
+        if (lane == 0) qex = 0.f;
+        __syncwarp();
+        if (t < ntiles) tsum[t] = qex;
+        if (lane == 31) gcar[gg] = q;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float C = 0.f;
+        for (int64_t gg = 0; gg < ngroups; ++gg) {
+            float tot = gcar[gg];
+            gcar[gg] = C;
+            C = __fadd_rn(C, tot);
+        }
+    }
+    __syncthreads();
+    for (int64_t t = warp; t < ntiles; t += nw) {
+        int64_t i = (t << 5) + lane;
+        float C = gcar[t >> 5], qx = tsum[t];
+        float p = 0.f;
+        if (i < d) p = __fadd_rn(C, __fadd_rn(qx, P[i]));
+        p = warp_max_scan(p, lane);
+        if (i < d) P[i] = p;
+        __syncwarp();
+        if (lane == 31) tsum[t] = p;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        float carry = 0.f;
+        for (int64_t base = 0; base < ntiles; base += 32) {
+            int64_t t = base + lane;
+            float m = t < ntiles ? tsum[t] : 0.f;
+            float ms = warp_max_scan(m, lane);
+            float ex = __shfl_up_sync(FULL, ms, 1);
+            if (lane == 0) ex = 0.f;
+            ex = fmaxf(ex, carry);
+            __syncwarp();
+            if (t < ntiles) tsum[t] = ex;
+            carry = fmaxf(carry, __shfl_sync(FULL, ms, 31));
+        }
+    }
+    __syncthreads();
+    for (int64_t t = warp; t < ntiles; t += nw) {
+        int64_t i = (t << 5) + lane;
+        if (i < d) P[i] = fmaxf(P[i], tsum[t]);
+    }
+    __syncthreads();
+    return P[d - 1];
+}
+
+// ------------------------------------------------------------- selection
+// Draw words of one slot: word A of slot `slot` of item (p, s, l).
+struct DrawCtx {
+    uint32_t k0, k1, p, s, l;
+};
+
+struct SlotRng {
+    uint4 blk;
+    int blk_id = -1;
+    __device__ __forceinline__ uint32_t word(const DrawCtx &dc, int slot, int A) {
+        if ((A >> 2) != blk_id) {
+            blk = philox(make_uint4(dc.p, dc.s, (TAG_SAMPLE << 24) | dc.l,
+                                    ((uint32_t)slot << 16) | (uint32_t)(A >> 2)),
+                         dc.k0, dc.k1);
+            blk_id = A >> 2;
+        }
+        return word_of(blk, A & 3);
+    }
+};
+
+// Resolver state of the warp-parallel sequential-order selection: lane j owns
+// slot j.  j (current slot) and a (draws in this phase for slot j) are warp
+// uniform; A (draws used by the lane's slot), cand and sel are per lane.
+struct SelState {
+    int j = 0, a = 1, A = 0;
+    int cand = -1, sel = -1;
+};
+
+// Runs slots in order until all N are accepted (returns 0) or the current slot
+// has exhausted its REJECT_ATTEMPTS draws in this phase (returns 1: rebuild).
+// A slot that has used MAX_SLOT_DRAWS draws takes the smallest unselected
+// index, so the loop always ends.
+template <typename CandFn>
+__device__ __forceinline__ int resolve_slots(SelState &st, int N, int lane, const DrawCtx &dc,
+                                             SlotRng &rng, CandFn cand_of) {
+    while (st.j < N) {
+        const int j = st.j;
+        int c = __shfl_sync(FULL, st.cand, j);
+        unsigned coll = __ballot_sync(FULL, lane < j && st.sel == c);
+        if (!coll) {
+            if (lane == j) st.sel = c;
+            st.j = j + 1;
+            st.a = 1;
+            continue;
+        }
+        if (__shfl_sync(FULL, st.A, j) == MAX_SLOT_DRAWS) {
+            int i = 0;
+            while (__ballot_sync(FULL, lane < j && st.sel == i)) ++i;
+            if (lane == j) st.sel = i;
+            st.j = j + 1;
+            st.a = 1;
+            continue;
+        }
+        if (st.a == REJECT_ATTEMPTS) return 1;
+        if (lane == j) {
+            st.cand = cand_of(rng.word(dc, lane, st.A));
+            st.A++;
+        }
+        st.a++;
+    }
+    return 0;
+}
+
+// Zero-mass fill: slots j..N-1 take the smallest indices not yet selected.
+__device__ __forceinline__ void zero_fill(SelState &st, int N, int lane) {
+    int i = 0;
+    for (int jj = st.j; jj < N; ++jj) {
+        while (__ballot_sync(FULL, lane < jj && st.sel == i)) ++i;
+        if (lane == jj) st.sel = i;
+        ++i;
+    }
+    st.j = N;
+}
+
+// Sorted copy of the selections of lanes < j into zs[0..j) (unbiased phases).
+__device__ __forceinline__ void sort_selected(const SelState &st, int j, int *zs, int lane) {
+    int rank = 0;
+    for (int m = 0; m < j; ++m) {
+        int sm = __shfl_sync(FULL, st.sel, m);
+        if (sm < st.sel) ++rank;
+    }
+    __syncwarp();
+    if (lane < j) zs[rank] = st.sel;
+    __syncwarp();
+}
+
+// Index of the t-th (0-based) element of [0, d) not in the sorted zs[0..nZ).
+__device__ __forceinline__ int kth_not_excluded(uint32_t t, const int *zs, int nZ) {
+    for (int m = 0; m < nZ; ++m)
+        if ((uint32_t)zs[m] <= t) ++t;
+    return (int)t;
+}
+
+// ----------------------------------------------------------- staged output
+// Per-warp staging of output edges in shared memory; one atomic per flush.
+struct OutArgs {
+    int32_t *src, *dst, *smp, *dep;
+    unsigned long long *count;
+    int64_t cap;
+};
+
+constexpr int STAGE = 64;
+
+struct WarpStage {
+    int32_t *s_src, *s_dst, *s_smp, *s_dep;  // STAGE entries each (shared)
+    int cnt = 0;
+
+    __device__ __forceinline__ void flush(const OutArgs &o, int lane) {
+        if (cnt == 0) return;
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(o.count, (unsigned long long)cnt);
+        base = __shfl_sync(FULL, base, 0);
+        for (int i = lane; i < cnt; i += 32) {
+            int64_t pos = (int64_t)base + i;
+            if (pos < o.cap) {
+                o.src[pos] = s_src[i];
+                o.dst[pos] = s_dst[i];
+                if (o.smp) o.smp[pos] = s_smp[i];
+                if (o.dep) o.dep[pos] = s_dep[i];
+            }
+        }
+        cnt = 0;
+        __syncwarp();
+    }
+
+    __device__ __forceinline__ void push(const OutArgs &o, bool act, int32_t u, int32_t v, int32_t s,
+                                         int32_t l, int lane) {
+        unsigned m = __ballot_sync(FULL, act);
+        int n = __popc(m);
+        if (n == 0) return;
+        if (cnt + n > STAGE) flush(o, lane);
+        if (act) {
+            int pos = cnt + __popc(m & ((1u << lane) - 1u));
+            s_src[pos] = u;
+            s_dst[pos] = v;
+            s_smp[pos] = s;
+            s_dep[pos] = l;
+        }
+        cnt += n;
+        __syncwarp();
+    }
+};
+
+}  // namespace csaw

@@ -1,0 +1,86 @@
+// csaw_internal.h -- constants and launch-argument structs shared by the
+// csaw-b200 kernels and their host driver.
+//
+// Output semantics (the CPU oracle restates them in plain C):
+//
+// RNG.  Philox4x32-10 keyed by (seed lo, seed hi).  Neighbor selection of
+// (sample s, depth l, lineage item p, slot j, draw A) uses word (A & 3) of the
+// block at counter {p, s, (TAG_SAMPLE << 24) | l, (j << 16) | (A >> 2)}.  A
+// walk is neighbor sampling with N = 1.  MDRW step t of sample s uses words 0
+// and 1 of {0, s, (TAG_MDRW << 24) | t, 0}; seed i uses word 0 of
+// {i lo, i hi, TAG_SEED << 24, 0}.  Because the counter names the work item and
+// never the thread, the output does not depend on the schedule.
+//
+// Canonical prefix of d biases: Kogge-Stone scans over 32-element tiles,
+// Kogge-Stone over the tile totals of each 32-tile group, serial carry across
+// groups, P_i = C_g + (Qex_t + v_i), then a running max.  Inverse transform:
+// t = unit24(x) * T (kept below T), index = first i with P_i > t.
+//
+// Selection without replacement (k = min(N, d)): d <= N takes every neighbor;
+// otherwise slots 0..N-1 in order draw until the index is new; after
+// REJECT_ATTEMPTS rejected draws in one phase the selected set is zeroed out of
+// the prefix (unbiased: excluded from the index range) and a new phase starts;
+// with no positive mass left, remaining slots take the smallest unselected
+// indices, and a slot that has used MAX_SLOT_DRAWS draws takes the smallest
+// unselected index (termination guard).
+#pragma once
+
+#include <cstdint>
+
+namespace csaw {
+
+constexpr uint32_t TAG_SAMPLE = 1u;
+constexpr uint32_t TAG_MDRW = 2u;
+constexpr uint32_t TAG_SEED = 3u;
+constexpr int REJECT_ATTEMPTS = 4;
+constexpr int MAX_SLOT_DRAWS = 16;     // termination guard per slot
+
+constexpr int MAX_FANOUT = 32;      // slots are lanes of one warp
+constexpr int WBUF = 1024;          // prefix held in shared memory per warp
+constexpr int EXPAND_THREADS = 256; // 8 warps per CTA
+constexpr int HEAVY_THREADS = 256;
+constexpr int WALK_THREADS = 256;
+
+// One level of neighbor sampling: input queue -> output edges + next queue.
+struct LevelArgs {
+    const int32_t *in_v;
+    const int32_t *in_s;
+    const uint32_t *in_p;
+    const uint32_t *n_in;     // device count of input items
+    int32_t *out_v;
+    int32_t *out_s;
+    uint32_t *out_p;
+    uint32_t *n_out;          // device count of next-level items
+    uint32_t *heavy;          // deferred item indices (biased, d > WBUF)
+    uint32_t *n_heavy;
+    float *heavy_scratch;     // per-CTA scratch for the heavy kernel
+    int64_t heavy_stride;     // floats per CTA
+    int32_t *o_src, *o_dst, *o_smp, *o_dep;
+    unsigned long long *o_count;
+    int64_t cap;
+    unsigned long long *bytes; // algorithmic bytes accumulator
+    unsigned long long *items; // expanded-items accumulator
+    int *err;
+    uint32_t k0, k1;
+    int depth, N, push;
+};
+
+struct WalkArgs {
+    const int32_t *seeds;
+    int n;                    // walks (or samples for MDRW)
+    int len;                  // steps
+    int F;                    // MDRW frontier size
+    int32_t *o_src, *o_dst, *o_smp, *o_dep;
+    unsigned long long *o_count;
+    int64_t cap;
+    float *scratch;           // per-warp prefix scratch for d > WBUF (walks)
+    int64_t scratch_stride;
+    unsigned long long *bytes;
+    unsigned long long *items;
+    int *err;
+    uint32_t k0, k1;
+};
+
+enum : int { ERR_SEED_RANGE = 1, ERR_UPDATE_RANGE = 2, ERR_SCRATCH = 4 };
+
+}  // namespace csaw

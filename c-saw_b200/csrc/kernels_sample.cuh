@@ -1,0 +1,545 @@
+// kernels_sample.cuh -- sampling and walk kernels (sm_100a).
+//
+// C-SAW counterparts (non-stream/): check (main.cu:21-93) is the level
+// expansion below; get_neighbors (functions.cuh:872-892), ITS/gpu_prefix
+// (:112-176), binary_search (:11-43), bitmap_search (:45-70) and
+// heur_normalize (:743-868) are the canonical prefix, inverse-transform search
+// and slot resolver of csaw_device.cuh; frontier (:971-1011) is the staged
+// output and queue push; check_layer + ITS_MDRW (main.cu:95-194,
+// functions.cuh:1014-1060) is k_mdrw.
+#pragma once
+
+#include "csaw_device.cuh"
+
+namespace csaw {
+
+// Algorithmic bytes of one expansion (what the algorithm must touch; sector
+// waste not counted): queue item 12 B, rowptr pair, bias reads when the
+// prefix is scanned, the selected col entries, the output edges and the pushed
+// children.
+template <typename I, int BIAS>
+__device__ __forceinline__ unsigned long long expansion_bytes(const DevGraph &g, int64_t d, int k,
+                                                              bool scanned, const LevelArgs &a) {
+    unsigned long long b = 12 + 2 * sizeof(I);
+    if (scanned) {
+        if (BIAS == CSAW_BIAS_EDGE_WEIGHT || (BIAS == CSAW_BIAS_DEGREE && g.ebias))
+            b += 4ull * d + 4ull * k;
+        else
+            b += (4ull + 2ull * sizeof(I)) * d;  // col + neighbor rowptr pairs
+    } else {
+        b += 4ull * k;
+    }
+    b += 4ull * k * (2 + (a.o_smp != nullptr) + (a.o_dep != nullptr));
+    if (a.push) b += 12ull * k;
+    return b;
+}
+
+// -------------------------------------------------------------- queue init
+__global__ void k_init_queue(const int32_t *seeds, uint32_t n, int F, int s0, int64_t V,
+                             int32_t *qv, int32_t *qs, uint32_t *qp, uint32_t *qn, int *err) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) *qn = n;
+    if (i >= n) return;
+    int32_t v = seeds[i];
+    if (v < 0 || v >= V) {
+        atomicOr(err, ERR_SEED_RANGE);
+        v = 0;
+    }
+    qv[i] = v;
+    qs[i] = s0 + (int32_t)(i / (uint32_t)F);
+    qp[i] = i % (uint32_t)F;
+}
+
+// ------------------------------------------------------- warp selection
+// Selection for one item with d > N by one warp; returns the lane's slot
+// selection (lanes < N).  P/zb/zs: the warp's shared buffers (d <= WBUF).
+template <typename I, int BIAS>
+__device__ __forceinline__ int select_warp(const DevGraph &g, int64_t beg, int64_t d, int N,
+                                           const DrawCtx &dc, float *P, uint32_t *zb, int *zs,
+                                           int lane) {
+    constexpr bool BIASED = BIAS != CSAW_BIAS_UNBIASED;
+    auto wfn = [&](int64_t i) { return edge_bias<I, BIAS>(g, beg + i); };
+    float T = 0.f;
+    int nZ = 0;
+    const float *PP = P;
+    if constexpr (BIASED) {
+        if (g.cdf && g.cdf_bias == BIAS) {
+            PP = g.cdf + beg;
+            T = PP[d - 1];
+        } else {
+            T = warp_canon_prefix(wfn, d, P, nullptr, lane);
+        }
+    }
+    SlotRng rng;
+    SelState st;
+    auto cand_of = [&](uint32_t x) -> int {
+        if constexpr (BIASED) return (int)search_upper(PP, d, its_target(x, T));
+        else return kth_not_excluded(mulhi(x, (uint32_t)(d - nZ)), zs, nZ);
+    };
+    bool zero = BIASED && !(T > 0.f);
+    if (!zero && lane < N) {
+        st.cand = cand_of(rng.word(dc, lane, 0));
+        st.A = 1;
+    }
+    for (;;) {
+        if (zero) {
+            zero_fill(st, N, lane);
+            break;
+        }
+        if (resolve_slots(st, N, lane, dc, rng, cand_of) == 0) break;
+        const int j = st.j;
+        if constexpr (BIASED) {
+            const int nwords = (int)((d + 31) >> 5);
+            for (int w = lane; w < nwords; w += 32) zb[w] = 0u;
+            __syncwarp();
+            if (lane < j) atomicOr(&zb[st.sel >> 5], 1u << (st.sel & 31));
+            __syncwarp();
+            T = warp_canon_prefix(wfn, d, P, zb, lane);
+            PP = P;
+            if (!(T > 0.f)) {
+                zero = true;
+                continue;
+            }
+        } else {
+            sort_selected(st, j, zs, lane);
+            nZ = j;
+        }
+        if (lane == j) {
+            st.cand = cand_of(rng.word(dc, lane, st.A));
+            st.A++;
+        } else if (lane > j && lane < N) {
+            st.cand = cand_of(rng.word(dc, lane, 0));
+        }
+        st.a = 1;
+    }
+    return st.sel;
+}
+
+// ----------------------------------------------------- level expansion
+// One warp per queue item (grid-stride, persistent grid).  Biased items whose
+// degree exceeds WBUF are deferred to k_expand_heavy.
+template <typename I, int BIAS>
+__global__ void __launch_bounds__(EXPAND_THREADS)
+k_expand_warp(DevGraph g, LevelArgs a) {
+    constexpr bool BIASED = BIAS != CSAW_BIAS_UNBIASED;
+    constexpr int NW = EXPAND_THREADS / 32;
+    __shared__ float s_P[BIASED ? NW * WBUF : 1];
+    __shared__ uint32_t s_z[BIASED ? NW * (WBUF / 32) : 1];
+    __shared__ int s_zs[NW * 32];
+    __shared__ int32_t s_out[NW * 4 * STAGE];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    float *P = s_P + (BIASED ? wib * WBUF : 0);
+    uint32_t *zb = s_z + (BIASED ? wib * (WBUF / 32) : 0);
+    int *zs = s_zs + wib * 32;
+    WarpStage stg;
+    stg.s_src = s_out + wib * 4 * STAGE;
+    stg.s_dst = stg.s_src + STAGE;
+    stg.s_smp = stg.s_dst + STAGE;
+    stg.s_dep = stg.s_smp + STAGE;
+    const OutArgs oa{a.o_src, a.o_dst, a.o_smp, a.o_dep, a.o_count, a.cap};
+    const uint32_t n = *a.n_in;
+    const int N = a.N;
+    unsigned long long my_bytes = 0, my_items = 0;
+    for (uint32_t it = gw; it < n; it += nw) {
+        const int32_t v = a.in_v[it];
+        const int32_t s = a.in_s[it];
+        const uint32_t p = a.in_p[it];
+        const int64_t beg = row_begin<I>(g, v);
+        const int64_t d = row_begin<I>(g, v + 1) - beg;
+        if (d <= 0) {
+            my_items++;
+            my_bytes += 12 + 2 * sizeof(I);
+            continue;
+        }
+        if (BIASED && d > N && d > WBUF && !(g.cdf && g.cdf_bias == BIAS)) {
+            if (lane == 0) {
+                uint32_t h = atomicAdd(a.n_heavy, 1u);
+                a.heavy[h] = it;
+            }
+            continue;
+        }
+        my_items++;
+        const int k = d < N ? (int)d : N;
+        int sel = lane;
+        bool scanned = false;
+        if (d > N) {
+            scanned = BIASED && !(g.cdf && g.cdf_bias == BIAS);
+            const DrawCtx dc{a.k0, a.k1, p, (uint32_t)s, (uint32_t)a.depth};
+            sel = select_warp<I, BIAS>(g, beg, d, N, dc, P, zb, zs, lane);
+        }
+        bool act = lane < k;
+        int32_t dst = 0;
+        if (act) {
+            dst = Update(&g.v, __ldg(g.v.col + beg + sel), v);
+            if (dst < 0 || dst >= g.v.n_vertices) {
+                atomicOr(a.err, ERR_UPDATE_RANGE);
+                dst = 0;
+            }
+        }
+        stg.push(oa, act, v, dst, s, a.depth, lane);
+        if (a.push) {
+            uint32_t q = 0;
+            if (lane == 0) q = atomicAdd(a.n_out, (uint32_t)k);
+            q = __shfl_sync(FULL, q, 0);
+            if (act) {
+                a.out_v[q + lane] = dst;
+                a.out_s[q + lane] = s;
+                a.out_p[q + lane] = p * (uint32_t)N + (uint32_t)lane;
+            }
+        }
+        my_bytes += expansion_bytes<I, BIAS>(g, d, k, scanned, a);
+    }
+    stg.flush(oa, lane);
+    if (lane == 0) {
+        atomicAdd(&a.bytes[0], my_bytes);
+        atomicAdd(&a.items[0], my_items);
+    }
+}
+
+// ------------------------------------------------ high-degree expansion
+// One CTA per deferred item: the canonical prefix is built by the whole CTA in
+// global scratch (same canonical order, so bit-identical to the warp path);
+// warp 0 runs the slot resolver; every rebuild is a CTA-wide rescan.
+template <typename I, int BIAS>
+__global__ void __launch_bounds__(HEAVY_THREADS)
+k_expand_heavy(DevGraph g, LevelArgs a) {
+    __shared__ int s_flag, s_j;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float *P = a.heavy_scratch + (int64_t)blockIdx.x * a.heavy_stride;
+    const uint32_t nh = *a.n_heavy;
+    const int N = a.N;
+    unsigned long long my_bytes = 0, my_items = 0;
+    for (uint32_t h = blockIdx.x; h < nh; h += gridDim.x) {
+        const uint32_t it = a.heavy[h];
+        const int32_t v = a.in_v[it];
+        const int32_t s = a.in_s[it];
+        const uint32_t p = a.in_p[it];
+        const int64_t beg = row_begin<I>(g, v);
+        const int64_t d = row_begin<I>(g, v + 1) - beg;
+        if (d + (d >> 5) + (d >> 10) + (d >> 5) + 8 > a.heavy_stride) {
+            if (threadIdx.x == 0) atomicOr(a.err, ERR_SCRATCH);
+            continue;
+        }
+        float *tsum = P + d;
+        float *gcar = tsum + (d >> 5) + 1;
+        uint32_t *zb = (uint32_t *)(gcar + (d >> 10) + 1);
+        auto wfn = [&](int64_t i) { return edge_bias<I, BIAS>(g, beg + i); };
+        float T = cta_canon_prefix(wfn, d, P, tsum, gcar, nullptr);
+        const DrawCtx dc{a.k0, a.k1, p, (uint32_t)s, (uint32_t)a.depth};
+        SlotRng rng;
+        SelState st;
+        auto cand_of = [&](uint32_t x) -> int { return (int)search_upper(P, d, its_target(x, T)); };
+        bool zero = !(T > 0.f);
+        if (warp == 0 && !zero && lane < N) {
+            st.cand = cand_of(rng.word(dc, lane, 0));
+            st.A = 1;
+        }
+        for (;;) {
+            if (warp == 0) {
+                int r = 0;
+                if (zero) zero_fill(st, N, lane);
+                else r = resolve_slots(st, N, lane, dc, rng, cand_of);
+                if (lane == 0) {
+                    s_flag = r;
+                    s_j = st.j;
+                }
+            }
+            __syncthreads();
+            const int need = s_flag, j = s_j;
+            if (!need) break;
+            const int64_t nwords = (d + 31) >> 5;
+            for (int64_t w = threadIdx.x; w < nwords; w += blockDim.x) zb[w] = 0u;
+            __syncthreads();
+            if (warp == 0 && lane < j) atomicOr(&zb[st.sel >> 5], 1u << (st.sel & 31));
+            __syncthreads();
+            T = cta_canon_prefix(wfn, d, P, tsum, gcar, zb);
+            if (warp == 0) {
+                if (!(T > 0.f)) {
+                    zero = true;
+                } else {
+                    if (lane == j) {
+                        st.cand = cand_of(rng.word(dc, lane, st.A));
+                        st.A++;
+                    } else if (lane > j && lane < N) {
+                        st.cand = cand_of(rng.word(dc, lane, 0));
+                    }
+                    st.a = 1;
+                }
+            }
+        }
+        if (warp == 0) {
+            bool act = lane < N;
+            int32_t dst = 0;
+            if (act) {
+                dst = Update(&g.v, __ldg(g.v.col + beg + st.sel), v);
+                if (dst < 0 || dst >= g.v.n_vertices) {
+                    atomicOr(a.err, ERR_UPDATE_RANGE);
+                    dst = 0;
+                }
+            }
+            unsigned long long ob = 0;
+            uint32_t q = 0;
+            if (lane == 0) {
+                ob = atomicAdd(a.o_count, (unsigned long long)N);
+                if (a.push) q = atomicAdd(a.n_out, (uint32_t)N);
+            }
+            ob = __shfl_sync(FULL, ob, 0);
+            q = __shfl_sync(FULL, q, 0);
+            if (act) {
+                int64_t pos = (int64_t)ob + lane;
+                if (pos < a.cap) {
+                    a.o_src[pos] = v;
+                    a.o_dst[pos] = dst;
+                    if (a.o_smp) a.o_smp[pos] = s;
+                    if (a.o_dep) a.o_dep[pos] = a.depth;
+                }
+                if (a.push) {
+                    a.out_v[q + lane] = dst;
+                    a.out_s[q + lane] = s;
+                    a.out_p[q + lane] = p * (uint32_t)N + (uint32_t)lane;
+                }
+            }
+        }
+        my_items++;
+        my_bytes += expansion_bytes<I, BIAS>(g, d, N, true, a);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        atomicAdd(&a.bytes[1], my_bytes);
+        atomicAdd(&a.items[1], my_items);
+    }
+}
+
+// ------------------------------------------------------------ walks
+// Unbiased walks: one thread per walk (a step is a rowptr pair, one Philox
+// word and one col read).  Equivalent to neighbor sampling with N = 1.
+template <typename I>
+__global__ void __launch_bounds__(WALK_THREADS)
+k_walk_thread(DevGraph g, WalkArgs a) {
+    __shared__ int32_t s_out[(WALK_THREADS / 32) * 4 * STAGE];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    WarpStage stg;
+    stg.s_src = s_out + wib * 4 * STAGE;
+    stg.s_dst = stg.s_src + STAGE;
+    stg.s_smp = stg.s_dst + STAGE;
+    stg.s_dep = stg.s_smp + STAGE;
+    const OutArgs oa{a.o_src, a.o_dst, a.o_smp, a.o_dep, a.o_count, a.cap};
+    const int stride = gridDim.x * blockDim.x;
+    unsigned long long steps = 0;
+    for (int base = blockIdx.x * blockDim.x; base < a.n; base += stride) {
+        const int w = base + threadIdx.x;
+        bool alive = w < a.n;
+        int32_t v = 0;
+        if (alive) {
+            v = a.seeds[w];
+            if (v < 0 || v >= g.v.n_vertices) {
+                atomicOr(a.err, ERR_SEED_RANGE);
+                alive = false;
+            }
+        }
+        for (int t = 0; t < a.len; ++t) {
+            if (!__any_sync(FULL, alive)) break;
+            bool act = false;
+            int32_t dst = 0;
+            if (alive) {
+                const int64_t beg = row_begin<I>(g, v), d = row_begin<I>(g, v + 1) - beg;
+                if (d <= 0) {
+                    alive = false;
+                } else {
+                    uint32_t idx = 0;
+                    if (d > 1) {
+                        uint4 b = philox(make_uint4(0u, (uint32_t)w, (TAG_SAMPLE << 24) | (uint32_t)t, 0u),
+                                         a.k0, a.k1);
+                        idx = mulhi(b.x, (uint32_t)d);
+                    }
+                    dst = Update(&g.v, __ldg(g.v.col + beg + idx), v);
+                    if (dst < 0 || dst >= g.v.n_vertices) {
+                        atomicOr(a.err, ERR_UPDATE_RANGE);
+                        dst = 0;
+                    }
+                    act = true;
+                    ++steps;
+                }
+            }
+            stg.push(oa, act, v, dst, w, t, lane);
+            if (act) v = dst;
+        }
+    }
+    stg.flush(oa, lane);
+    unsigned long long tot = steps;
+    for (int off = 16; off; off >>= 1) tot += __shfl_xor_sync(FULL, tot, off);
+    if (lane == 0) {
+        unsigned long long per = 2 * sizeof(I) + 4 + 4ull * (2 + (a.o_smp != nullptr) + (a.o_dep != nullptr));
+        atomicAdd(&a.bytes[2], tot * per);
+        atomicAdd(&a.items[2], tot);
+    }
+}
+
+// Biased walks: one warp per walk; per step the warp builds the canonical
+// prefix of the neighbor biases (shared memory up to WBUF, else per-warp
+// global scratch) unless a CDF cache for this bias exists.
+template <typename I, int BIAS>
+__global__ void __launch_bounds__(WALK_THREADS)
+k_walk_warp(DevGraph g, WalkArgs a) {
+    constexpr int NW = WALK_THREADS / 32;
+    __shared__ float s_P[NW * WBUF];
+    __shared__ int32_t s_out[NW * 4 * STAGE];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    float *P = s_P + wib * WBUF;
+    WarpStage stg;
+    stg.s_src = s_out + wib * 4 * STAGE;
+    stg.s_dst = stg.s_src + STAGE;
+    stg.s_smp = stg.s_dst + STAGE;
+    stg.s_dep = stg.s_smp + STAGE;
+    const OutArgs oa{a.o_src, a.o_dst, a.o_smp, a.o_dep, a.o_count, a.cap};
+    const bool cached = g.cdf && g.cdf_bias == BIAS;
+    unsigned long long steps = 0, bytes = 0;
+    const unsigned long long obytes = 4ull * (2 + (a.o_smp != nullptr) + (a.o_dep != nullptr));
+    for (int w = gw; w < a.n; w += nw) {
+        int32_t v = a.seeds[w];
+        if (v < 0 || v >= g.v.n_vertices) {
+            if (lane == 0) atomicOr(a.err, ERR_SEED_RANGE);
+            continue;
+        }
+        for (int t = 0; t < a.len; ++t) {
+            const int64_t beg = row_begin<I>(g, v), d = row_begin<I>(g, v + 1) - beg;
+            if (d <= 0) break;
+            int64_t idx = 0;
+            bytes += 2 * sizeof(I) + 4 + obytes;
+            if (d > 1) {
+                const float *PP;
+                float T;
+                if (cached) {
+                    PP = g.cdf + beg;
+                    T = PP[d - 1];
+                    bytes += 4ull * (64 - __clzll((unsigned long long)d));
+                } else {
+                    float *buf = P;
+                    if (d > WBUF) {
+                        if (d > a.scratch_stride) {
+                            if (lane == 0) atomicOr(a.err, ERR_SCRATCH);
+                            break;
+                        }
+                        buf = a.scratch + (int64_t)gw * a.scratch_stride;
+                    }
+                    auto wfn = [&](int64_t i) { return edge_bias<I, BIAS>(g, beg + i); };
+                    T = warp_canon_prefix(wfn, d, buf, nullptr, lane);
+                    PP = buf;
+                    bytes += (BIAS == CSAW_BIAS_EDGE_WEIGHT || (BIAS == CSAW_BIAS_DEGREE && g.ebias))
+                                 ? 4ull * d
+                                 : (4ull + 2ull * sizeof(I)) * d;
+                }
+                if (T > 0.f) {
+                    uint4 b = philox(make_uint4(0u, (uint32_t)w, (TAG_SAMPLE << 24) | (uint32_t)t, 0u),
+                                     a.k0, a.k1);
+                    idx = search_upper(PP, d, its_target(b.x, T));
+                }
+            }
+            int32_t dst = Update(&g.v, __ldg(g.v.col + beg + idx), v);
+            if (dst < 0 || dst >= g.v.n_vertices) {
+                if (lane == 0) atomicOr(a.err, ERR_UPDATE_RANGE);
+                dst = 0;
+            }
+            stg.push(oa, lane == 0, v, dst, w, t, lane);
+            v = dst;
+            ++steps;
+        }
+    }
+    stg.flush(oa, lane);
+    if (lane == 0) {
+        atomicAdd(&a.bytes[2], bytes);
+        atomicAdd(&a.items[2], steps);
+    }
+}
+
+// ------------------------------------------------------------- MDRW
+// One warp per sample; frontier and its bias prefix in dynamic shared memory
+// (F ints + F floats per warp).
+template <typename I, int BIAS>
+__global__ void k_mdrw(DevGraph g, WalkArgs a) {
+    extern __shared__ int32_t s_dyn[];
+    __shared__ int32_t s_out[(WALK_THREADS / 32) * 4 * STAGE];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    const int F = a.F;
+    int32_t *f = s_dyn + (int64_t)wib * 2 * F;
+    float *P = (float *)(f + F);
+    WarpStage stg;
+    stg.s_src = s_out + wib * 4 * STAGE;
+    stg.s_dst = stg.s_src + STAGE;
+    stg.s_smp = stg.s_dst + STAGE;
+    stg.s_dep = stg.s_smp + STAGE;
+    const OutArgs oa{a.o_src, a.o_dst, a.o_smp, a.o_dep, a.o_count, a.cap};
+    unsigned long long steps = 0, bytes = 0;
+    const unsigned long long obytes = 4ull * (2 + (a.o_smp != nullptr) + (a.o_dep != nullptr));
+    for (int s = gw; s < a.n; s += nw) {
+        for (int i = lane; i < F; i += 32) {
+            int32_t v = a.seeds[(int64_t)s * F + i];
+            if (v < 0 || v >= g.v.n_vertices) {
+                atomicOr(a.err, ERR_SEED_RANGE);
+                v = 0;
+            }
+            f[i] = v;
+        }
+        __syncwarp();
+        for (int t = 0; t < a.len; ++t) {
+            uint4 b = philox(make_uint4(0u, (uint32_t)s, (TAG_MDRW << 24) | (uint32_t)t, 0u), a.k0, a.k1);
+            int slot = 0;
+            if (F > 1) {
+                auto wfn = [&](int64_t i) -> float {
+                    if constexpr (BIAS == CSAW_BIAS_UNBIASED) return 1.f;
+                    else if constexpr (BIAS == CSAW_BIAS_DEGREE) return degree_f<I>(g, f[i]);
+                    else return VertexBias(f[i], &g.v);
+                };
+                float T = warp_canon_prefix(wfn, F, P, nullptr, lane);
+                if (T > 0.f) slot = (int)search_upper(P, F, its_target(b.x, T));
+                bytes += BIAS == CSAW_BIAS_UNBIASED ? 0 : 2ull * sizeof(I) * F;
+            }
+            const int32_t v = f[slot];
+            const int64_t beg = row_begin<I>(g, v), d = row_begin<I>(g, v + 1) - beg;
+            bytes += 2 * sizeof(I);
+            if (d > 0) {
+                int32_t dst = Update(&g.v, __ldg(g.v.col + beg + mulhi(b.y, (uint32_t)d)), v);
+                if (dst < 0 || dst >= g.v.n_vertices) {
+                    if (lane == 0) atomicOr(a.err, ERR_UPDATE_RANGE);
+                    dst = 0;
+                }
+                stg.push(oa, lane == 0, v, dst, s, t, lane);
+                bytes += 4 + obytes;
+                ++steps;
+                __syncwarp();
+                if (lane == 0) f[slot] = dst;
+            }
+            __syncwarp();
+        }
+    }
+    stg.flush(oa, lane);
+    if (lane == 0) {
+        atomicAdd(&a.bytes[3], bytes);
+        atomicAdd(&a.items[3], steps);
+    }
+}
+
+// -------------------------------------------------------------- utilities
+__global__ void k_make_seeds(const int32_t *nonisolated, uint32_t n_non, int64_t n, uint32_t k0,
+                             uint32_t k1, int32_t *out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        uint4 b = philox(make_uint4((uint32_t)i, (uint32_t)(i >> 32), TAG_SEED << 24, 0u), k0, k1);
+        out[i] = nonisolated[mulhi(b.x, n_non)];
+    }
+}
+
+template <typename I>
+__global__ void k_edge_degree(DevGraph g, float *ebias) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < g.v.n_edges;
+         e += (int64_t)gridDim.x * blockDim.x)
+        ebias[e] = degree_f<I>(g, __ldg(g.v.col + e));
+}
+
+}  // namespace csaw

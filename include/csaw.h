@@ -1,0 +1,159 @@
+/*
+ * csaw.h -- C ABI of the csaw-b200 graph sampling / random-walk engine.
+ *
+ * Drop-in boundary for C-SAW's sampler.  C-SAW's own boundary is
+ *   - the compile-time operator plugin api.cuh (non-stream/api.cuh:4-27):
+ *     VertexBias / EdgeBias / Update, kept in include/csaw_api.cuh, and
+ *   - the host entry Sampler(beg, csr, n_blocks, n_threads, n_subgraph,
+ *     FrontierSize, NeighborSize, Depth, args, rank) (non-stream/sampler.cuh:3-8,
+ *     non-stream/main.cu:196-308), kept as csaw_sampler_compat() below,
+ * plus its CSR input (graph.hpp:9-111: int64 beg_pos/adj files) and its Si
+ * edge-list output (sample_class.cuh:76-90).
+ *
+ * Everything here is plain C: opaque handles, plain pointers and sizes, int
+ * status codes (no exit(), unlike HRR/H_ERR in herror.h:1-10 and util.h:4-14).
+ * "stream" arguments are cudaStream_t passed as void* (NULL = legacy default
+ * stream).  Device pointers are marked "device"; everything else is host.
+ * One handle per host thread; calls on one handle are not thread-safe.
+ */
+#ifndef CSAW_H
+#define CSAW_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------- status */
+enum {
+    CSAW_OK = 0,
+    CSAW_ERR_INVALID = 1,   /* bad argument (see csaw_last_error) */
+    CSAW_ERR_CUDA = 2,      /* a CUDA runtime call failed */
+    CSAW_ERR_CAPACITY = 3,  /* output capacity too small; *n_out = needed */
+    CSAW_ERR_NOMEM = 4,     /* device allocation failed */
+    CSAW_ERR_DEVICE = 5     /* a kernel reported an error flag */
+};
+
+/* ------------------------------------------------------------- modes */
+enum {
+    CSAW_MODE_NEIGHBOR = 0, /* neighbor sampling, check (main.cu:21-93) */
+    CSAW_MODE_WALK = 1,     /* random walk (README.md:30: NeighborSize 1) */
+    CSAW_MODE_MDRW = 2      /* multi-dimensional RW, check_layer (main.cu:95-194) */
+};
+
+enum {
+    CSAW_BIAS_UNBIASED = 0,    /* every neighbor equally likely */
+    CSAW_BIAS_DEGREE = 1,      /* bias = out-degree of the neighbor (api.cuh:14-20) */
+    CSAW_BIAS_EDGE_WEIGHT = 2, /* bias = weight of the edge */
+    CSAW_BIAS_HOOK = 3         /* bias = EdgeBias()/VertexBias() of csaw_api.cuh */
+};
+
+enum {
+    CSAW_SCHED_PLAIN = 0,    /* one launch per level, degree-threshold rule */
+    CSAW_SCHED_BATCHED = 1,  /* persistent work-queue kernel */
+    CSAW_SCHED_LEARNED = 2   /* batched + learned granularity */
+};
+
+#define CSAW_MAX_DEPTH 64
+
+typedef struct {
+    int32_t mode;           /* CSAW_MODE_* */
+    int32_t bias;           /* CSAW_BIAS_* */
+    int32_t schedule;       /* CSAW_SCHED_* (never changes the output) */
+    int32_t n_samples;      /* #samples (n_subgraph) or #walks */
+    int32_t frontier_size;  /* FrontierSize: seeds per sample (walk: 1) */
+    int32_t neighbor_size;  /* NeighborSize: used for hops whose fanout is 0 */
+    int32_t depth;          /* Depth (hops), walk length, or MDRW steps */
+    int32_t fanout[CSAW_MAX_DEPTH]; /* per-hop NeighborSize (0 = neighbor_size) */
+    uint64_t seed;          /* Philox key: the whole output is a function of it */
+} csaw_params;
+
+typedef struct csaw_graph_s *csaw_graph;
+
+/* graph creation flags */
+enum {
+    CSAW_GRAPH_DEGREE_BIAS = 1, /* materialise per-edge neighbor degree (4E B) */
+    CSAW_GRAPH_CDF_CACHE = 2    /* precompute per-vertex bias prefix (4E B) */
+};
+
+typedef struct {
+    int64_t n_vertices, n_edges, max_degree;
+    int64_t device_bytes;     /* graph residency bytes */
+    int64_t workspace_bytes;  /* scratch currently held */
+    int64_t kernel_launches;  /* launches since creation */
+    int64_t last_edges;       /* edges emitted by the last run */
+    int64_t last_items;       /* vertex expansions (or walk steps) of the last run */
+    int64_t last_bytes;       /* algorithmic bytes of the last run */
+} csaw_stats;
+
+/* Last error message of this thread (never NULL). */
+const char *csaw_last_error(void);
+/* Library version string. */
+const char *csaw_version(void);
+
+/*
+ * CSR residency (replaces gpu_graph, non-stream/gpu_graph.cuh:25-66, which
+ * built a misindexed per-edge degree list and never loaded weights).
+ * rowptr: n_vertices+1 entries, int32 or int64 (rowptr_is_64); col: n_edges
+ * int32 in [0, n_vertices); weights: n_edges float >= 0, or NULL.
+ * csaw_graph_create copies host arrays to the current device.
+ */
+int csaw_graph_create(const void *rowptr, int rowptr_is_64, const int32_t *col,
+                      const float *weights, int64_t n_vertices, int64_t n_edges,
+                      int flags, csaw_graph *out);
+int csaw_graph_destroy(csaw_graph g);
+int csaw_graph_stats(csaw_graph g, csaw_stats *out);
+
+/*
+ * Per-kernel timing (replaces the clock() stamps accumulated into
+ * wvar->total_counter, functions.cuh:342-396).  With profiling on, every
+ * launch is bracketed by CUDA events on its stream; csaw_graph_kernel_stats
+ * returns, per kernel kind, the summed device time, launches, algorithmic
+ * bytes and work items since profiling was (re)enabled.
+ * Kinds: 0 level expansion, 1 high-degree expansion, 2 walk, 3 MDRW,
+ * 4 queue/seed setup.
+ */
+int csaw_graph_profile(csaw_graph g, int enable);
+int csaw_graph_kernel_stats(csaw_graph g, int kind, double *ms, int64_t *launches,
+                            int64_t *bytes, int64_t *items);
+
+/* Seeds uniform over non-isolated vertices (Philox keyed by seed).
+ * out: device, n entries. */
+int csaw_make_seeds(csaw_graph g, int64_t n, uint64_t seed, int32_t *out, void *stream);
+
+/*
+ * Run one sampling job (all three modes).  seeds: device, n_samples *
+ * frontier_size vertex ids (walk: n_samples).  Outputs: device arrays of
+ * `capacity` entries; out_sample and out_depth may be NULL.  Edge (src, dst)
+ * of sample s at hop/step l.  Order within the output is unspecified; the
+ * multiset is a pure function of (graph, params, seeds).  Synchronises
+ * `stream` and stores the edge count in *n_out.
+ */
+int csaw_sample(csaw_graph g, const csaw_params *p, const int32_t *seeds,
+                int32_t *out_src, int32_t *out_dst, int32_t *out_sample,
+                int32_t *out_depth, int64_t capacity, int64_t *n_out, void *stream);
+
+/* Same, with HOST seeds and HOST outputs (copies inside the call). */
+int csaw_sample_host(csaw_graph g, const csaw_params *p, const int32_t *seeds,
+                     int32_t *out_src, int32_t *out_dst, int32_t *out_sample,
+                     int32_t *out_depth, int64_t capacity, int64_t *n_out, void *stream);
+
+/*
+ * Reference-compatible entry (Sampler, non-stream/main.cu:196-308): loads
+ * int64 beg.bin / csr.bin (graph.hpp:18-34 format), draws FrontierSize seeds
+ * per sample, runs neighbor sampling (FrontierSize == 1) or MDRW
+ * (FrontierSize > 1) exactly as the reference dispatches (main.cu:281-288),
+ * and returns the number of sampled edges and the sampling time in seconds.
+ * n_blocks and n_threads are accepted and ignored (the engine sizes its own
+ * grids).  The edge list stays inside the call, as in the reference.
+ */
+int csaw_sampler_compat(const char *beg_file, const char *csr_file, int n_blocks,
+                        int n_threads, int n_subgraph, int frontier_size,
+                        int neighbor_size, int depth, int *sampled_edges,
+                        double *seconds);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

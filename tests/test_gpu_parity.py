@@ -1,0 +1,169 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle,
+bit-exact on the multiset of (sample, depth, src, dst) after a canonical sort."""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import sort_edges
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def csaw():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("gpu test without a CUDA device")
+    import csaw as c
+    c.lib()
+    return c
+
+
+def gpu_run(csaw, csr, mode, bias, n, F, depth, fanout, seed, seeds, degree_bias=False, graph=None):
+    import torch
+    g = graph or csaw.Graph(csr, degree_bias=degree_bias)
+    p = csaw.make_params(mode, bias, n, F, (fanout or [1])[0], depth, fanout, seed)
+    out = g.sample(p, torch.from_numpy(np.ascontiguousarray(seeds, dtype=np.int32)).cuda())
+    return [x.cpu().numpy() for x in out]
+
+
+def oracle_run(csr, mode, bias, n, F, depth, fanout, seed, seeds):
+    return oracle.run(csr.rowptr, csr.col, csr.weight, seeds, mode, bias, n, F, depth, fanout, seed=seed,
+                      n_threads=8)
+
+
+def assert_parity(a, b):
+    sa, sb = sort_edges(*a), sort_edges(*b)
+    assert sa.shape == sb.shape, (sa.shape, sb.shape)
+    assert np.array_equal(sa, sb)
+
+
+def test_rmat16_unbiased_small_config(csaw, rmat16):
+    """R-MAT scale 16 ef 8, unbiased, 1000 samples, F 1, N 2, D 2, Philox seed 0."""
+    g = rmat16
+    seeds = oracle.make_seeds(g.rowptr, 1000, 0)
+    a = gpu_run(csaw, g, 0, 0, 1000, 1, 2, [2, 2], 0, seeds)
+    b = oracle_run(g, 0, 0, 1000, 1, 2, [2, 2], 0, seeds)
+    assert len(a[0]) > 0
+    assert_parity(a, b)
+
+
+@pytest.mark.parametrize("bias", [0, 1, 2])
+@pytest.mark.parametrize("fan", [[20, 20, 20], [3, 7], [1, 1, 1, 1], [32, 2]])
+def test_powerlaw_neighbor_parity(csaw, powerlaw_small, bias, fan):
+    g = powerlaw_small
+    n, F = 150, 4
+    seeds = oracle.make_seeds(g.rowptr, n * F, 17)
+    a = gpu_run(csaw, g, 0, bias, n, F, len(fan), fan, 0x1234, seeds)
+    b = oracle_run(g, 0, bias, n, F, len(fan), fan, 0x1234, seeds)
+    assert_parity(a, b)
+
+
+@pytest.mark.parametrize("bias", [0, 1, 2])
+def test_rmat_pareto_heavy_vertices(csaw, rmat12_pareto, bias):
+    """Hub vertices above 1024 neighbors take the CTA path for biased kinds."""
+    g = rmat12_pareto
+    deg = np.diff(g.rowptr)
+    assert deg.max() > 1024
+    hubs = np.argsort(deg)[-8:].astype(np.int32)
+    seeds = np.concatenate([hubs, oracle.make_seeds(g.rowptr, 192, 2)]).astype(np.int32)
+    a = gpu_run(csaw, g, 0, bias, 200, 1, 2, [25, 10], 77, seeds)
+    b = oracle_run(g, 0, bias, 200, 1, 2, [25, 10], 77, seeds)
+    assert_parity(a, b)
+
+
+@pytest.mark.parametrize("bias", [0, 1, 2])
+def test_walk_parity(csaw, powerlaw_small, bias):
+    g = powerlaw_small
+    seeds = oracle.make_seeds(g.rowptr, 500, 5)
+    a = gpu_run(csaw, g, 1, bias, 500, 1, 64, None, 9, seeds)
+    b = oracle_run(g, 1, bias, 500, 1, 64, None, 9, seeds)
+    assert_parity(a, b)
+
+
+@pytest.mark.parametrize("bias", [0, 1, 2])
+def test_walk_parity_hubs(csaw, rmat12_pareto, bias):
+    g = rmat12_pareto
+    seeds = oracle.make_seeds(g.rowptr, 300, 6)
+    a = gpu_run(csaw, g, 1, bias, 300, 1, 40, None, 10, seeds)
+    b = oracle_run(g, 1, bias, 300, 1, 40, None, 10, seeds)
+    assert_parity(a, b)
+
+
+@pytest.mark.parametrize("bias,F", [(0, 4), (1, 4), (1, 33), (1, 1)])
+def test_mdrw_parity(csaw, powerlaw_small, bias, F):
+    g = powerlaw_small
+    seeds = oracle.make_seeds(g.rowptr, 100 * F, 8)
+    a = gpu_run(csaw, g, 2, bias, 100, F, 50, None, 11, seeds)
+    b = oracle_run(g, 2, bias, 100, F, 50, None, 11, seeds)
+    assert_parity(a, b)
+
+
+def test_hook_bias_equals_degree_bias(csaw, powerlaw_small):
+    g = powerlaw_small
+    seeds = oracle.make_seeds(g.rowptr, 400, 3)
+    a = gpu_run(csaw, g, 0, 3, 100, 4, 3, [10, 5, 3], 5, seeds)
+    b = gpu_run(csaw, g, 0, 1, 100, 4, 3, [10, 5, 3], 5, seeds)
+    assert_parity(a, b)
+
+
+def test_materialised_degree_bias_same_output(csaw, powerlaw_small):
+    g = powerlaw_small
+    seeds = oracle.make_seeds(g.rowptr, 400, 4)
+    a = gpu_run(csaw, g, 0, 1, 100, 4, 3, [20, 20, 20], 6, seeds, degree_bias=True)
+    b = gpu_run(csaw, g, 0, 1, 100, 4, 3, [20, 20, 20], 6, seeds, degree_bias=False)
+    assert_parity(a, b)
+
+
+def test_make_seeds_matches_oracle(csaw, rmat16):
+    g = csaw.Graph(rmat16)
+    s = g.make_seeds(5000, 123).cpu().numpy()
+    assert np.array_equal(s, oracle.make_seeds(rmat16.rowptr, 5000, 123))
+
+
+def test_host_buffers_equal_device_buffers(csaw, powerlaw_small):
+    g = csaw.Graph(powerlaw_small)
+    seeds = oracle.make_seeds(powerlaw_small.rowptr, 200, 1)
+    p = csaw.make_params(0, 1, 50, 4, 20, 3, [20, 20, 20], 3)
+    h = g.sample_host(p, seeds)
+    d = gpu_run(csaw, powerlaw_small, 0, 1, 50, 4, 3, [20, 20, 20], 3, seeds, graph=g)
+    assert_parity(h, d)
+
+
+def test_capacity_error_reports_needed(csaw, powerlaw_small):
+    g = csaw.Graph(powerlaw_small)
+    seeds = oracle.make_seeds(powerlaw_small.rowptr, 40, 1)
+    import torch
+    p = csaw.make_params(0, 0, 10, 4, 5, 2, [5, 5], 3)
+    full = g.sample(p, torch.from_numpy(seeds).cuda())
+    with pytest.raises(csaw.CsawError) as ei:
+        g.sample(p, torch.from_numpy(seeds).cuda(), capacity=3)
+    assert ei.value.code == 3
+    assert len(full[0]) > 3
+
+
+def test_bad_seed_is_rejected(csaw, powerlaw_small):
+    import torch
+    g = csaw.Graph(powerlaw_small)
+    p = csaw.make_params(0, 0, 2, 1, 5, 2, [5, 5], 3)
+    with pytest.raises(csaw.CsawError) as ei:
+        g.sample(p, torch.tensor([0, powerlaw_small.n_vertices + 5], dtype=torch.int32).cuda())
+    assert ei.value.code == 1
+
+
+def test_reference_compatible_sampler(csaw, powerlaw_small, tmp_path):
+    from csaw import graphgen
+    beg, csr = tmp_path / "beg.bin", tmp_path / "csr.bin"
+    graphgen.write_reference_format(powerlaw_small, beg, csr)
+    r = csaw.Sampler(beg, csr, 400, 128, 100, 1, 5, 3)
+    assert r.sampled_edges > 0 and r.time > 0
+    r2 = csaw.Sampler(beg, csr, 400, 128, 50, 4, 1, 30)   # FrontierSize > 1: MDRW
+    assert 0 < r2.sampled_edges <= 50 * 30
+
+
+def test_repeat_runs_identical(csaw, rmat12_pareto):
+    g = rmat12_pareto
+    seeds = oracle.make_seeds(g.rowptr, 300, 2)
+    a = gpu_run(csaw, g, 0, 2, 300, 1, 3, [10, 5, 2], 4, seeds)
+    b = gpu_run(csaw, g, 0, 2, 300, 1, 3, [10, 5, 2], 4, seeds)
+    assert_parity(a, b)
