@@ -8,8 +8,13 @@ law exponent 2.1 capped at 460, int32 CSR, lognormal(0,1) weights -- run with
   (b) degree-biased random walks: 4000 walks of length 64.
 value = (edges of a + edges of b) / device time of the step.  Inputs are
 resident in HBM; between timed steps a 256 MiB buffer is written to flush L2.
-e2e = the same metric through csaw_sample_host: host seeds in, host edge list
-(src, dst, sample) out, copies inside the timed region.
+e2e = the same metric through the host-buffer entry points (csaw_sample_host
+for the plain form, csaw_sample_batch with host buffers for the batched form):
+host seeds in, host edge list (src, dst, sample) out, copies inside the timed
+region.
+Both forms run: "plain" (one warp per item, level by level, gathered degree
+bias) and "batched" (the default product path); value is the batched form,
+forms.plain the plain one, on the same graph, seeds and keys.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl csaw|reference]
 
@@ -163,7 +168,7 @@ def cpu_baseline(g):
         eb = oracle.run(g.rowptr, g.col, g.weight, sb, 1, 1, nb, 1, 64, seed=SEED_B, n_threads=threads)
         edges += len(ea[0]) + len(eb[0])
         reps += 1
-        if time.perf_counter() - t0 > 10.0 or reps >= 200:
+        if time.perf_counter() - t0 > 10.0:
             break
     dt = time.perf_counter() - t0
     return {"value": edges / dt, "unit": "edges/s", "cores": threads, "kind": "port",
@@ -177,6 +182,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="csaw", choices=["csaw", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--forms", default="plain,batched",
+                    help="forms to time; the last one is reported as value (profiling runs use one form)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -194,50 +201,70 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     g = build_graph()
-    G = csaw.Graph(g)                       # plain residency (gathered degrees)
+    G = csaw.Graph(g)                       # one resident CSR for both forms
     stream = torch.cuda.current_stream()
-    pa = csaw.make_params(**WORK_A, seed=SEED_A + 7919 * rank)
-    pb = csaw.make_params(**WORK_B, seed=SEED_B + 7919 * rank)
     seeds_a = G.make_seeds(4000 * 4, SEED_A + 7919 * rank)
     seeds_b = G.make_seeds(4000, SEED_B + 7919 * rank)
+    params = {f: (csaw.make_params(**WORK_A, seed=SEED_A + 7919 * rank, schedule=sch),
+                  csaw.make_params(**WORK_B, seed=SEED_B + 7919 * rank, schedule=sch))
+              for f, sch in (("plain", csaw.SCHED_PLAIN), ("batched", csaw.SCHED_BATCHED))}
+    pa, pb = params["batched"]
     cap_a, cap_b = csaw.edge_bound(pa), csaw.edge_bound(pb)
     out_a = torch.empty((3, cap_a), dtype=torch.int32, device="cuda")
     out_b = torch.empty((3, cap_b), dtype=torch.int32, device="cuda")
     flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.int32, device="cuda")
 
-    def step():
-        a = G.sample(pa, seeds_a, capacity=cap_a, out=out_a, with_depth=False)
-        b = G.sample(pb, seeds_b, capacity=cap_b, out=out_b, with_depth=False)
-        return a[0].numel() + b[0].numel()
+    batch_jobs = [csaw.BatchJob(params["batched"][0], seeds_a, cap_a, out_a, with_depth=False),
+                  csaw.BatchJob(params["batched"][1], seeds_b, cap_b, out_b, with_depth=False)]
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
+    def step(form):
+        if form == "plain":   # one job after the other, as the reference runs them
+            qa, qb = params[form]
+            a = G.sample(qa, seeds_a, capacity=cap_a, out=out_a, with_depth=False)
+            b = G.sample(qb, seeds_b, capacity=cap_b, out=out_b, with_depth=False)
+            return a[0].numel() + b[0].numel()
+        res = G.sample_batch(batch_jobs)   # both workloads as one batch
+        return res[0][0].numel() + res[1][0].numel()
 
     def barrier():
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
-    # ---- device-timed steps (L2 flushed before each)
-    G.profile(True)
-    launches0 = G.stats()["kernel_launches"]
-    clocks = Clocks(local)
-    clocks.start()
-    barrier()
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    edges = 0
-    for i in range(args.steps):
-        flush.zero_()
-        evs[i][0].record(stream)
-        edges += step()
-        evs[i][1].record(stream)
-    barrier()
-    clk = clocks.stop()
-    launches = G.stats()["kernel_launches"] - launches0
-    ms = sum(a.elapsed_time(b) for a, b in evs)
-    kstats = {k: G.kernel_stats(k) for k in ("expand", "heavy", "walk", "setup")}
-    G.profile(False)
+    def timed(form, clocks=None):
+        """K device-timed steps (L2 flushed before each); returns edges, ms, kernel stats, launches."""
+        for _ in range(args.warmup):
+            step(form)
+        G.profile(True)
+        launches0 = G.stats()["kernel_launches"]
+        if clocks:
+            clocks.start()
+        barrier()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+        edges = 0
+        for i in range(args.steps):
+            flush.zero_()
+            evs[i][0].record(stream)
+            edges += step(form)
+            evs[i][1].record(stream)
+        barrier()
+        clk = clocks.stop() if clocks else None
+        launches = G.stats()["kernel_launches"] - launches0
+        ms = sum(x.elapsed_time(y) for x, y in evs)
+        ks = {k: G.kernel_stats(k) for k in ("expand", "select", "heavy", "walk", "setup")}
+        G.profile(False)
+        return edges, ms, ks, launches, clk
+
+    forms = [f.strip() for f in args.forms.split(",") if f.strip()]
+    main_form = forms[-1]
+    plain_ms, plain_k = None, {}
+    if "plain" in forms and main_form != "plain":
+        plain_edges, plain_ms, plain_k, _, _ = timed("plain")
+    edges, ms, kstats, launches, clk = timed(main_form, Clocks(local))
+    if plain_ms is not None and edges != plain_edges:
+        raise SystemExit(f"plain and {main_form} forms emitted different edge counts: {plain_edges} vs {edges}")
+    pa, pb = params[main_form]
 
     # ---- end to end through the host-buffer entry point
     seeds_a_h = seeds_a.cpu().numpy()
@@ -246,23 +273,33 @@ def main():
     host_b = torch.empty((3, cap_b), dtype=torch.int32).pin_memory().numpy()
     sa_pin = torch.from_numpy(seeds_a_h).pin_memory().numpy()
     sb_pin = torch.from_numpy(seeds_b_h).pin_memory().numpy()
+    host_jobs = [csaw.BatchJob(pa, sa_pin, cap_a, host_a, with_depth=False, host=True),
+                 csaw.BatchJob(pb, sb_pin, cap_b, host_b, with_depth=False, host=True)]
+
+    def e2e_step():
+        if main_form == "plain":
+            ra = G.sample_host(pa, sa_pin, capacity=cap_a, out=host_a, with_depth=False, stream=stream.cuda_stream)
+            rb = G.sample_host(pb, sb_pin, capacity=cap_b, out=host_b, with_depth=False, stream=stream.cuda_stream)
+        else:
+            ra, rb = G.sample_batch(host_jobs, stream=stream.cuda_stream)
+        return ra[0].size + rb[0].size
+
     e2e_steps = max(3, args.steps // 2)
-    G.sample_host(pa, sa_pin, capacity=cap_a, out=host_a, with_depth=False)
+    e2e_step()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     e2e_edges = 0
     for _ in range(e2e_steps):
-        ra = G.sample_host(pa, sa_pin, capacity=cap_a, out=host_a, with_depth=False, stream=stream.cuda_stream)
-        rb = G.sample_host(pb, sb_pin, capacity=cap_b, out=host_b, with_depth=False, stream=stream.cuda_stream)
-        e2e_edges += ra[0].size + rb[0].size
+        e2e_edges += e2e_step()
     e1.record(stream)
     barrier()
     e2e_ms = e0.elapsed_time(e1)
 
     # ---- max over ranks
     t_s = ms / 1e3
-    tot = torch.tensor([float(edges), t_s, float(e2e_edges), e2e_ms / 1e3], dtype=torch.float64, device="cuda")
+    tot = torch.tensor([float(edges), t_s, float(e2e_edges), e2e_ms / 1e3, (plain_ms or 0.0) / 1e3],
+                       dtype=torch.float64, device="cuda")
     if world > 1:
         import torch.distributed as dist
         s = tot.clone()
@@ -270,9 +307,9 @@ def main():
         dist.all_reduce(s[2:3])
         m = tot.clone()
         dist.all_reduce(m[1:2], op=dist.ReduceOp.MAX)
-        dist.all_reduce(m[3:4], op=dist.ReduceOp.MAX)
-        tot = torch.stack([s[0], m[1], s[2], m[3]])
-    all_edges, t_max, e2e_all, e2e_t = (float(x) for x in tot.cpu())
+        dist.all_reduce(m[3:5], op=dist.ReduceOp.MAX)
+        tot = torch.stack([s[0], m[1], s[2], m[3], m[4]])
+    all_edges, t_max, e2e_all, e2e_t, plain_t = (float(x) for x in tot.cpu())
     value = all_edges / t_max
     e2e_value = e2e_all / e2e_t
 
@@ -296,6 +333,9 @@ def main():
                         "d2h_bytes_per_step": int(12 * e2e_edges / e2e_steps)},
                 "gpu_launches": int(launches), "clocks": clk, "roofline": roofline,
                 "kernels": {k: v for k, v in kstats.items() if v["launches"]},
+                "forms": {main_form: value, "plain": all_edges / plain_t if plain_t else None,
+                          "speedup_vs_plain": plain_t / t_max if plain_t else None,
+                          "plain_kernels": {k: v for k, v in plain_k.items() if v["launches"]}},
                 "edges_per_step": all_edges / args.steps / world}
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(g)

@@ -15,13 +15,13 @@ BIAS_UNBIASED, BIAS_DEGREE, BIAS_EDGE_WEIGHT, BIAS_HOOK = 0, 1, 2, 3
 SCHED_PLAIN, SCHED_BATCHED, SCHED_LEARNED = 0, 1, 2
 GRAPH_DEGREE_BIAS, GRAPH_CDF_CACHE = 1, 2
 MAX_DEPTH = 64
-KERNEL_KINDS = {"expand": 0, "heavy": 1, "walk": 2, "mdrw": 3, "setup": 4}
+KERNEL_KINDS = {"expand": 0, "heavy": 1, "walk": 2, "mdrw": 3, "setup": 4, "select": 5}
 
 # Every symbol include/csaw.h declares (tests check the library exports them).
 EXPORTS = [
     "csaw_last_error", "csaw_version", "csaw_graph_create", "csaw_graph_destroy",
     "csaw_graph_stats", "csaw_graph_profile", "csaw_graph_kernel_stats", "csaw_make_seeds",
-    "csaw_sample", "csaw_sample_host", "csaw_sampler_compat",
+    "csaw_sample", "csaw_sample_host", "csaw_sample_batch", "csaw_sampler_compat",
 ]
 
 
@@ -42,6 +42,21 @@ class Params(ctypes.Structure):
         ("depth", ctypes.c_int32),
         ("fanout", ctypes.c_int32 * MAX_DEPTH),
         ("seed", ctypes.c_uint64),
+    ]
+
+
+class Job(ctypes.Structure):
+    _fields_ = [
+        ("params", ctypes.POINTER(Params)),
+        ("seeds", ctypes.c_void_p),
+        ("out_src", ctypes.c_void_p),
+        ("out_dst", ctypes.c_void_p),
+        ("out_sample", ctypes.c_void_p),
+        ("out_depth", ctypes.c_void_p),
+        ("capacity", ctypes.c_int64),
+        ("n_out", ctypes.c_int64),
+        ("status", ctypes.c_int32),
+        ("host_buffers", ctypes.c_int32),
     ]
 
 
@@ -75,6 +90,7 @@ def lib():
     sig = [p, ctypes.POINTER(Params), p, p, p, p, p, i64, P64, p]
     L.csaw_sample.argtypes = sig
     L.csaw_sample_host.argtypes = sig
+    L.csaw_sample_batch.argtypes = [p, ctypes.POINTER(Job), i32, p]
     L.csaw_sampler_compat.argtypes = [ctypes.c_char_p, ctypes.c_char_p, i32, i32, i32, i32, i32, i32,
                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
     for name in EXPORTS:

@@ -129,6 +129,18 @@ class Graph:
         res.append(out[2 + with_sample, :k] if with_depth else None)
         return tuple(res)
 
+    def sample_batch(self, jobs, stream=None):
+        """Run several BatchJobs together (csaw_sample_batch); returns their edge lists."""
+        arr = (_lib.Job * len(jobs))()
+        for j, bj in zip(arr, jobs):
+            bj.fill(j)
+        if stream is None and not all(b.host for b in jobs):
+            stream = _torch().cuda.current_stream().cuda_stream
+        check(lib().csaw_sample_batch(self.h, arr, len(jobs), ctypes.c_void_p(stream) if stream else None))
+        for j, bj in zip(arr, jobs):
+            bj.n = j.n_out
+        return [bj.result() for bj in jobs]
+
     def sample_host(self, params, seeds, capacity=None, with_sample=True, with_depth=True, out=None,
                     stream=None):
         """Host seeds in, host edge list out (copies inside the call)."""
@@ -146,6 +158,47 @@ class Graph:
         k = n.value
         return (out[0, :k], out[1, :k], out[2, :k] if with_sample else None,
                 out[2 + with_sample, :k] if with_depth else None)
+
+
+class BatchJob:
+    """One job of Graph.sample_batch: params, seeds and output buffers (device
+    tensors, or numpy arrays with host=True)."""
+
+    def __init__(self, params, seeds, capacity=None, out=None, with_sample=True, with_depth=True, host=False):
+        self.params = params
+        self.capacity = edge_bound(params) if capacity is None else capacity
+        self.host = host
+        self.with_sample, self.with_depth = with_sample, with_depth
+        rows = 2 + with_sample + with_depth
+        if host:
+            self.seeds = np.ascontiguousarray(seeds, dtype=np.int32)
+            self.out = out if out is not None else np.empty((rows, max(self.capacity, 1)), dtype=np.int32)
+        else:
+            torch = _torch()
+            self.seeds = seeds.to(device="cuda", dtype=torch.int32).contiguous()
+            self.out = out if out is not None else torch.empty((rows, max(self.capacity, 1)), dtype=torch.int32,
+                                                                 device="cuda")
+        self.n = 0
+
+    def _ptr(self, x):
+        if self.host:
+            return x.ctypes.data_as(ctypes.c_void_p).value
+        return x.data_ptr()
+
+    def fill(self, j):
+        j.params = ctypes.pointer(self.params)
+        j.seeds = self._ptr(self.seeds)
+        j.out_src, j.out_dst = self._ptr(self.out[0]), self._ptr(self.out[1])
+        j.out_sample = self._ptr(self.out[2]) if self.with_sample else None
+        j.out_depth = self._ptr(self.out[2 + self.with_sample]) if self.with_depth else None
+        j.capacity = self.capacity
+        j.host_buffers = int(self.host)
+
+    def result(self):
+        k = self.n
+        o = self.out
+        return (o[0, :k], o[1, :k], o[2, :k] if self.with_sample else None,
+                o[2 + self.with_sample, :k] if self.with_depth else None)
 
 
 class Arguments:
@@ -169,4 +222,4 @@ def Sampler(beg, csr, n_blocks, n_threads, n_subgraph, FrontierSize, NeighborSiz
     return out
 
 
-__all__ = ["Graph", "Sampler", "Arguments", "make_params", "edge_bound", "CsawError"]
+__all__ = ["Graph", "Sampler", "Arguments", "BatchJob", "make_params", "edge_bound", "CsawError"]

@@ -13,11 +13,12 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <array>
 #include <vector>
 
 #include "csaw.h"
 #include "csaw_internal.h"
-#include "kernels_sample.cuh"
+#include "kernels_fast.cuh"
 
 using namespace csaw;
 
@@ -46,7 +47,7 @@ int fail(int code, const std::string &msg) {
         if (rc_) return rc_;   \
     } while (0)
 
-enum { KK_EXPAND = 0, KK_HEAVY = 1, KK_WALK = 2, KK_MDRW = 3, KK_INIT = 4, KK_COUNT = 8 };
+enum { KK_EXPAND = 0, KK_HEAVY = 1, KK_WALK = 2, KK_MDRW = 3, KK_INIT = 4, KK_SELECT = 5, KK_COUNT = 8 };
 
 struct Counters {
     unsigned long long out_count;
@@ -54,6 +55,7 @@ struct Counters {
     unsigned long long items[KK_COUNT];
     uint32_t nq[2];
     uint32_t n_heavy;
+    uint32_t n_sel;
     int err;
 };
 
@@ -83,6 +85,16 @@ constexpr int64_t QUEUE_ITEM_BUDGET = 32ll << 20;   // items per ping-pong queue
 constexpr int64_t SCRATCH_BUDGET = 1ll << 30;        // bytes of high-degree scratch
 constexpr int MDRW_MAX_F = 4096;
 
+// Per-job device state: counters, frontier queues, work lists and scratch.
+// Job 0 serves csaw_sample; csaw_sample_batch runs job i on context i, each
+// on its own stream, so independent jobs overlap on the device.
+struct JobCtx {
+    DevBuf q[2][5], heavy, sel, hlist, hscratch, wscratch, seeds_in, out_dev;
+    Counters *ctr = nullptr, *hctr = nullptr;
+    cudaStream_t stream = nullptr;   // owned (batch jobs); job 0 uses the caller's
+    cudaEvent_t done = nullptr;
+};
+
 }  // namespace
 
 struct csaw_graph_s {
@@ -93,12 +105,14 @@ struct csaw_graph_s {
     int32_t *col = nullptr;
     float *weight = nullptr;
     float *ebias = nullptr;
+    bool ebias_flag = false;   // materialised at creation (visible to every schedule)
     float *cdf = nullptr;
     int cdf_bias = -1;
+    void *nbr_beg = nullptr;      // per-edge neighbor records (batched schedules)
+    int32_t *nbr_deg = nullptr;
     int32_t *nonisolated = nullptr;
     int64_t dev_bytes = 0;
-    DevBuf q[2][3], heavy, hscratch, wscratch, seeds_in, out_dev;
-    Counters *ctr = nullptr, *hctr = nullptr;
+    std::vector<JobCtx *> jobs;
     int64_t launches = 0;
     csaw_stats last{};
     bool prof = false;
@@ -111,7 +125,9 @@ struct csaw_graph_s {
 
 namespace {
 
-DevGraph dev_view(const csaw_graph_s *g) {
+// The plain schedule sees the per-edge degree array only when the caller asked
+// for it at creation; the batched schedules materialise it on first use.
+DevGraph dev_view(const csaw_graph_s *g, int schedule = CSAW_SCHED_BATCHED) {
     DevGraph d;
     d.v.rowptr = g->rowptr;
     d.v.rowptr_is_64 = g->idx64;
@@ -119,9 +135,12 @@ DevGraph dev_view(const csaw_graph_s *g) {
     d.v.weight = g->weight;
     d.v.n_vertices = g->V;
     d.v.n_edges = g->E;
-    d.ebias = g->ebias;
+    d.ebias = (schedule != CSAW_SCHED_PLAIN || g->ebias_flag) ? g->ebias : nullptr;
     d.cdf = g->cdf;
     d.cdf_bias = g->cdf_bias;
+    const bool fast = schedule != CSAW_SCHED_PLAIN;
+    d.nbr_beg = fast ? g->nbr_beg : nullptr;
+    d.nbr_deg = fast ? g->nbr_deg : nullptr;
     return d;
 }
 
@@ -178,14 +197,32 @@ int grid_for(K kernel, int threads, size_t dyn_smem, int sm_count) {
     return per_sm * sm_count;
 }
 
+// Per-edge neighbor records, built once per graph on first batched use
+// (E * (sizeof(rowptr) + 4) bytes of HBM).
+int ensure_nbr(csaw_graph_s *g, cudaStream_t st) {
+    if (g->nbr_beg || g->E == 0) return 0;
+    const size_t bsz = g->idx64 ? 8 : 4;
+    CK(cudaMalloc(&g->nbr_beg, bsz * (size_t)g->E));
+    CK(cudaMalloc((void **)&g->nbr_deg, sizeof(int32_t) * (size_t)g->E));
+    g->dev_bytes += (int64_t)(bsz + 4) * g->E;
+    DevGraph dg = dev_view(g);
+    LaunchScope ls(g, KK_INIT, st);
+    if (g->idx64) k_nbr_records<int64_t><<<g->sm_count * 8, 256, 0, st>>>(dg, (int64_t *)g->nbr_beg, g->nbr_deg);
+    else k_nbr_records<int32_t><<<g->sm_count * 8, 256, 0, st>>>(dg, (int32_t *)g->nbr_beg, g->nbr_deg);
+    CK(cudaGetLastError());
+    return 0;
+}
+
 int check_params(const csaw_graph_s *g, const csaw_params *p, int fan[CSAW_MAX_DEPTH]) {
     if (!p) return fail(CSAW_ERR_INVALID, "params is NULL");
     if (p->mode < CSAW_MODE_NEIGHBOR || p->mode > CSAW_MODE_MDRW)
         return fail(CSAW_ERR_INVALID, "unknown mode");
     if (p->bias < CSAW_BIAS_UNBIASED || p->bias > CSAW_BIAS_HOOK)
         return fail(CSAW_ERR_INVALID, "unknown bias");
+    if (p->schedule < CSAW_SCHED_PLAIN || p->schedule > CSAW_SCHED_LEARNED)
+        return fail(CSAW_ERR_INVALID, "unknown schedule");
     if (p->n_samples < 0) return fail(CSAW_ERR_INVALID, "n_samples < 0");
-    if (p->depth < 0 || p->depth > (p->mode == CSAW_MODE_NEIGHBOR ? CSAW_MAX_DEPTH : (1 << 24) - 1))
+    if (p->depth < 0 || p->depth > (p->mode == CSAW_MODE_NEIGHBOR ? CSAW_MAX_DEPTH : (1 << 24) - 64))
         return fail(CSAW_ERR_INVALID, "depth out of range");
     if (p->frontier_size < 1) return fail(CSAW_ERR_INVALID, "frontier_size < 1");
     if (p->bias == CSAW_BIAS_EDGE_WEIGHT && !g->weight)
@@ -205,7 +242,7 @@ int check_params(const csaw_graph_s *g, const csaw_params *p, int fan[CSAW_MAX_D
 }
 
 template <typename I, int BIAS>
-int run_neighbor_t(csaw_graph_s *g, const csaw_params *p, const int fan[], const int32_t *seeds,
+int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int fan[], const int32_t *seeds,
                    const OutArgs &o, cudaStream_t st) {
     constexpr bool BIASED = BIAS != CSAW_BIAS_UNBIASED;
     const int S = p->n_samples, F = p->frontier_size, D = p->depth;
@@ -223,46 +260,73 @@ int run_neighbor_t(csaw_graph_s *g, const csaw_params *p, const int fan[], const
     if (B > S) B = S;
     if (B < 1) B = 1;
     const int64_t qcap = (int64_t)(B * per_sample) + 32;
-    for (int k = 0; k < 2; ++k)
-        for (int a = 0; a < 3; ++a) TRY(ensure(g->q[k][a], sizeof(int32_t) * qcap));
+    const bool plain = p->schedule == CSAW_SCHED_PLAIN;
+    for (int k = 0; k < 2; ++k) {
+        for (int a = 0; a < 3; ++a) TRY(ensure(c->q[k][a], sizeof(int32_t) * qcap));
+        if (!plain) {
+            TRY(ensure(c->q[k][3], sizeof(int64_t) * qcap));
+            TRY(ensure(c->q[k][4], sizeof(int32_t) * qcap));
+        }
+    }
+    if (!plain) {
+        TRY(ensure_nbr(g, st));
+        TRY(ensure(c->sel, sizeof(SelEntry) * qcap));
+        TRY(ensure(c->hlist, sizeof(SelEntry) * qcap));
+    }
+    const int64_t smem_cap = plain ? WBUF : WF;
     int hblocks = 0;
     int64_t hstride = 0;
-    if (BIASED && g->maxdeg > WBUF && !(g->cdf && g->cdf_bias == BIAS)) {
-        TRY(ensure(g->heavy, sizeof(uint32_t) * qcap));
+    if (BIASED && g->maxdeg > smem_cap && !(g->cdf && g->cdf_bias == BIAS)) {
+        TRY(ensure(c->heavy, sizeof(uint32_t) * qcap));
         hstride = g->maxdeg + 2 * ((g->maxdeg >> 5) + 1) + (g->maxdeg >> 10) + 1 + 8;
         hstride = (hstride + 63) & ~63ll;
         hblocks = g->sm_count * 2;
         while (hblocks > 1 && (int64_t)hblocks * hstride * 4 > SCRATCH_BUDGET) hblocks /= 2;
-        TRY(ensure(g->hscratch, sizeof(float) * hstride * hblocks));
+        TRY(ensure(c->hscratch, sizeof(float) * hstride * hblocks));
     }
-    const DevGraph dg = dev_view(g);
+    const DevGraph dg = dev_view(g, p->schedule);
     const uint64_t seed = p->seed;
-    const int grid = grid_for(k_expand_warp<I, BIAS>, EXPAND_THREADS, 0, g->sm_count);
+    const int grid = plain ? grid_for(k_expand_warp<I, BIAS>, EXPAND_THREADS, 0, g->sm_count)
+                           : grid_for(k_coop_fast<I, BIAS>, FAST_THREADS, 0, g->sm_count);
+    const int sgrid = plain ? 0 : grid_for(k_select_fast<I, BIAS>, FAST_THREADS, 0, g->sm_count);
     for (int64_t s0 = 0; s0 < S; s0 += B) {
         const int64_t nb = (S - s0 < B) ? S - s0 : B;
         const uint32_t n0 = (uint32_t)(nb * F);
         {
             LaunchScope ls(g, KK_INIT, st);
-            k_init_queue<<<(n0 + 255) / 256, 256, 0, st>>>(
-                seeds + s0 * F, n0, F, (int)s0, g->V, (int32_t *)g->q[0][0].p, (int32_t *)g->q[0][1].p,
-                (uint32_t *)g->q[0][2].p, &g->ctr->nq[0], &g->ctr->err);
+            if (plain)
+                k_init_queue<<<(n0 + 255) / 256, 256, 0, st>>>(
+                    seeds + s0 * F, n0, F, (int)s0, g->V, (int32_t *)c->q[0][0].p, (int32_t *)c->q[0][1].p,
+                    (uint32_t *)c->q[0][2].p, &c->ctr->nq[0], &c->ctr->err);
+            else
+                k_init_queue_fast<I><<<(n0 + 255) / 256, 256, 0, st>>>(
+                    dg, seeds + s0 * F, n0, F, (int)s0, (int32_t *)c->q[0][0].p, (int32_t *)c->q[0][1].p,
+                    (uint32_t *)c->q[0][2].p, (I *)c->q[0][3].p, (int32_t *)c->q[0][4].p, &c->ctr->nq[0],
+                    &c->ctr->err);
         }
         for (int l = 0; l < D; ++l) {
             const int cur = l & 1, nxt = cur ^ 1;
-            CK(cudaMemsetAsync(&g->ctr->nq[nxt], 0, sizeof(uint32_t), st));
-            CK(cudaMemsetAsync(&g->ctr->n_heavy, 0, sizeof(uint32_t), st));
+            CK(cudaMemsetAsync(&c->ctr->nq[nxt], 0, sizeof(uint32_t), st));
+            CK(cudaMemsetAsync(&c->ctr->n_heavy, 0, 2 * sizeof(uint32_t), st));  // n_heavy, n_sel
             LevelArgs a;
-            a.in_v = (const int32_t *)g->q[cur][0].p;
-            a.in_s = (const int32_t *)g->q[cur][1].p;
-            a.in_p = (const uint32_t *)g->q[cur][2].p;
-            a.n_in = &g->ctr->nq[cur];
-            a.out_v = (int32_t *)g->q[nxt][0].p;
-            a.out_s = (int32_t *)g->q[nxt][1].p;
-            a.out_p = (uint32_t *)g->q[nxt][2].p;
-            a.n_out = &g->ctr->nq[nxt];
-            a.heavy = (uint32_t *)g->heavy.p;
-            a.n_heavy = &g->ctr->n_heavy;
-            a.heavy_scratch = (float *)g->hscratch.p;
+            a.in_v = (const int32_t *)c->q[cur][0].p;
+            a.in_s = (const int32_t *)c->q[cur][1].p;
+            a.in_p = (const uint32_t *)c->q[cur][2].p;
+            a.n_in = &c->ctr->nq[cur];
+            a.out_v = (int32_t *)c->q[nxt][0].p;
+            a.out_s = (int32_t *)c->q[nxt][1].p;
+            a.out_p = (uint32_t *)c->q[nxt][2].p;
+            a.n_out = &c->ctr->nq[nxt];
+            a.in_beg = plain ? nullptr : c->q[cur][3].p;
+            a.in_deg = plain ? nullptr : (const int32_t *)c->q[cur][4].p;
+            a.out_beg = plain ? nullptr : c->q[nxt][3].p;
+            a.out_deg = plain ? nullptr : (int32_t *)c->q[nxt][4].p;
+            a.heavy = (uint32_t *)c->heavy.p;
+            a.n_heavy = &c->ctr->n_heavy;
+            a.sel_list = plain ? nullptr : (SelEntry *)c->sel.p;
+            a.n_sel = &c->ctr->n_sel;
+            a.heavy_list = plain ? nullptr : (SelEntry *)c->hlist.p;
+            a.heavy_scratch = (float *)c->hscratch.p;
             a.heavy_stride = hstride;
             a.o_src = o.src;
             a.o_dst = o.dst;
@@ -270,9 +334,9 @@ int run_neighbor_t(csaw_graph_s *g, const csaw_params *p, const int fan[], const
             a.o_dep = o.dep;
             a.o_count = o.count;
             a.cap = o.cap;
-            a.bytes = g->ctr->bytes;
-            a.items = g->ctr->items;
-            a.err = &g->ctr->err;
+            a.bytes = c->ctr->bytes;
+            a.items = c->ctr->items;
+            a.err = &c->ctr->err;
             a.k0 = (uint32_t)seed;
             a.k1 = (uint32_t)(seed >> 32);
             a.depth = l;
@@ -280,7 +344,12 @@ int run_neighbor_t(csaw_graph_s *g, const csaw_params *p, const int fan[], const
             a.push = l + 1 < D;
             {
                 LaunchScope ls(g, KK_EXPAND, st);
-                k_expand_warp<I, BIAS><<<grid, EXPAND_THREADS, 0, st>>>(dg, a);
+                if (plain) k_expand_warp<I, BIAS><<<grid, EXPAND_THREADS, 0, st>>>(dg, a);
+                else k_coop_fast<I, BIAS><<<grid, FAST_THREADS, 0, st>>>(dg, a);
+            }
+            if (!plain) {
+                LaunchScope ls(g, KK_SELECT, st);
+                k_select_fast<I, BIAS><<<sgrid, FAST_THREADS, 0, st>>>(dg, a);
             }
             if (hblocks) {
                 LaunchScope ls(g, KK_HEAVY, st);
@@ -293,9 +362,11 @@ int run_neighbor_t(csaw_graph_s *g, const csaw_params *p, const int fan[], const
 }
 
 template <typename I, int BIAS>
-int run_walk_t(csaw_graph_s *g, const csaw_params *p, const int32_t *seeds, const OutArgs &o,
+int run_walk_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int32_t *seeds, const OutArgs &o,
                cudaStream_t st) {
-    const DevGraph dg = dev_view(g);
+    const bool plain = p->schedule == CSAW_SCHED_PLAIN;
+    if (!plain) TRY(ensure_nbr(g, st));
+    const DevGraph dg = dev_view(g, p->schedule);
     WalkArgs a{};
     a.seeds = seeds;
     a.n = p->n_samples;
@@ -307,39 +378,43 @@ int run_walk_t(csaw_graph_s *g, const csaw_params *p, const int32_t *seeds, cons
     a.o_dep = o.dep;
     a.o_count = o.count;
     a.cap = o.cap;
-    a.bytes = g->ctr->bytes;
-    a.items = g->ctr->items;
-    a.err = &g->ctr->err;
+    a.bytes = c->ctr->bytes;
+    a.items = c->ctr->items;
+    a.err = &c->ctr->err;
     a.k0 = (uint32_t)p->seed;
     a.k1 = (uint32_t)(p->seed >> 32);
     if (BIAS == CSAW_BIAS_UNBIASED) {
         int grid = (p->n_samples + WALK_THREADS - 1) / WALK_THREADS;
-        int gmax = grid_for(k_walk_thread<I>, WALK_THREADS, 0, g->sm_count);
+        int gmax = plain ? grid_for(k_walk_thread<I>, WALK_THREADS, 0, g->sm_count)
+                         : grid_for(k_walk_thread_fast<I>, WALK_THREADS, 0, g->sm_count);
         if (grid > gmax) grid = gmax;
         LaunchScope ls(g, KK_WALK, st);
-        k_walk_thread<I><<<grid, WALK_THREADS, 0, st>>>(dg, a);
+        if (plain) k_walk_thread<I><<<grid, WALK_THREADS, 0, st>>>(dg, a);
+        else k_walk_thread_fast<I><<<grid, WALK_THREADS, 0, st>>>(dg, a);
     } else {
-        int gmax = grid_for(k_walk_warp<I, BIAS>, WALK_THREADS, 0, g->sm_count);
+        int gmax = plain ? grid_for(k_walk_warp<I, BIAS>, WALK_THREADS, 0, g->sm_count)
+                         : grid_for(k_walk_fast<I, BIAS>, FAST_THREADS, 0, g->sm_count);
         int grid = (p->n_samples + (WALK_THREADS / 32) - 1) / (WALK_THREADS / 32);
         if (grid > gmax) grid = gmax;
-        if (g->maxdeg > WBUF && !(g->cdf && g->cdf_bias == BIAS)) {
+        if (g->maxdeg > (plain ? WBUF : WF) && !(g->cdf && g->cdf_bias == BIAS)) {
             int64_t stride = (g->maxdeg + 63) & ~63ll;
             while (grid > 1 && (int64_t)grid * (WALK_THREADS / 32) * stride * 4 > SCRATCH_BUDGET) grid /= 2;
-            TRY(ensure(g->wscratch, sizeof(float) * stride * grid * (WALK_THREADS / 32)));
-            a.scratch = (float *)g->wscratch.p;
+            TRY(ensure(c->wscratch, sizeof(float) * stride * grid * (WALK_THREADS / 32)));
+            a.scratch = (float *)c->wscratch.p;
             a.scratch_stride = stride;
         }
         LaunchScope ls(g, KK_WALK, st);
-        k_walk_warp<I, BIAS><<<grid, WALK_THREADS, 0, st>>>(dg, a);
+        if (plain) k_walk_warp<I, BIAS><<<grid, WALK_THREADS, 0, st>>>(dg, a);
+        else k_walk_fast<I, BIAS><<<grid, FAST_THREADS, 0, st>>>(dg, a);
     }
     CK(cudaGetLastError());
     return 0;
 }
 
 template <typename I, int BIAS>
-int run_mdrw_t(csaw_graph_s *g, const csaw_params *p, const int32_t *seeds, const OutArgs &o,
+int run_mdrw_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int32_t *seeds, const OutArgs &o,
                cudaStream_t st) {
-    const DevGraph dg = dev_view(g);
+    const DevGraph dg = dev_view(g, p->schedule);
     WalkArgs a{};
     a.seeds = seeds;
     a.n = p->n_samples;
@@ -351,9 +426,9 @@ int run_mdrw_t(csaw_graph_s *g, const csaw_params *p, const int32_t *seeds, cons
     a.o_dep = o.dep;
     a.o_count = o.count;
     a.cap = o.cap;
-    a.bytes = g->ctr->bytes;
-    a.items = g->ctr->items;
-    a.err = &g->ctr->err;
+    a.bytes = c->ctr->bytes;
+    a.items = c->ctr->items;
+    a.err = &c->ctr->err;
     a.k0 = (uint32_t)p->seed;
     a.k1 = (uint32_t)(p->seed >> 32);
     const size_t per_warp = (size_t)8 * a.F;
@@ -372,13 +447,13 @@ int run_mdrw_t(csaw_graph_s *g, const csaw_params *p, const int32_t *seeds, cons
 }
 
 template <typename I>
-int dispatch_bias(csaw_graph_s *g, const csaw_params *p, const int fan[], const int32_t *seeds,
+int dispatch_bias(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int fan[], const int32_t *seeds,
                   const OutArgs &o, cudaStream_t st) {
 #define CSAW_MODES(BIAS)                                                        \
     switch (p->mode) {                                                          \
-        case CSAW_MODE_NEIGHBOR: return run_neighbor_t<I, BIAS>(g, p, fan, seeds, o, st); \
-        case CSAW_MODE_WALK: return run_walk_t<I, BIAS>(g, p, seeds, o, st);    \
-        default: return run_mdrw_t<I, BIAS>(g, p, seeds, o, st);                \
+        case CSAW_MODE_NEIGHBOR: return run_neighbor_t<I, BIAS>(g, c, p, fan, seeds, o, st); \
+        case CSAW_MODE_WALK: return run_walk_t<I, BIAS>(g, c, p, seeds, o, st);    \
+        default: return run_mdrw_t<I, BIAS>(g, c, p, seeds, o, st);                \
     }
     switch (p->bias) {
         case CSAW_BIAS_UNBIASED: CSAW_MODES(CSAW_BIAS_UNBIASED)
@@ -386,56 +461,108 @@ int dispatch_bias(csaw_graph_s *g, const csaw_params *p, const int fan[], const 
         case CSAW_BIAS_EDGE_WEIGHT:
             if (p->mode == CSAW_MODE_MDRW) return fail(CSAW_ERR_INVALID, "MDRW edge-weight bias");
             if (p->mode == CSAW_MODE_NEIGHBOR)
-                return run_neighbor_t<I, CSAW_BIAS_EDGE_WEIGHT>(g, p, fan, seeds, o, st);
-            return run_walk_t<I, CSAW_BIAS_EDGE_WEIGHT>(g, p, seeds, o, st);
+                return run_neighbor_t<I, CSAW_BIAS_EDGE_WEIGHT>(g, c, p, fan, seeds, o, st);
+            return run_walk_t<I, CSAW_BIAS_EDGE_WEIGHT>(g, c, p, seeds, o, st);
         default: CSAW_MODES(CSAW_BIAS_HOOK)
     }
 #undef CSAW_MODES
 }
 
-int sample_impl(csaw_graph_s *g, const csaw_params *p, const int32_t *seeds, int32_t *src, int32_t *dst,
-                int32_t *smp, int32_t *dep, int64_t cap, int64_t *n_out, cudaStream_t st) {
+int new_job(JobCtx **out, bool own_stream) {
+    auto *c = new JobCtx();
+    cudaError_t e = cudaMalloc((void **)&c->ctr, sizeof(Counters));
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&c->hctr, sizeof(Counters));
+    if (e == cudaSuccess && own_stream) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(c->ctr);
+        if (c->hctr) cudaFreeHost(c->hctr);
+        delete c;
+        return fail(CSAW_ERR_NOMEM, std::string("job context: ") + cudaGetErrorString(e));
+    }
+    *out = c;
+    return 0;
+}
+
+void free_job(JobCtx *c) {
+    if (!c) return;
+    for (auto &qq : c->q)
+        for (auto &b : qq) cudaFree(b.p);
+    for (DevBuf *b : {&c->heavy, &c->sel, &c->hlist, &c->hscratch, &c->wscratch, &c->seeds_in, &c->out_dev})
+        cudaFree(b->p);
+    cudaFree(c->ctr);
+    if (c->hctr) cudaFreeHost(c->hctr);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->done) cudaEventDestroy(c->done);
+    delete c;
+}
+
+int64_t job_workspace(const JobCtx *c) {
+    int64_t ws = 0;
+    for (auto &qq : c->q)
+        for (auto &b : qq) ws += (int64_t)b.n;
+    for (const DevBuf *b : {&c->heavy, &c->sel, &c->hlist, &c->hscratch, &c->wscratch, &c->seeds_in, &c->out_dev})
+        ws += (int64_t)b->n;
+    return ws;
+}
+
+int get_job(csaw_graph_s *g, size_t i, JobCtx **out) {
+    while (g->jobs.size() <= i) {
+        JobCtx *c = nullptr;
+        TRY(new_job(&c, true));
+        g->jobs.push_back(c);
+    }
+    *out = g->jobs[i];
+    return 0;
+}
+
+// Enqueues one job on `st` (no host synchronisation): counter reset, the
+// mode's kernels, and the asynchronous read-back of the counter block.
+int enqueue_job(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int32_t *seeds, int32_t *src,
+                int32_t *dst, int32_t *smp, int32_t *dep, int64_t cap, cudaStream_t st) {
     int fan[CSAW_MAX_DEPTH];
-    if (!g) return fail(CSAW_ERR_INVALID, "graph is NULL");
-    if (!n_out) return fail(CSAW_ERR_INVALID, "n_out is NULL");
     TRY(check_params(g, p, fan));
     if (cap < 0) return fail(CSAW_ERR_INVALID, "capacity < 0");
     if (cap > 0 && (!src || !dst)) return fail(CSAW_ERR_INVALID, "out_src/out_dst are NULL");
     if (p->n_samples > 0 && !seeds) return fail(CSAW_ERR_INVALID, "seeds is NULL");
-    CK(cudaSetDevice(g->device));
-    CK(cudaMemsetAsync(g->ctr, 0, sizeof(Counters), st));
-    OutArgs o{src, dst, smp, dep, &g->ctr->out_count, cap};
+    CK(cudaMemsetAsync(c->ctr, 0, sizeof(Counters), st));
+    OutArgs o{src, dst, smp, dep, &c->ctr->out_count, cap};
     if (p->n_samples > 0 && p->depth > 0) {
-        int rc = g->idx64 ? dispatch_bias<int64_t>(g, p, fan, seeds, o, st)
-                          : dispatch_bias<int32_t>(g, p, fan, seeds, o, st);
-        if (rc) {
-            cudaStreamSynchronize(st);
-            drain_profile(g);
-            return rc;
-        }
+        int rc = g->idx64 ? dispatch_bias<int64_t>(g, c, p, fan, seeds, o, st)
+                          : dispatch_bias<int32_t>(g, c, p, fan, seeds, o, st);
+        if (rc) return rc;
     }
-    CK(cudaMemcpyAsync(g->hctr, g->ctr, sizeof(Counters), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    drain_profile(g);
-    const Counters &c = *g->hctr;
-    g->last.last_edges = (int64_t)c.out_count;
-    int64_t items = 0, bytes = 0;
-    for (int k = 0; k < KK_COUNT; ++k) {
-        items += (int64_t)c.items[k];
-        bytes += (int64_t)c.bytes[k];
-        g->kbytes[k] += c.bytes[k];
-        g->kitems[k] += c.items[k];
-    }
-    g->last.last_items = items;
-    g->last.last_bytes = bytes;
-    *n_out = (int64_t)c.out_count;
-    if (c.err & ERR_SEED_RANGE) return fail(CSAW_ERR_INVALID, "a seed vertex is out of range");
-    if (c.err & ERR_UPDATE_RANGE) return fail(CSAW_ERR_DEVICE, "Update() returned a vertex out of range");
-    if (c.err) return fail(CSAW_ERR_DEVICE, "kernel error flag " + std::to_string(c.err));
-    if ((int64_t)c.out_count > cap)
-        return fail(CSAW_ERR_CAPACITY, "output capacity " + std::to_string(cap) + " < " +
-                                           std::to_string(c.out_count) + " edges");
+    CK(cudaMemcpyAsync(c->hctr, c->ctr, sizeof(Counters), cudaMemcpyDeviceToHost, st));
     return 0;
+}
+
+// After the job's stream has been synchronised: edge count, errors, stats.
+int finish_job(csaw_graph_s *g, JobCtx *c, int64_t cap, int64_t *n_out) {
+    const Counters &k = *c->hctr;
+    g->last.last_edges += (int64_t)k.out_count;
+    for (int i = 0; i < KK_COUNT; ++i) {
+        g->last.last_items += (int64_t)k.items[i];
+        g->last.last_bytes += (int64_t)k.bytes[i];
+        g->kbytes[i] += k.bytes[i];
+        g->kitems[i] += k.items[i];
+    }
+    *n_out = (int64_t)k.out_count;
+    if (k.err & ERR_SEED_RANGE) return fail(CSAW_ERR_INVALID, "a seed vertex is out of range");
+    if (k.err & ERR_UPDATE_RANGE) return fail(CSAW_ERR_DEVICE, "Update() returned a vertex out of range");
+    if (k.err) return fail(CSAW_ERR_DEVICE, "kernel error flag " + std::to_string(k.err));
+    if ((int64_t)k.out_count > cap)
+        return fail(CSAW_ERR_CAPACITY, "output capacity " + std::to_string(cap) + " < " +
+                                           std::to_string(k.out_count) + " edges");
+    return 0;
+}
+
+void reset_last(csaw_graph_s *g) {
+    g->last.last_edges = g->last.last_items = g->last.last_bytes = 0;
+}
+
+int64_t seed_count(const csaw_params *p) {
+    return (int64_t)p->n_samples * (p->mode == CSAW_MODE_WALK ? 1 : p->frontier_size);
 }
 
 }  // namespace
@@ -512,9 +639,14 @@ extern "C" int csaw_graph_create(const void *rowptr, int rowptr_is_64, const int
     if (n_non > 0)
         CKG(cudaMemcpy(g->nonisolated, non.data(), sizeof(int32_t) * (size_t)n_non, cudaMemcpyHostToDevice));
     g->dev_bytes += 4 * n_non;
-    CKG(cudaMalloc((void **)&g->ctr, sizeof(Counters)));
-    CKG(cudaMallocHost((void **)&g->hctr, sizeof(Counters)));
+    {
+        JobCtx *c0 = nullptr;
+        int rc = new_job(&c0, false);
+        if (rc) return bail(rc);
+        g->jobs.push_back(c0);
+    }
     if ((flags & CSAW_GRAPH_DEGREE_BIAS) && n_edges > 0) {
+        g->ebias_flag = true;
         CKG(cudaMalloc((void **)&g->ebias, sizeof(float) * (size_t)n_edges));
         g->dev_bytes += 4 * n_edges;
         DevGraph dg = dev_view(g);
@@ -538,16 +670,10 @@ extern "C" int csaw_graph_destroy(csaw_graph g) {
     cudaFree(g->weight);
     cudaFree(g->ebias);
     cudaFree(g->cdf);
+    cudaFree(g->nbr_beg);
+    cudaFree(g->nbr_deg);
     cudaFree(g->nonisolated);
-    for (auto &qq : g->q)
-        for (auto &b : qq) cudaFree(b.p);
-    cudaFree(g->heavy.p);
-    cudaFree(g->hscratch.p);
-    cudaFree(g->wscratch.p);
-    cudaFree(g->seeds_in.p);
-    cudaFree(g->out_dev.p);
-    cudaFree(g->ctr);
-    if (g->hctr) cudaFreeHost(g->hctr);
+    for (JobCtx *c : g->jobs) free_job(c);
     for (auto &pe : g->pending) {
         cudaEventDestroy(pe.second.first);
         cudaEventDestroy(pe.second.second);
@@ -565,9 +691,7 @@ extern "C" int csaw_graph_stats(csaw_graph g, csaw_stats *out) {
     out->max_degree = g->maxdeg;
     out->device_bytes = g->dev_bytes;
     int64_t ws = 0;
-    for (auto &qq : g->q)
-        for (auto &b : qq) ws += (int64_t)b.n;
-    ws += (int64_t)(g->heavy.n + g->hscratch.n + g->wscratch.n + g->seeds_in.n + g->out_dev.n);
+    for (const JobCtx *c : g->jobs) ws += job_workspace(c);
     out->workspace_bytes = ws;
     out->kernel_launches = g->launches;
     return 0;
@@ -614,37 +738,118 @@ extern "C" int csaw_make_seeds(csaw_graph g, int64_t n, uint64_t seed, int32_t *
 extern "C" int csaw_sample(csaw_graph g, const csaw_params *p, const int32_t *seeds, int32_t *out_src,
                            int32_t *out_dst, int32_t *out_sample, int32_t *out_depth, int64_t capacity,
                            int64_t *n_out, void *stream) {
-    return sample_impl(g, p, seeds, out_src, out_dst, out_sample, out_depth, capacity, n_out,
-                       (cudaStream_t)stream);
+    if (!g) return fail(CSAW_ERR_INVALID, "graph is NULL");
+    if (!n_out) return fail(CSAW_ERR_INVALID, "n_out is NULL");
+    CK(cudaSetDevice(g->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    JobCtx *c = g->jobs[0];
+    reset_last(g);
+    int rc = enqueue_job(g, c, p, seeds, out_src, out_dst, out_sample, out_depth, capacity, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    drain_profile(g);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(CSAW_ERR_CUDA, std::string("stream sync: ") + cudaGetErrorString(e));
+    return finish_job(g, c, capacity, n_out);
+}
+
+// Host-buffer job on context c: seeds staged in, outputs staged out.
+static int enqueue_host_job(csaw_graph_s *g, JobCtx *c, csaw_job *j, cudaStream_t st, int32_t **dev_out) {
+    const csaw_params *p = j->params;
+    if (!p) return fail(CSAW_ERR_INVALID, "params is NULL");
+    const int64_t cap = j->capacity;
+    if (cap < 0) return fail(CSAW_ERR_INVALID, "capacity < 0");
+    const int64_t ns = seed_count(p);
+    TRY(ensure(c->seeds_in, sizeof(int32_t) * (size_t)(ns > 0 ? ns : 1)));
+    const int narr = 2 + (j->out_sample != nullptr) + (j->out_depth != nullptr);
+    TRY(ensure(c->out_dev, sizeof(int32_t) * (size_t)(cap > 0 ? cap : 1) * narr));
+    if (ns > 0) CK(cudaMemcpyAsync(c->seeds_in.p, j->seeds, sizeof(int32_t) * ns, cudaMemcpyHostToDevice, st));
+    int32_t *d_src = (int32_t *)c->out_dev.p, *d_dst = d_src + cap;
+    int32_t *d_smp = j->out_sample ? d_dst + cap : nullptr;
+    int32_t *d_dep = j->out_depth ? (d_smp ? d_smp : d_dst) + cap : nullptr;
+    dev_out[0] = d_src;
+    dev_out[1] = d_dst;
+    dev_out[2] = d_smp;
+    dev_out[3] = d_dep;
+    return enqueue_job(g, c, p, (const int32_t *)c->seeds_in.p, d_src, d_dst, d_smp, d_dep, cap, st);
+}
+
+// Copies a finished host-buffer job's edges back (n edges per array).
+static int copy_back(csaw_job *j, int32_t *const *dev_out, int64_t n, cudaStream_t st) {
+    const size_t nb = sizeof(int32_t) * (size_t)n;
+    if (!nb) return 0;
+    CK(cudaMemcpyAsync(j->out_src, dev_out[0], nb, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(j->out_dst, dev_out[1], nb, cudaMemcpyDeviceToHost, st));
+    if (j->out_sample) CK(cudaMemcpyAsync(j->out_sample, dev_out[2], nb, cudaMemcpyDeviceToHost, st));
+    if (j->out_depth) CK(cudaMemcpyAsync(j->out_depth, dev_out[3], nb, cudaMemcpyDeviceToHost, st));
+    return 0;
 }
 
 extern "C" int csaw_sample_host(csaw_graph g, const csaw_params *p, const int32_t *seeds,
                                 int32_t *out_src, int32_t *out_dst, int32_t *out_sample,
                                 int32_t *out_depth, int64_t capacity, int64_t *n_out, void *stream) {
     if (!g || !p || !n_out) return fail(CSAW_ERR_INVALID, "NULL argument");
-    if (capacity < 0) return fail(CSAW_ERR_INVALID, "capacity < 0");
-    cudaStream_t st = (cudaStream_t)stream;
+    csaw_job j{p, seeds, out_src, out_dst, out_sample, out_depth, capacity, 0, 0, 1};
+    int rc = csaw_sample_batch(g, &j, 1, stream);
+    *n_out = j.n_out;
+    return rc;
+}
+
+extern "C" int csaw_sample_batch(csaw_graph g, csaw_job *jobs, int n_jobs, void *stream) {
+    if (!g) return fail(CSAW_ERR_INVALID, "graph is NULL");
+    if (n_jobs < 0 || (n_jobs > 0 && !jobs)) return fail(CSAW_ERR_INVALID, "bad job array");
+    if (n_jobs == 0) return 0;
     CK(cudaSetDevice(g->device));
-    const int64_t nseeds = (int64_t)p->n_samples * (p->mode == CSAW_MODE_WALK ? 1 : p->frontier_size);
-    TRY(ensure(g->seeds_in, sizeof(int32_t) * (size_t)(nseeds > 0 ? nseeds : 1)));
-    const int narr = 2 + (out_sample != nullptr) + (out_depth != nullptr);
-    TRY(ensure(g->out_dev, sizeof(int32_t) * (size_t)(capacity > 0 ? capacity : 1) * narr));
-    if (nseeds > 0)
-        CK(cudaMemcpyAsync(g->seeds_in.p, seeds, sizeof(int32_t) * nseeds, cudaMemcpyHostToDevice, st));
-    int32_t *d_src = (int32_t *)g->out_dev.p, *d_dst = d_src + capacity;
-    int32_t *d_smp = out_sample ? d_dst + capacity : nullptr;
-    int32_t *d_dep = out_depth ? (d_smp ? d_smp : d_dst) + capacity : nullptr;
-    int rc = sample_impl(g, p, (const int32_t *)g->seeds_in.p, d_src, d_dst, d_smp, d_dep, capacity, n_out, st);
-    if (rc) return rc;
-    const size_t nb = sizeof(int32_t) * (size_t)*n_out;
-    if (nb) {
-        CK(cudaMemcpyAsync(out_src, d_src, nb, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(out_dst, d_dst, nb, cudaMemcpyDeviceToHost, st));
-        if (out_sample) CK(cudaMemcpyAsync(out_sample, d_smp, nb, cudaMemcpyDeviceToHost, st));
-        if (out_depth) CK(cudaMemcpyAsync(out_depth, d_dep, nb, cudaMemcpyDeviceToHost, st));
+    cudaStream_t st = (cudaStream_t)stream;
+    reset_last(g);
+    // fork: every job stream waits for work already queued on the caller's stream
+    JobCtx *c0 = g->jobs[0];
+    CK(cudaEventRecord(c0->done, st));
+    std::vector<JobCtx *> ctx((size_t)n_jobs);
+    std::vector<std::array<int32_t *, 4>> dev_out((size_t)n_jobs);
+    int first_rc = 0;
+    for (int i = 0; i < n_jobs; ++i) {
+        csaw_job &j = jobs[i];
+        j.n_out = 0;
+        j.status = 0;
+        int rc = get_job(g, (size_t)i + 1, &ctx[i]);
+        if (!rc) rc = cudaStreamWaitEvent(ctx[i]->stream, c0->done, 0) == cudaSuccess ? 0 :
+                      fail(CSAW_ERR_CUDA, "cudaStreamWaitEvent failed");
+        if (!rc) {
+            if (j.host_buffers) {
+                rc = enqueue_host_job(g, ctx[i], &j, ctx[i]->stream, dev_out[i].data());
+            } else {
+                rc = enqueue_job(g, ctx[i], j.params, j.seeds, j.out_src, j.out_dst, j.out_sample, j.out_depth,
+                                 j.capacity, ctx[i]->stream);
+            }
+        }
+        j.status = rc;
+        if (rc && !first_rc) first_rc = rc;
     }
-    CK(cudaStreamSynchronize(st));
-    return 0;
+    // join
+    for (int i = 0; i < n_jobs; ++i) {
+        if (!ctx[i]) continue;
+        cudaEventRecord(ctx[i]->done, ctx[i]->stream);
+        cudaStreamWaitEvent(st, ctx[i]->done, 0);
+    }
+    cudaError_t e = cudaStreamSynchronize(st);
+    drain_profile(g);
+    if (e != cudaSuccess) return fail(CSAW_ERR_CUDA, std::string("stream sync: ") + cudaGetErrorString(e));
+    std::string first_msg;
+    for (int i = 0; i < n_jobs; ++i) {
+        csaw_job &j = jobs[i];
+        if (j.status) continue;
+        int rc = finish_job(g, ctx[i], j.capacity, &j.n_out);
+        if (!rc && j.host_buffers) rc = copy_back(&j, dev_out[i].data(), j.n_out, ctx[i]->stream);
+        j.status = rc;
+        if (rc && !first_rc) {
+            first_rc = rc;
+            first_msg = g_err;
+        }
+    }
+    for (int i = 0; i < n_jobs; ++i)
+        if (jobs[i].host_buffers && ctx[i]) CK(cudaStreamSynchronize(ctx[i]->stream));
+    if (first_rc && !first_msg.empty()) g_err = first_msg;
+    return first_rc;
 }
 
 // Reference file format: beg.bin = int64[V+1], csr.bin = int64[E]

@@ -23,6 +23,11 @@ struct DevGraph {
     const float *ebias;    // materialised neighbor degree per edge, or null
     const float *cdf;      // canonical per-vertex prefix of cdf_bias, or null
     int cdf_bias;          // bias kind the cdf was built for
+    // Per-edge neighbor records (batched schedules): row begin and degree of
+    // col[e], so a selected neighbor carries its own adjacency range and the
+    // next expansion or walk step skips the dependent rowptr load.
+    const void *nbr_beg;   // I[E] or null
+    const int32_t *nbr_deg;  // int32[E] or null
 };
 
 template <typename I>
@@ -42,6 +47,7 @@ __device__ __forceinline__ float edge_bias(const DevGraph &g, int64_t e) {
     if constexpr (BIAS == CSAW_BIAS_EDGE_WEIGHT) {
         return __ldg(g.v.weight + e);
     } else if constexpr (BIAS == CSAW_BIAS_DEGREE) {
+        if (g.nbr_deg) return __int2float_rn(__ldg(g.nbr_deg + e));
         if (g.ebias) return __ldg(g.ebias + e);
         return degree_f<I>(g, __ldg(g.v.col + e));
     } else {
@@ -252,6 +258,8 @@ struct SelState {
     int cand = -1, sel = -1;
 };
 
+// cand_of(x, act) maps a draw word to a neighbor offset; it is called by all
+// lanes together, and only lanes with act set use the result.
 // Runs slots in order until all N are accepted (returns 0) or the current slot
 // has exhausted its REJECT_ATTEMPTS draws in this phase (returns 1: rebuild).
 // A slot that has used MAX_SLOT_DRAWS draws takes the smallest unselected
@@ -278,13 +286,33 @@ __device__ __forceinline__ int resolve_slots(SelState &st, int N, int lane, cons
             continue;
         }
         if (st.a == REJECT_ATTEMPTS) return 1;
-        if (lane == j) {
-            st.cand = cand_of(rng.word(dc, lane, st.A));
+        const bool me = lane == j;
+        const uint32_t x = me ? rng.word(dc, lane, st.A) : 0u;
+        const int nc = cand_of(x, me);  // warp-uniform call (may shuffle)
+        if (me) {
+            st.cand = nc;
             st.A++;
         }
         st.a++;
     }
     return 0;
+}
+
+// First draws of slots lanes [from, N): the lane `from` continues with its
+// next draw index, later lanes (re)draw their index-0 word on the current
+// prefix.  Warp-uniform.
+template <typename CandFn>
+__device__ __forceinline__ void draw_pending(SelState &st, int from, int N, int lane, const DrawCtx &dc,
+                                             SlotRng &rng, CandFn cand_of) {
+    const bool act = lane >= from && lane < N;
+    const int A = lane == from ? st.A : 0;
+    const uint32_t x = act ? rng.word(dc, lane, A) : 0u;
+    const int c = cand_of(x, act);
+    if (act) {
+        st.cand = c;
+        st.A = A + 1;
+    }
+    st.a = 1;
 }
 
 // Zero-mass fill: slots j..N-1 take the smallest indices not yet selected.

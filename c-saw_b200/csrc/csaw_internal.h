@@ -41,6 +41,21 @@ constexpr int EXPAND_THREADS = 256; // 8 warps per CTA
 constexpr int HEAVY_THREADS = 256;
 constexpr int WALK_THREADS = 256;
 
+// A frontier item whose output and next-queue slots are already reserved
+// (batched schedules): item index in the input queue, first queue slot,
+// first output slot, and a copy of the item (vertex, sample, lineage, degree,
+// row begin) so the consumer needs a single load.
+struct SelEntry {
+    uint32_t it;
+    uint32_t q;
+    unsigned long long ob;
+    int32_t v;
+    int32_t s;
+    uint32_t p;
+    int32_t d;
+    long long beg;
+};
+
 // One level of neighbor sampling: input queue -> output edges + next queue.
 struct LevelArgs {
     const int32_t *in_v;
@@ -51,8 +66,15 @@ struct LevelArgs {
     int32_t *out_s;
     uint32_t *out_p;
     uint32_t *n_out;          // device count of next-level items
+    const void *in_beg;       // batched queues: row begin (I) and degree of
+    const int32_t *in_deg;    //   each item, or null (then read rowptr)
+    void *out_beg;
+    int32_t *out_deg;
     uint32_t *heavy;          // deferred item indices (biased, d > WBUF)
     uint32_t *n_heavy;
+    SelEntry *sel_list;       // batched: warp-granularity items (d > N)
+    uint32_t *n_sel;
+    SelEntry *heavy_list;     // batched: CTA-granularity items (count n_heavy)
     float *heavy_scratch;     // per-CTA scratch for the heavy kernel
     int64_t heavy_stride;     // floats per CTA
     int32_t *o_src, *o_dst, *o_smp, *o_dep;

@@ -1,0 +1,598 @@
+// kernels_fast.cuh -- batched-form level expansion and walk kernels (sm_100a).
+//
+// Same output as kernels_sample.cuh (the canonical prefix, draw keys and slot
+// resolver are shared), scheduled for latency.  On power-law graphs most
+// frontier items have d <= N and take every neighbor, so the work is a chain
+// of dependent loads, not arithmetic:
+//   - queue items carry their own row begin and degree, and every edge has a
+//     materialised neighbor record (row begin, degree of col[e]), so a pushed
+//     child or a walk's next vertex needs no rowptr round trip;
+//   - a warp takes a batch of up to 32 items (lane-parallel loads), reserves
+//     output and next-queue space for the whole batch with one atomic each,
+//     then expands all take-all items together: lanes stride over the batch's
+//     edges, find the owning item by a shuffle binary search over the
+//     inclusive prefix of degrees, and issue every column load at once;
+//   - items with d > N are selected one at a time by the whole warp: biases,
+//     prefix and column ids in registers when d <= 32 (shuffle scans and a
+//     5-step shuffle search), biases preloaded into shared memory in batches
+//     of 8 tiles when d <= WF, the CTA kernel beyond;
+//   - batch size shrinks on small levels so every warp gets work.
+#pragma once
+
+#include "kernels_sample.cuh"
+
+namespace csaw {
+
+constexpr int WF = 512;  // per-warp shared prefix capacity of the fast kernels
+constexpr int FAST_THREADS = 256;
+
+// Canonical prefix of a single tile held one element per lane (w = 0 for
+// lanes >= d): identical to warp_canon_prefix for d <= 32.
+__device__ __forceinline__ float tile_prefix(float w, int d, int lane) {
+    float v = warp_ks_sum(w, lane);
+    float p = lane < d ? __fadd_rn(0.f, __fadd_rn(0.f, v)) : 0.f;
+    return fmaxf(warp_max_scan(p, lane), 0.f);
+}
+
+// First lane whose P exceeds t (P monotone across lanes, P[31] > t).
+__device__ __forceinline__ int shfl_search(float P, float t) {
+    int lo = 0;
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) {
+        float pv = __shfl_sync(FULL, P, lo + s - 1);
+        if (!(pv > t)) lo += s;
+    }
+    return lo;
+}
+
+// First lane whose inclusive count exceeds e (incl monotone, incl[31] > e).
+__device__ __forceinline__ int shfl_search_int(int incl, int e) {
+    int lo = 0;
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) {
+        int pv = __shfl_sync(FULL, incl, lo + s - 1);
+        if (!(pv > e)) lo += s;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int warp_incl_scan(int x, int lane) {
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        int up = __shfl_up_sync(FULL, x, off);
+        if (lane >= off) x += up;
+    }
+    return x;
+}
+
+// Row begin and degree of vertex u: from the neighbor record of edge e when
+// the record describes u, else from rowptr.
+template <typename I>
+__device__ __forceinline__ void row_of(const DevGraph &g, int64_t e, int32_t col_u, int32_t u, int64_t &beg,
+                                       int32_t &deg) {
+    if (g.nbr_beg && u == col_u) {
+        beg = (int64_t)__ldg(((const I *)g.nbr_beg) + e);
+        deg = __ldg(g.nbr_deg + e);
+    } else {
+        beg = row_begin<I>(g, u);
+        deg = (int32_t)(row_begin<I>(g, u + 1) - beg);
+    }
+}
+
+// Loads the biases of edges [beg, beg+d) into W, 8 tiles per round trip.
+template <typename I, int BIAS>
+__device__ __forceinline__ void preload_bias(const DevGraph &g, int64_t beg, int d, float *W, int lane) {
+    for (int i0 = 0; i0 < d; i0 += 256) {
+        float r[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            int i = i0 + u * 32 + lane;
+            r[u] = i < d ? edge_bias<I, BIAS>(g, beg + i) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            int i = i0 + u * 32 + lane;
+            if (i < d) W[i] = r[u];
+        }
+    }
+    __syncwarp();
+}
+
+// Selection for N < d <= 32 entirely in registers.
+template <typename I, int BIAS>
+__device__ __forceinline__ int select_reg(const DevGraph &g, int64_t beg, int d, int N, const DrawCtx &dc,
+                                          int lane) {
+    float w = lane < d ? edge_bias<I, BIAS>(g, beg + lane) : 0.f;
+    float P = tile_prefix(w, d, lane);
+    float T = __shfl_sync(FULL, P, 31);
+    SlotRng rng;
+    SelState st;
+    auto cand_of = [&](uint32_t x, bool act) -> int {
+        float t = act ? its_target(x, T) : 0.f;
+        return shfl_search(P, t);
+    };
+    bool zero = !(T > 0.f);
+    if (!zero) draw_pending(st, 0, N, lane, dc, rng, cand_of);
+    for (;;) {
+        if (zero) {
+            zero_fill(st, N, lane);
+            break;
+        }
+        if (resolve_slots(st, N, lane, dc, rng, cand_of) == 0) break;
+        const int j = st.j;
+        const unsigned zm = __reduce_or_sync(FULL, lane < j ? (1u << st.sel) : 0u);
+        P = tile_prefix(((zm >> lane) & 1u) ? 0.f : w, d, lane);
+        T = __shfl_sync(FULL, P, 31);
+        if (!(T > 0.f)) {
+            zero = true;
+            continue;
+        }
+        draw_pending(st, j, N, lane, dc, rng, cand_of);
+    }
+    return st.sel;
+}
+
+// Selection for 32 < d <= WF with the biases preloaded into W (shared).
+__device__ __forceinline__ int select_smem(const float *W, int d, int N, const DrawCtx &dc, float *P,
+                                           uint32_t *zb, int lane) {
+    auto wfn = [&](int64_t i) { return W[i]; };
+    float T = warp_canon_prefix(wfn, d, P, nullptr, lane);
+    SlotRng rng;
+    SelState st;
+    auto cand_of = [&](uint32_t x, bool act) -> int {
+        return act ? (int)search_upper(P, d, its_target(x, T)) : -1;
+    };
+    bool zero = !(T > 0.f);
+    if (!zero) draw_pending(st, 0, N, lane, dc, rng, cand_of);
+    for (;;) {
+        if (zero) {
+            zero_fill(st, N, lane);
+            break;
+        }
+        if (resolve_slots(st, N, lane, dc, rng, cand_of) == 0) break;
+        const int j = st.j;
+        const int nwords = (d + 31) >> 5;
+        for (int w = lane; w < nwords; w += 32) zb[w] = 0u;
+        __syncwarp();
+        if (lane < j) atomicOr(&zb[st.sel >> 5], 1u << (st.sel & 31));
+        __syncwarp();
+        T = warp_canon_prefix(wfn, d, P, zb, lane);
+        if (!(T > 0.f)) {
+            zero = true;
+            continue;
+        }
+        draw_pending(st, j, N, lane, dc, rng, cand_of);
+    }
+    return st.sel;
+}
+
+// Seeds -> level-0 queue with row begin and degree.
+template <typename I>
+__global__ void k_init_queue_fast(DevGraph g, const int32_t *seeds, uint32_t n, int F, int s0, int32_t *qv,
+                                  int32_t *qs, uint32_t *qp, I *qb, int32_t *qd, uint32_t *qn, int *err) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) *qn = n;
+    if (i >= n) return;
+    int32_t v = seeds[i];
+    if (v < 0 || v >= g.v.n_vertices) {
+        atomicOr(err, ERR_SEED_RANGE);
+        v = 0;
+    }
+    const int64_t b = row_begin<I>(g, v);
+    qv[i] = v;
+    qs[i] = s0 + (int32_t)(i / (uint32_t)F);
+    qp[i] = i % (uint32_t)F;
+    qb[i] = (I)b;
+    qd[i] = (int32_t)(row_begin<I>(g, v + 1) - b);
+}
+
+// Writes one output edge and, on inner levels, the child queue item.
+template <typename I>
+__device__ __forceinline__ void emit_edge(const DevGraph &g, const LevelArgs &a, int64_t e, int32_t v, int32_t s,
+                                          uint32_t child_p, int64_t pos, uint32_t q) {
+    const int32_t u = __ldg(g.v.col + e);
+    int32_t dst = Update(&g.v, u, v);
+    if (dst < 0 || dst >= g.v.n_vertices) {
+        atomicOr(a.err, ERR_UPDATE_RANGE);
+        dst = 0;
+    }
+    if (pos < a.cap) {
+        a.o_src[pos] = v;
+        a.o_dst[pos] = dst;
+        if (a.o_smp) a.o_smp[pos] = s;
+        if (a.o_dep) a.o_dep[pos] = a.depth;
+    }
+    if (a.push) {
+        int64_t nb;
+        int32_t nd;
+        row_of<I>(g, e, u, dst, nb, nd);
+        a.out_v[q] = dst;
+        a.out_s[q] = s;
+        a.out_p[q] = child_p;
+        ((I *)a.out_beg)[q] = (I)nb;
+        a.out_deg[q] = nd;
+    }
+}
+
+// Level expansion, part 1 (every item): batches of up to 32 items per warp,
+// output and next-queue slots reserved for the whole batch, take-all items
+// (d <= N) expanded cooperatively, items needing a draw appended with their
+// reserved slots to the warp list (or the CTA list when biased and d > WF).
+template <typename I, int BIAS>
+__global__ void __launch_bounds__(FAST_THREADS)
+k_coop_fast(DevGraph g, LevelArgs a) {
+    constexpr bool BIASED = BIAS != CSAW_BIAS_UNBIASED;
+    const int lane = threadIdx.x & 31;
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t n = *a.n_in;
+    const int N = a.N;
+    const bool cached = BIASED && g.cdf && g.cdf_bias == BIAS;
+    const int nout = 2 + (a.o_smp != nullptr) + (a.o_dep != nullptr);
+    const unsigned long long per_edge = 4ull + 4ull * nout + (a.push ? 12ull + 2 * (sizeof(I) + 4) : 0ull);
+    uint32_t bs = (n + nw - 1) / nw;
+    bs = bs < 1 ? 1 : (bs > 32 ? 32 : bs);
+    unsigned long long my_bytes = 0, my_items = 0;
+    for (uint32_t base = gw * bs; base < n; base += nw * bs) {
+        const uint32_t it = base + lane;
+        const bool valid = lane < (int)bs && it < n;
+        int32_t v = 0, s = 0;
+        uint32_t p = 0;
+        int64_t beg = 0, d = 0;
+        if (valid) {
+            v = a.in_v[it];
+            s = a.in_s[it];
+            p = a.in_p[it];
+            beg = (int64_t)((const I *)a.in_beg)[it];
+            d = a.in_deg[it];
+        }
+        const int k = (valid && d > 0) ? (int)(d < N ? d : N) : 0;
+        const bool drawn = k > 0 && d > N;
+        const bool heavy = drawn && BIASED && !cached && d > WF;
+        const int incl = warp_incl_scan(k, lane);
+        const int excl = incl - k;
+        const int K = __shfl_sync(FULL, incl, 31);
+        unsigned long long ob = 0;
+        uint32_t qb = 0;
+        if (K) {
+            if (lane == 0) {
+                ob = atomicAdd(a.o_count, (unsigned long long)K);
+                if (a.push) qb = atomicAdd(a.n_out, (uint32_t)K);
+            }
+            ob = __shfl_sync(FULL, ob, 0);
+            qb = __shfl_sync(FULL, qb, 0);
+        }
+        // hand off items that need draws, with their reserved slots
+        const unsigned sm = __ballot_sync(FULL, drawn && !heavy);
+        if (sm) {
+            uint32_t pos = 0;
+            if (lane == 0) pos = atomicAdd(a.n_sel, (uint32_t)__popc(sm));
+            pos = __shfl_sync(FULL, pos, 0);
+            if (drawn && !heavy)
+                a.sel_list[pos + __popc(sm & ((1u << lane) - 1u))] =
+                    SelEntry{it, qb + (uint32_t)excl, ob + excl, v, s, p, (int32_t)d, (long long)beg};
+        }
+        const unsigned hm = __ballot_sync(FULL, heavy);
+        if (hm) {
+            uint32_t pos = 0;
+            if (lane == 0) pos = atomicAdd(a.n_heavy, (uint32_t)__popc(hm));
+            pos = __shfl_sync(FULL, pos, 0);
+            if (heavy)
+                a.heavy_list[pos + __popc(hm & ((1u << lane) - 1u))] =
+                    SelEntry{it, qb + (uint32_t)excl, ob + excl, v, s, p, (int32_t)d, (long long)beg};
+        }
+        if (valid) {
+            my_items++;
+            my_bytes += 12 + sizeof(I) + 4 + (k > 0 && d <= N ? per_edge * k : 0ull);
+        }
+        // take-all items: all lanes stride over their edges together
+        const int ks = (k > 0 && d <= N) ? k : 0;
+        const int incl_s = warp_incl_scan(ks, lane);
+        const int Ks = __shfl_sync(FULL, incl_s, 31);
+        for (int e0 = 0; e0 < Ks; e0 += 32) {
+            const int e = e0 + lane;
+            const bool act = e < Ks;
+            const int b = shfl_search_int(incl_s, act ? e : 0);
+            const int32_t vb = __shfl_sync(FULL, v, b);
+            const int32_t sb = __shfl_sync(FULL, s, b);
+            const uint32_t pb = __shfl_sync(FULL, p, b);
+            const int64_t begb = __shfl_sync(FULL, beg, b);
+            const int exb = __shfl_sync(FULL, excl, b);
+            const int j = e - (__shfl_sync(FULL, incl_s, b) - __shfl_sync(FULL, ks, b));
+            if (act)
+                emit_edge<I>(g, a, begb + j, vb, sb, pb * (uint32_t)N + (uint32_t)j, (int64_t)ob + exb + j,
+                             qb + (uint32_t)(exb + j));
+        }
+    }
+#pragma unroll
+    for (int off = 16; off; off >>= 1) {
+        my_bytes += __shfl_xor_sync(FULL, my_bytes, off);
+        my_items += __shfl_xor_sync(FULL, my_items, off);
+    }
+    if (lane == 0 && my_items) {
+        atomicAdd(&a.bytes[0], my_bytes);
+        atomicAdd(&a.items[0], my_items);
+    }
+}
+
+// Level expansion, part 2: one warp per listed item (N < d, and d <= WF when
+// biased without a CDF cache); writes into the slots reserved by part 1.
+template <typename I, int BIAS>
+__global__ void __launch_bounds__(FAST_THREADS, 4)
+k_select_fast(DevGraph g, LevelArgs a) {
+    constexpr bool BIASED = BIAS != CSAW_BIAS_UNBIASED;
+    constexpr int NW = FAST_THREADS / 32;
+    __shared__ float s_W[BIASED ? NW * WF : 1];
+    __shared__ float s_P[BIASED ? NW * WF : 1];
+    __shared__ uint32_t s_z[BIASED ? NW * (WF / 32) : 1];
+    __shared__ int s_zs[NW * 32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    float *W = s_W + (BIASED ? wib * WF : 0);
+    float *P = s_P + (BIASED ? wib * WF : 0);
+    uint32_t *zb = s_z + (BIASED ? wib * (WF / 32) : 0);
+    int *zs = s_zs + wib * 32;
+    const uint32_t n = *a.n_sel;
+    const int N = a.N;
+    const bool cached = BIASED && g.cdf && g.cdf_bias == BIAS;
+    const int nout = 2 + (a.o_smp != nullptr) + (a.o_dep != nullptr);
+    unsigned long long my_bytes = 0, my_items = 0;
+    for (uint32_t i = gw; i < n; i += nw) {
+        const SelEntry en = a.sel_list[i];
+        const int32_t v = en.v, s = en.s;
+        const uint32_t p = en.p;
+        const int64_t beg = en.beg, d = en.d;
+        const DrawCtx dc{a.k0, a.k1, p, (uint32_t)s, (uint32_t)a.depth};
+        int sel;
+        if constexpr (!BIASED) {
+            sel = select_warp<I, BIAS>(g, beg, d, N, dc, nullptr, nullptr, zs, lane);
+        } else {
+            if (cached) {
+                sel = select_warp<I, BIAS>(g, beg, d, N, dc, P, zb, zs, lane);
+            } else if (d <= 32) {
+                sel = select_reg<I, BIAS>(g, beg, (int)d, N, dc, lane);
+            } else {
+                preload_bias<I, BIAS>(g, beg, (int)d, W, lane);
+                sel = select_smem(W, (int)d, N, dc, P, zb, lane);
+            }
+        }
+        if (lane < N)
+            emit_edge<I>(g, a, beg + sel, v, s, p * (uint32_t)N + (uint32_t)lane, (int64_t)en.ob + lane,
+                         en.q + (uint32_t)lane);
+        if (lane == 0) {
+            my_items++;
+            my_bytes += 16 + (BIASED && !cached ? 4ull * d : 0ull) +
+                        (unsigned long long)N * (4ull + 4ull * nout + (a.push ? 12ull + 2 * (sizeof(I) + 4) : 0ull));
+        }
+    }
+    if (lane == 0 && my_items) {
+        atomicAdd(&a.bytes[5], my_bytes);
+        atomicAdd(&a.items[5], my_items);
+    }
+}
+
+// Biased walks: one warp per walk.  A step with d <= 32 is one round trip:
+// the biases, column ids and neighbor records of all neighbors load together,
+// the prefix and search run in registers, and the chosen lane's record gives
+// the next vertex's adjacency range.  Lane l computes the Philox block of step
+// t0 + l, so one warp-wide Philox serves 32 steps, and lane l holds the edge
+// of step t0 + l until 32 records are written out together.
+template <typename I, int BIAS>
+__global__ void __launch_bounds__(FAST_THREADS, 4)
+k_walk_fast(DevGraph g, WalkArgs a) {
+    constexpr int NW = FAST_THREADS / 32;
+    __shared__ float s_W[NW * WF];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    float *W = s_W + wib * WF;
+    const bool cached = BIAS != CSAW_BIAS_UNBIASED && g.cdf && g.cdf_bias == BIAS;
+    const bool mat = BIAS == CSAW_BIAS_EDGE_WEIGHT || BIAS == CSAW_BIAS_DEGREE;
+    const unsigned long long obytes = 4ull * (2 + (a.o_smp != nullptr) + (a.o_dep != nullptr));
+    const unsigned long long rec = 4ull + sizeof(I) + 4ull;   // col + neighbor record
+    unsigned long long steps = 0, bytes = 0;
+    for (int w = gw; w < a.n; w += nw) {
+        int32_t v = a.seeds[w];
+        if (v < 0 || v >= g.v.n_vertices) {
+            if (lane == 0) atomicOr(a.err, ERR_SEED_RANGE);
+            continue;
+        }
+        int64_t beg = row_begin<I>(g, v);
+        int32_t d = (int32_t)(row_begin<I>(g, v + 1) - beg);
+        bytes += 2 * sizeof(I);
+        uint32_t xw = 0;
+        int32_t rs = 0, rd = 0;
+        int t0 = 0, nrec = 0;
+        auto flush = [&]() {
+            if (nrec == 0) return;
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(a.o_count, (unsigned long long)nrec);
+            base = __shfl_sync(FULL, base, 0);
+            const int64_t pos = (int64_t)base + lane;
+            if (lane < nrec && pos < a.cap) {
+                a.o_src[pos] = rs;
+                a.o_dst[pos] = rd;
+                if (a.o_smp) a.o_smp[pos] = w;
+                if (a.o_dep) a.o_dep[pos] = t0 + lane;
+            }
+            nrec = 0;
+        };
+        for (int t = 0; t < a.len; ++t) {
+            if ((t & 31) == 0) {
+                flush();
+                t0 = t;
+                xw = philox(make_uint4(0u, (uint32_t)w, (TAG_SAMPLE << 24) | (uint32_t)(t + lane), 0u), a.k0,
+                            a.k1).x;
+            }
+            if (d <= 0) break;
+            const uint32_t x = __shfl_sync(FULL, xw, t & 31);
+            int64_t e = beg;
+            int32_t u = 0, nd = 0;
+            int64_t nb = 0;
+            bool have = false;
+            bytes += obytes + rec;
+            if (d == 1) {
+            } else if (BIAS == CSAW_BIAS_UNBIASED) {
+                e = beg + mulhi(x, (uint32_t)d);
+            } else if (cached) {
+                const float *cp = g.cdf + beg;
+                const float T = cp[d - 1];
+                e = beg + (T > 0.f ? search_upper(cp, d, its_target(x, T)) : 0);
+                bytes += 4ull * (64 - __clzll((unsigned long long)d));
+            } else if (d <= 32) {
+                float wl = 0.f;
+                int32_t ul = 0, dl = 0;
+                int64_t bl = 0;
+                if (lane < d) {
+                    wl = edge_bias<I, BIAS>(g, beg + lane);
+                    ul = __ldg(g.v.col + beg + lane);
+                    if (g.nbr_beg) {
+                        bl = (int64_t)__ldg(((const I *)g.nbr_beg) + beg + lane);
+                        dl = __ldg(g.nbr_deg + beg + lane);
+                    }
+                }
+                const float P = tile_prefix(wl, d, lane);
+                const float T = __shfl_sync(FULL, P, 31);
+                int idx = shfl_search(P, T > 0.f ? its_target(x, T) : 0.f);
+                if (!(T > 0.f)) idx = 0;
+                e = beg + idx;
+                u = __shfl_sync(FULL, ul, idx);
+                nb = __shfl_sync(FULL, bl, idx);
+                nd = __shfl_sync(FULL, dl, idx);
+                have = g.nbr_beg != nullptr;
+                bytes += (mat ? 4ull : 4ull + 2ull * sizeof(I)) * d + rec * (d - 1);
+            } else if (d <= WF) {
+                preload_bias<I, BIAS>(g, beg, d, W, lane);
+                auto wfn = [&](int64_t i) { return W[i]; };
+                const float T = warp_canon_prefix(wfn, d, W, nullptr, lane);
+                e = beg + (T > 0.f ? search_upper(W, d, its_target(x, T)) : 0);
+                __syncwarp();
+                bytes += (mat ? 4ull : 4ull + 2ull * sizeof(I)) * d;
+            } else {
+                if (d > a.scratch_stride) {
+                    if (lane == 0) atomicOr(a.err, ERR_SCRATCH);
+                    break;
+                }
+                float *buf = a.scratch + (int64_t)gw * a.scratch_stride;
+                auto wfn = [&](int64_t i) { return edge_bias<I, BIAS>(g, beg + i); };
+                const float T = warp_canon_prefix(wfn, d, buf, nullptr, lane);
+                e = beg + (T > 0.f ? search_upper(buf, d, its_target(x, T)) : 0);
+                bytes += (mat ? 4ull : 4ull + 2ull * sizeof(I)) * d;
+            }
+            if (!have) {
+                u = __ldg(g.v.col + e);
+                if (g.nbr_beg) {
+                    nb = (int64_t)__ldg(((const I *)g.nbr_beg) + e);
+                    nd = __ldg(g.nbr_deg + e);
+                }
+            }
+            int32_t dst = Update(&g.v, u, v);
+            if (dst < 0 || dst >= g.v.n_vertices) {
+                if (lane == 0) atomicOr(a.err, ERR_UPDATE_RANGE);
+                dst = 0;
+            }
+            if (!g.nbr_beg || dst != u) {
+                nb = row_begin<I>(g, dst);
+                nd = (int32_t)(row_begin<I>(g, dst + 1) - nb);
+            }
+            if (lane == (t & 31)) {
+                rs = v;
+                rd = dst;
+            }
+            ++nrec;
+            v = dst;
+            beg = nb;
+            d = nd;
+            ++steps;
+        }
+        flush();
+    }
+    if (lane == 0 && steps) {
+        atomicAdd(&a.bytes[2], bytes);
+        atomicAdd(&a.items[2], steps);
+    }
+}
+
+// Unbiased walks, one thread per walk, one round trip per step via the
+// neighbor records.
+template <typename I>
+__global__ void __launch_bounds__(WALK_THREADS)
+k_walk_thread_fast(DevGraph g, WalkArgs a) {
+    __shared__ int32_t s_out[(WALK_THREADS / 32) * 4 * STAGE];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    WarpStage stg;
+    stg.s_src = s_out + wib * 4 * STAGE;
+    stg.s_dst = stg.s_src + STAGE;
+    stg.s_smp = stg.s_dst + STAGE;
+    stg.s_dep = stg.s_smp + STAGE;
+    const OutArgs oa{a.o_src, a.o_dst, a.o_smp, a.o_dep, a.o_count, a.cap};
+    const int stride = gridDim.x * blockDim.x;
+    unsigned long long steps = 0;
+    for (int base = blockIdx.x * blockDim.x; base < a.n; base += stride) {
+        const int w = base + threadIdx.x;
+        bool alive = w < a.n;
+        int32_t v = 0;
+        int64_t beg = 0;
+        int32_t d = 0;
+        if (alive) {
+            v = a.seeds[w];
+            if (v < 0 || v >= g.v.n_vertices) {
+                atomicOr(a.err, ERR_SEED_RANGE);
+                alive = false;
+            } else {
+                beg = row_begin<I>(g, v);
+                d = (int32_t)(row_begin<I>(g, v + 1) - beg);
+            }
+        }
+        for (int t = 0; t < a.len; ++t) {
+            if (alive && d <= 0) alive = false;
+            if (!__any_sync(FULL, alive)) break;
+            int32_t dst = 0;
+            if (alive) {
+                uint32_t idx = 0;
+                if (d > 1) {
+                    uint4 b = philox(make_uint4(0u, (uint32_t)w, (TAG_SAMPLE << 24) | (uint32_t)t, 0u), a.k0, a.k1);
+                    idx = mulhi(b.x, (uint32_t)d);
+                }
+                const int64_t e = beg + idx;
+                const int32_t u = __ldg(g.v.col + e);
+                dst = Update(&g.v, u, v);
+                if (dst < 0 || dst >= g.v.n_vertices) {
+                    atomicOr(a.err, ERR_UPDATE_RANGE);
+                    dst = 0;
+                }
+                int64_t nb;
+                int32_t nd;
+                row_of<I>(g, e, u, dst, nb, nd);
+                beg = nb;
+                d = nd;
+                ++steps;
+            }
+            stg.push(oa, alive, v, dst, w, t, lane);
+            if (alive) v = dst;
+        }
+    }
+    stg.flush(oa, lane);
+    unsigned long long tot = steps;
+    for (int off = 16; off; off >>= 1) tot += __shfl_xor_sync(FULL, tot, off);
+    if (lane == 0) {
+        unsigned long long per = 4 + sizeof(I) + 4 + 4ull * (2 + (a.o_smp != nullptr) + (a.o_dep != nullptr));
+        atomicAdd(&a.bytes[2], tot * per);
+        atomicAdd(&a.items[2], tot);
+    }
+}
+
+template <typename I>
+__global__ void k_nbr_records(DevGraph g, I *nbeg, int32_t *ndeg) {
+    const I *r = (const I *)g.v.rowptr;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < g.v.n_edges;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t u = __ldg(g.v.col + e);
+        const I b = __ldg(r + u);
+        nbeg[e] = b;
+        ndeg[e] = (int32_t)(__ldg(r + u + 1) - b);
+    }
+}
+
+}  // namespace csaw

@@ -72,15 +72,13 @@ __device__ __forceinline__ int select_warp(const DevGraph &g, int64_t beg, int64
     }
     SlotRng rng;
     SelState st;
-    auto cand_of = [&](uint32_t x) -> int {
+    auto cand_of = [&](uint32_t x, bool act) -> int {
+        if (!act) return -1;
         if constexpr (BIASED) return (int)search_upper(PP, d, its_target(x, T));
         else return kth_not_excluded(mulhi(x, (uint32_t)(d - nZ)), zs, nZ);
     };
     bool zero = BIASED && !(T > 0.f);
-    if (!zero && lane < N) {
-        st.cand = cand_of(rng.word(dc, lane, 0));
-        st.A = 1;
-    }
+    if (!zero) draw_pending(st, 0, N, lane, dc, rng, cand_of);
     for (;;) {
         if (zero) {
             zero_fill(st, N, lane);
@@ -104,13 +102,7 @@ __device__ __forceinline__ int select_warp(const DevGraph &g, int64_t beg, int64
             sort_selected(st, j, zs, lane);
             nZ = j;
         }
-        if (lane == j) {
-            st.cand = cand_of(rng.word(dc, lane, st.A));
-            st.A++;
-        } else if (lane > j && lane < N) {
-            st.cand = cand_of(rng.word(dc, lane, 0));
-        }
-        st.a = 1;
+        draw_pending(st, j, N, lane, dc, rng, cand_of);
     }
     return st.sel;
 }
@@ -212,7 +204,7 @@ k_expand_heavy(DevGraph g, LevelArgs a) {
     const int N = a.N;
     unsigned long long my_bytes = 0, my_items = 0;
     for (uint32_t h = blockIdx.x; h < nh; h += gridDim.x) {
-        const uint32_t it = a.heavy[h];
+        const uint32_t it = a.heavy_list ? a.heavy_list[h].it : a.heavy[h];
         const int32_t v = a.in_v[it];
         const int32_t s = a.in_s[it];
         const uint32_t p = a.in_p[it];
@@ -230,12 +222,11 @@ k_expand_heavy(DevGraph g, LevelArgs a) {
         const DrawCtx dc{a.k0, a.k1, p, (uint32_t)s, (uint32_t)a.depth};
         SlotRng rng;
         SelState st;
-        auto cand_of = [&](uint32_t x) -> int { return (int)search_upper(P, d, its_target(x, T)); };
+        auto cand_of = [&](uint32_t x, bool act) -> int {
+            return act ? (int)search_upper(P, d, its_target(x, T)) : -1;
+        };
         bool zero = !(T > 0.f);
-        if (warp == 0 && !zero && lane < N) {
-            st.cand = cand_of(rng.word(dc, lane, 0));
-            st.A = 1;
-        }
+        if (warp == 0 && !zero) draw_pending(st, 0, N, lane, dc, rng, cand_of);
         for (;;) {
             if (warp == 0) {
                 int r = 0;
@@ -256,17 +247,8 @@ k_expand_heavy(DevGraph g, LevelArgs a) {
             __syncthreads();
             T = cta_canon_prefix(wfn, d, P, tsum, gcar, zb);
             if (warp == 0) {
-                if (!(T > 0.f)) {
-                    zero = true;
-                } else {
-                    if (lane == j) {
-                        st.cand = cand_of(rng.word(dc, lane, st.A));
-                        st.A++;
-                    } else if (lane > j && lane < N) {
-                        st.cand = cand_of(rng.word(dc, lane, 0));
-                    }
-                    st.a = 1;
-                }
+                if (!(T > 0.f)) zero = true;
+                else draw_pending(st, j, N, lane, dc, rng, cand_of);
             }
         }
         if (warp == 0) {
@@ -281,12 +263,17 @@ k_expand_heavy(DevGraph g, LevelArgs a) {
             }
             unsigned long long ob = 0;
             uint32_t q = 0;
-            if (lane == 0) {
-                ob = atomicAdd(a.o_count, (unsigned long long)N);
-                if (a.push) q = atomicAdd(a.n_out, (uint32_t)N);
+            if (a.heavy_list) {  // slots reserved by the batched first pass
+                ob = a.heavy_list[h].ob;
+                q = a.heavy_list[h].q;
+            } else {
+                if (lane == 0) {
+                    ob = atomicAdd(a.o_count, (unsigned long long)N);
+                    if (a.push) q = atomicAdd(a.n_out, (uint32_t)N);
+                }
+                ob = __shfl_sync(FULL, ob, 0);
+                q = __shfl_sync(FULL, q, 0);
             }
-            ob = __shfl_sync(FULL, ob, 0);
-            q = __shfl_sync(FULL, q, 0);
             if (act) {
                 int64_t pos = (int64_t)ob + lane;
                 if (pos < a.cap) {
@@ -299,6 +286,11 @@ k_expand_heavy(DevGraph g, LevelArgs a) {
                     a.out_v[q + lane] = dst;
                     a.out_s[q + lane] = s;
                     a.out_p[q + lane] = p * (uint32_t)N + (uint32_t)lane;
+                    if (a.out_beg) {
+                        const int64_t nb = row_begin<I>(g, dst);
+                        ((I *)a.out_beg)[q + lane] = (I)nb;
+                        a.out_deg[q + lane] = (int32_t)(row_begin<I>(g, dst + 1) - nb);
+                    }
                 }
             }
         }

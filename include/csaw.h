@@ -111,8 +111,9 @@ int csaw_graph_stats(csaw_graph g, csaw_stats *out);
  * launch is bracketed by CUDA events on its stream; csaw_graph_kernel_stats
  * returns, per kernel kind, the summed device time, launches, algorithmic
  * bytes and work items since profiling was (re)enabled.
- * Kinds: 0 level expansion, 1 high-degree expansion, 2 walk, 3 MDRW,
- * 4 queue/seed setup.
+ * Kinds: 0 level expansion (batched: take-all pass), 1 high-degree (CTA)
+ * expansion, 2 walk, 3 MDRW, 4 queue/seed/residency setup, 5 batched
+ * warp-granularity selection pass.
  */
 int csaw_graph_profile(csaw_graph g, int enable);
 int csaw_graph_kernel_stats(csaw_graph g, int kind, double *ms, int64_t *launches,
@@ -138,6 +139,30 @@ int csaw_sample(csaw_graph g, const csaw_params *p, const int32_t *seeds,
 int csaw_sample_host(csaw_graph g, const csaw_params *p, const int32_t *seeds,
                      int32_t *out_src, int32_t *out_dst, int32_t *out_sample,
                      int32_t *out_depth, int64_t capacity, int64_t *n_out, void *stream);
+
+/*
+ * One job of a batch.  params/seeds/outputs as for csaw_sample (device
+ * pointers), or host pointers when host_buffers != 0.  n_out and status are
+ * written by the call.
+ */
+typedef struct {
+    const csaw_params *params;
+    const int32_t *seeds;
+    int32_t *out_src, *out_dst, *out_sample, *out_depth;
+    int64_t capacity;
+    int64_t n_out;
+    int32_t status;
+    int32_t host_buffers;
+} csaw_job;
+
+/*
+ * Runs n_jobs independent jobs together: each on its own stream and device
+ * context, forked from and joined back into `stream`, so latency-bound jobs
+ * (walks, small frontiers) overlap.  Every job's output equals what
+ * csaw_sample would give for it alone.  Returns the first failing status;
+ * per-job status in jobs[i].status.
+ */
+int csaw_sample_batch(csaw_graph g, csaw_job *jobs, int n_jobs, void *stream);
 
 /*
  * Reference-compatible entry (Sampler, non-stream/main.cu:196-308): loads

@@ -19,10 +19,13 @@ def csaw():
     return c
 
 
-def gpu_run(csaw, csr, mode, bias, n, F, depth, fanout, seed, seeds, degree_bias=False, graph=None):
+SCHEDULES = [0, 1]   # plain, batched: both must equal the oracle
+
+
+def gpu_run(csaw, csr, mode, bias, n, F, depth, fanout, seed, seeds, degree_bias=False, graph=None, schedule=0):
     import torch
     g = graph or csaw.Graph(csr, degree_bias=degree_bias)
-    p = csaw.make_params(mode, bias, n, F, (fanout or [1])[0], depth, fanout, seed)
+    p = csaw.make_params(mode, bias, n, F, (fanout or [1])[0], depth, fanout, seed, schedule=schedule)
     out = g.sample(p, torch.from_numpy(np.ascontiguousarray(seeds, dtype=np.int32)).cuda())
     return [x.cpu().numpy() for x in out]
 
@@ -38,54 +41,59 @@ def assert_parity(a, b):
     assert np.array_equal(sa, sb)
 
 
-def test_rmat16_unbiased_small_config(csaw, rmat16):
+@pytest.mark.parametrize("sched", SCHEDULES)
+def test_rmat16_unbiased_small_config(csaw, rmat16, sched):
     """R-MAT scale 16 ef 8, unbiased, 1000 samples, F 1, N 2, D 2, Philox seed 0."""
     g = rmat16
     seeds = oracle.make_seeds(g.rowptr, 1000, 0)
-    a = gpu_run(csaw, g, 0, 0, 1000, 1, 2, [2, 2], 0, seeds)
+    a = gpu_run(csaw, g, 0, 0, 1000, 1, 2, [2, 2], 0, seeds, schedule=sched)
     b = oracle_run(g, 0, 0, 1000, 1, 2, [2, 2], 0, seeds)
     assert len(a[0]) > 0
     assert_parity(a, b)
 
 
+@pytest.mark.parametrize("sched", SCHEDULES)
 @pytest.mark.parametrize("bias", [0, 1, 2])
 @pytest.mark.parametrize("fan", [[20, 20, 20], [3, 7], [1, 1, 1, 1], [32, 2]])
-def test_powerlaw_neighbor_parity(csaw, powerlaw_small, bias, fan):
+def test_powerlaw_neighbor_parity(csaw, powerlaw_small, bias, fan, sched):
     g = powerlaw_small
     n, F = 150, 4
     seeds = oracle.make_seeds(g.rowptr, n * F, 17)
-    a = gpu_run(csaw, g, 0, bias, n, F, len(fan), fan, 0x1234, seeds)
+    a = gpu_run(csaw, g, 0, bias, n, F, len(fan), fan, 0x1234, seeds, schedule=sched)
     b = oracle_run(g, 0, bias, n, F, len(fan), fan, 0x1234, seeds)
     assert_parity(a, b)
 
 
+@pytest.mark.parametrize("sched", SCHEDULES)
 @pytest.mark.parametrize("bias", [0, 1, 2])
-def test_rmat_pareto_heavy_vertices(csaw, rmat12_pareto, bias):
-    """Hub vertices above 1024 neighbors take the CTA path for biased kinds."""
+def test_rmat_pareto_heavy_vertices(csaw, rmat12_pareto, bias, sched):
+    """Hub vertices above the per-warp shared capacity take the CTA path."""
     g = rmat12_pareto
     deg = np.diff(g.rowptr)
     assert deg.max() > 1024
     hubs = np.argsort(deg)[-8:].astype(np.int32)
     seeds = np.concatenate([hubs, oracle.make_seeds(g.rowptr, 192, 2)]).astype(np.int32)
-    a = gpu_run(csaw, g, 0, bias, 200, 1, 2, [25, 10], 77, seeds)
+    a = gpu_run(csaw, g, 0, bias, 200, 1, 2, [25, 10], 77, seeds, schedule=sched)
     b = oracle_run(g, 0, bias, 200, 1, 2, [25, 10], 77, seeds)
     assert_parity(a, b)
 
 
+@pytest.mark.parametrize("sched", SCHEDULES)
 @pytest.mark.parametrize("bias", [0, 1, 2])
-def test_walk_parity(csaw, powerlaw_small, bias):
+def test_walk_parity(csaw, powerlaw_small, bias, sched):
     g = powerlaw_small
     seeds = oracle.make_seeds(g.rowptr, 500, 5)
-    a = gpu_run(csaw, g, 1, bias, 500, 1, 64, None, 9, seeds)
+    a = gpu_run(csaw, g, 1, bias, 500, 1, 64, None, 9, seeds, schedule=sched)
     b = oracle_run(g, 1, bias, 500, 1, 64, None, 9, seeds)
     assert_parity(a, b)
 
 
+@pytest.mark.parametrize("sched", SCHEDULES)
 @pytest.mark.parametrize("bias", [0, 1, 2])
-def test_walk_parity_hubs(csaw, rmat12_pareto, bias):
+def test_walk_parity_hubs(csaw, rmat12_pareto, bias, sched):
     g = rmat12_pareto
     seeds = oracle.make_seeds(g.rowptr, 300, 6)
-    a = gpu_run(csaw, g, 1, bias, 300, 1, 40, None, 10, seeds)
+    a = gpu_run(csaw, g, 1, bias, 300, 1, 40, None, 10, seeds, schedule=sched)
     b = oracle_run(g, 1, bias, 300, 1, 40, None, 10, seeds)
     assert_parity(a, b)
 
@@ -167,3 +175,38 @@ def test_repeat_runs_identical(csaw, rmat12_pareto):
     a = gpu_run(csaw, g, 0, 2, 300, 1, 3, [10, 5, 2], 4, seeds)
     b = gpu_run(csaw, g, 0, 2, 300, 1, 3, [10, 5, 2], 4, seeds)
     assert_parity(a, b)
+
+
+@pytest.mark.parametrize("bias", [0, 1, 2])
+def test_schedules_agree_on_tight_fanout(csaw, rmat12_pareto, bias):
+    """N close to d forces collisions, phase rebuilds and zero-mass fills."""
+    g = rmat12_pareto
+    deg = np.diff(g.rowptr)
+    pick = np.flatnonzero((deg > 20) & (deg < 40))[:300].astype(np.int32)
+    a = gpu_run(csaw, g, 0, bias, len(pick), 1, 2, [20, 3], 21, pick, schedule=0)
+    b = gpu_run(csaw, g, 0, bias, len(pick), 1, 2, [20, 3], 21, pick, schedule=1)
+    c = oracle_run(g, 0, bias, len(pick), 1, 2, [20, 3], 21, pick)
+    assert_parity(a, b)
+    assert_parity(a, c)
+
+
+def test_batch_jobs_equal_solo_runs(csaw, powerlaw_small, rmat12_pareto):
+    """Concurrent jobs (neighbor, walk, MDRW, mixed biases) give exactly the
+    edges each gives alone; host-buffer jobs too."""
+    import torch
+    g = csaw.Graph(powerlaw_small)
+    specs = [(0, 1, 60, 4, 3, [20, 20, 20]), (1, 1, 200, 1, 64, None), (1, 2, 150, 1, 30, None),
+             (0, 0, 80, 2, 2, [5, 5]), (2, 1, 40, 8, 20, None), (0, 2, 50, 1, 3, [10, 5, 2])]
+    jobs, solo = [], []
+    for i, (mode, bias, n, F, depth, fan) in enumerate(specs):
+        seeds = oracle.make_seeds(powerlaw_small.rowptr, n * (1 if mode == 1 else F), 40 + i)
+        p = csaw.make_params(mode, bias, n, F, (fan or [1])[0], depth, fan, 100 + i, schedule=1)
+        jobs.append(csaw.BatchJob(p, torch.from_numpy(seeds).cuda(), host=(i % 2 == 1) and False))
+        solo.append(gpu_run(csaw, powerlaw_small, mode, bias, n, F, depth, fan, 100 + i, seeds, graph=g,
+                            schedule=1))
+    res = g.sample_batch(jobs)
+    for r, s in zip(res, solo):
+        assert_parity([x.cpu().numpy() for x in r], s)
+    hjobs = [csaw.BatchJob(j.params, j.seeds.cpu().numpy(), host=True) for j in jobs]
+    for r, s in zip(g.sample_batch(hjobs), solo):
+        assert_parity(r, s)
