@@ -21,7 +21,7 @@ KERNEL_KINDS = {"expand": 0, "heavy": 1, "walk": 2, "mdrw": 3, "setup": 4, "sele
 EXPORTS = [
     "csaw_last_error", "csaw_version", "csaw_graph_create", "csaw_graph_destroy",
     "csaw_graph_stats", "csaw_graph_profile", "csaw_graph_kernel_stats", "csaw_make_seeds",
-    "csaw_sample", "csaw_sample_host", "csaw_sample_batch", "csaw_sampler_compat",
+    "csaw_sample", "csaw_sample_host", "csaw_sample_batch", "csaw_sample_noalloc", "csaw_sampler_compat",
 ]
 
 
@@ -90,6 +90,7 @@ def lib():
     sig = [p, ctypes.POINTER(Params), p, p, p, p, p, i64, P64, p]
     L.csaw_sample.argtypes = sig
     L.csaw_sample_host.argtypes = sig
+    L.csaw_sample_noalloc.argtypes = sig
     L.csaw_sample_batch.argtypes = [p, ctypes.POINTER(Job), i32, p]
     L.csaw_sampler_compat.argtypes = [ctypes.c_char_p, ctypes.c_char_p, i32, i32, i32, i32, i32, i32,
                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]

@@ -129,6 +129,26 @@ class Graph:
         res.append(out[2 + with_sample, :k] if with_depth else None)
         return tuple(res)
 
+    def sample_noalloc(self, params, seeds, out, capacity=None, with_sample=True, with_depth=True, stream=None):
+        """Neighbor sampling through csaw_sample_noalloc: the library allocates
+        nothing during the call (queues live in a fixed 32 MiB device array),
+        for callers that must not call cudaMalloc while sampling -- e.g. a
+        serving loop whose memory was reserved up front.  `out` is the
+        caller's preallocated device tensor of shape (rows, capacity)."""
+        torch = _torch()
+        if capacity is None:
+            capacity = out.shape[1]
+        ptrs = [ctypes.c_void_p(out[i].data_ptr()) for i in range(out.shape[0])]
+        n = ctypes.c_int64()
+        st = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        check(lib().csaw_sample_noalloc(self.h, ctypes.byref(params), ctypes.c_void_p(seeds.data_ptr()), ptrs[0],
+                                        ptrs[1], ptrs[2] if with_sample else None,
+                                        ptrs[2 + with_sample] if with_depth else None, capacity, ctypes.byref(n),
+                                        ctypes.c_void_p(st)))
+        k = n.value
+        return (out[0, :k], out[1, :k], out[2, :k] if with_sample else None,
+                out[2 + with_sample, :k] if with_depth else None)
+
     def sample_batch(self, jobs, stream=None):
         """Run several BatchJobs together (csaw_sample_batch); returns their edge lists."""
         arr = (_lib.Job * len(jobs))()

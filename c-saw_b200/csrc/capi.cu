@@ -567,6 +567,21 @@ int64_t seed_count(const csaw_params *p) {
 
 }  // namespace
 
+// Accessors for other translation units of this library (declared in
+// csaw_host.h); they touch no existing code path.
+int csaw_host_fail(int code, const char *msg) { return fail(code, msg); }
+
+int csaw_host_plain_view(csaw_graph g, const csaw_params *p, int fan[CSAW_MAX_DEPTH], DevGraph *view,
+                         int64_t *maxdeg, int *device, int *idx64) {
+    if (!g) return fail(CSAW_ERR_INVALID, "graph is NULL");
+    TRY(check_params(g, p, fan));
+    *view = dev_view(g, CSAW_SCHED_PLAIN);
+    *maxdeg = g->maxdeg;
+    *device = g->device;
+    *idx64 = g->idx64;
+    return 0;
+}
+
 // ===================================================================== C ABI
 
 extern "C" const char *csaw_last_error(void) { return g_err.c_str(); }

@@ -35,7 +35,7 @@ __device__ __forceinline__ unsigned long long expansion_bytes(const DevGraph &g,
 }
 
 // -------------------------------------------------------------- queue init
-__global__ void k_init_queue(const int32_t *seeds, uint32_t n, int F, int s0, int64_t V,
+static __global__ void k_init_queue(const int32_t *seeds, uint32_t n, int F, int s0, int64_t V,
                              int32_t *qv, int32_t *qs, uint32_t *qp, uint32_t *qn, int *err) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) *qn = n;
@@ -518,7 +518,7 @@ __global__ void k_mdrw(DevGraph g, WalkArgs a) {
 }
 
 // -------------------------------------------------------------- utilities
-__global__ void k_make_seeds(const int32_t *nonisolated, uint32_t n_non, int64_t n, uint32_t k0,
+static __global__ void k_make_seeds(const int32_t *nonisolated, uint32_t n_non, int64_t n, uint32_t k0,
                              uint32_t k1, int32_t *out) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {

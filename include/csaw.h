@@ -165,6 +165,25 @@ typedef struct {
 int csaw_sample_batch(csaw_graph g, csaw_job *jobs, int n_jobs, void *stream);
 
 /*
+ * Neighbor sampling that allocates no device memory.  No counterpart in the
+ * reference.  For callers that must not call cudaMalloc while sampling: a
+ * serving loop whose memory budget was reserved at start-up, a host thread
+ * that must not stall on the device synchronisation cudaMalloc/cudaFree can
+ * cause, code running inside another framework's memory pool.  Same
+ * arguments and output as csaw_sample (device seeds and outputs, plain
+ * schedule, mode CSAW_MODE_NEIGHBOR only); the frontier queues and counters
+ * live in one fixed 32 MiB device array per GPU, held until process exit.
+ * Rejects, with CSAW_ERR_INVALID and before any GPU work, jobs whose largest
+ * frontier level exceeds 1398090 items, and biased jobs on graphs with a
+ * vertex of degree above 1024.  All calls on a device share the array:
+ * calls whose GPU work overlaps race -- serialise them.  The first call on
+ * a device looks up the array's address; make it before any stream capture.
+ */
+int csaw_sample_noalloc(csaw_graph g, const csaw_params *p, const int32_t *seeds,
+                        int32_t *out_src, int32_t *out_dst, int32_t *out_sample,
+                        int32_t *out_depth, int64_t capacity, int64_t *n_out, void *stream);
+
+/*
  * Reference-compatible entry (Sampler, non-stream/main.cu:196-308): loads
  * int64 beg.bin / csr.bin (graph.hpp:18-34 format), draws FrontierSize seeds
  * per sample, runs neighbor sampling (FrontierSize == 1) or MDRW
