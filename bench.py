@@ -42,6 +42,9 @@ WORK_A = dict(mode=0, bias=1, n_samples=4000, frontier_size=4, neighbor_size=20,
 WORK_B = dict(mode=1, bias=1, n_samples=4000, frontier_size=1, neighbor_size=1, depth=64)
 SEED_A, SEED_B = 0xC5A0, 0xC5A1
 FLUSH_BYTES = 256 << 20
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one
+# ncu capture of this command's timed step, per kernel; see profiles/.
+DRAM_TRAFFIC = {}
 
 
 def load_peaks():
@@ -205,8 +208,10 @@ def main():
     stream = torch.cuda.current_stream()
     seeds_a = G.make_seeds(4000 * 4, SEED_A + 7919 * rank)
     seeds_b = G.make_seeds(4000, SEED_B + 7919 * rank)
-    params = {f: (csaw.make_params(**WORK_A, seed=SEED_A + 7919 * rank, schedule=sch),
-                  csaw.make_params(**WORK_B, seed=SEED_B + 7919 * rank, schedule=sch))
+    from csaw import dist as cdist
+    # replicas (weak scaling): same job shape, rank-disjoint global sample ids
+    params = {f: (cdist.replica_params(csaw.make_params(**WORK_A, seed=SEED_A, schedule=sch), rank),
+                  cdist.replica_params(csaw.make_params(**WORK_B, seed=SEED_B, schedule=sch), rank))
               for f, sch in (("plain", csaw.SCHED_PLAIN), ("batched", csaw.SCHED_BATCHED))}
     pa, pb = params["batched"]
     cap_a, cap_b = csaw.edge_bound(pa), csaw.edge_bound(pb)
@@ -231,11 +236,12 @@ def main():
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
-    def timed(form, clocks=None):
-        """K device-timed steps (L2 flushed before each); returns edges, ms, kernel stats, launches."""
+    def timed(form, clocks=None, profile=False):
+        """K device-timed steps (L2 flushed before each); returns edges, ms, kernel stats, launches.
+        With profile=True every kernel is bracketed by CUDA events (and CUDA-graph replay is off)."""
         for _ in range(args.warmup):
             step(form)
-        G.profile(True)
+        G.profile(profile)
         launches0 = G.stats()["kernel_launches"]
         if clocks:
             clocks.start()
@@ -260,8 +266,11 @@ def main():
     main_form = forms[-1]
     plain_ms, plain_k = None, {}
     if "plain" in forms and main_form != "plain":
-        plain_edges, plain_ms, plain_k, _, _ = timed("plain")
-    edges, ms, kstats, launches, clk = timed(main_form, Clocks(local))
+        plain_edges, plain_ms, plain_k, _, _ = timed("plain", profile=True)
+    # per-kernel events for the roofline come from a profiled pass of the same
+    # steps; the reported value is the unprofiled pass (graph replay allowed)
+    _, prof_ms, kstats, _, _ = timed(main_form, profile=True)
+    edges, ms, _, launches, clk = timed(main_form, Clocks(local))
     if plain_ms is not None and edges != plain_edges:
         raise SystemExit(f"plain and {main_form} forms emitted different edge counts: {plain_edges} vs {edges}")
     pa, pb = params[main_form]
@@ -296,32 +305,34 @@ def main():
     barrier()
     e2e_ms = e0.elapsed_time(e1)
 
-    # ---- max over ranks
+    # ---- whole-job totals: edges summed, device time max over ranks
     t_s = ms / 1e3
-    tot = torch.tensor([float(edges), t_s, float(e2e_edges), e2e_ms / 1e3, (plain_ms or 0.0) / 1e3],
-                       dtype=torch.float64, device="cuda")
     if world > 1:
-        import torch.distributed as dist
-        s = tot.clone()
-        dist.all_reduce(s[0:1])
-        dist.all_reduce(s[2:3])
-        m = tot.clone()
-        dist.all_reduce(m[1:2], op=dist.ReduceOp.MAX)
-        dist.all_reduce(m[3:5], op=dist.ReduceOp.MAX)
-        tot = torch.stack([s[0], m[1], s[2], m[3], m[4]])
-    all_edges, t_max, e2e_all, e2e_t, plain_t = (float(x) for x in tot.cpu())
+        all_edges, t_max = cdist.reduce_totals(edges, t_s)
+        e2e_all, e2e_t = cdist.reduce_totals(e2e_edges, e2e_ms / 1e3)
+        _, plain_t = cdist.reduce_totals(0, (plain_ms or 0.0) / 1e3)
+    else:
+        all_edges, t_max, e2e_all, e2e_t = float(edges), t_s, float(e2e_edges), e2e_ms / 1e3
+        plain_t = (plain_ms or 0.0) / 1e3
     value = all_edges / t_max
     e2e_value = e2e_all / e2e_t
 
     peak, peak_kind = load_peaks()
-    ke = kstats["expand"]
-    achieved = ke["bytes"] / (ke["ms"] * 1e-3) / 1e9 if ke["ms"] > 0 else None
-    per_launch_bytes = ke["bytes"] / ke["launches"] if ke["launches"] else None
-    roofline = {"bound": "hbm", "kernel": "k_expand_warp (level expansion)",
-                "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
-                "traffic": None, "algorithmic_bytes_per_launch": per_launch_bytes,
-                "launch_ms": ke["ms"] / ke["launches"] if ke["launches"] else None}
+    kernel_names = {"expand": "k_coop_fast" if main_form != "plain" else "k_expand_warp",
+                    "select": "k_select_fast", "heavy": "k_expand_heavy",
+                    "walk": "k_walk_fast" if main_form != "plain" else "k_walk_warp"}
+    timed_kinds = [k for k in kernel_names if kstats.get(k, {}).get("launches")]
+    dom = max(timed_kinds, key=lambda k: kstats[k]["ms"])
+    kd = kstats[dom]
+    achieved = kd["bytes"] / (kd["ms"] * 1e-3) / 1e9 if kd["ms"] > 0 else None
+    roofline = {"bound": "hbm", "kernel": kernel_names[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind + " (hbm_gbs copy)",
+                "traffic": DRAM_TRAFFIC.get(kernel_names[dom]),
+                "algorithmic_bytes_per_launch": kd["bytes"] / kd["launches"],
+                "launch_ms": kd["ms"] / kd["launches"],
+                "note": "per-kernel CUDA events on the job streams, from a profiled pass of the same steps "
+                        "(kernel by kernel, no graph replay); in the batched form the neighbor and walk jobs "
+                        "overlap, so each kernel's time includes sharing the GPU"}
 
     if rank == 0:
         line = {"metric": "sampled_edges_per_sec", "value": value, "unit": "edges/s", "n_gpus": world,
@@ -333,6 +344,7 @@ def main():
                         "d2h_bytes_per_step": int(12 * e2e_edges / e2e_steps)},
                 "gpu_launches": int(launches), "clocks": clk, "roofline": roofline,
                 "kernels": {k: v for k, v in kstats.items() if v["launches"]},
+                "profiled_pass_ms_per_step": prof_ms / args.steps,
                 "forms": {main_form: value, "plain": all_edges / plain_t if plain_t else None,
                           "speedup_vs_plain": plain_t / t_max if plain_t else None,
                           "plain_kernels": {k: v for k, v in plain_k.items() if v["launches"]}},

@@ -22,7 +22,9 @@ EXPORTS = [
     "csaw_last_error", "csaw_version", "csaw_graph_create", "csaw_graph_destroy",
     "csaw_graph_stats", "csaw_graph_profile", "csaw_graph_kernel_stats", "csaw_make_seeds",
     "csaw_sample", "csaw_sample_host", "csaw_sample_batch", "csaw_sample_noalloc", "csaw_sampler_compat",
+    "csaw_graph_set_option",
 ]
+OPT_CUDA_GRAPHS = 1
 
 
 class CsawError(RuntimeError):
@@ -42,6 +44,7 @@ class Params(ctypes.Structure):
         ("depth", ctypes.c_int32),
         ("fanout", ctypes.c_int32 * MAX_DEPTH),
         ("seed", ctypes.c_uint64),
+        ("sample_base", ctypes.c_int64),
     ]
 
 
@@ -92,6 +95,7 @@ def lib():
     L.csaw_sample_host.argtypes = sig
     L.csaw_sample_noalloc.argtypes = sig
     L.csaw_sample_batch.argtypes = [p, ctypes.POINTER(Job), i32, p]
+    L.csaw_graph_set_option.argtypes = [p, i32, i64]
     L.csaw_sampler_compat.argtypes = [ctypes.c_char_p, ctypes.c_char_p, i32, i32, i32, i32, i32, i32,
                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
     for name in EXPORTS:

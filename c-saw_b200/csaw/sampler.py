@@ -22,7 +22,7 @@ MODE_NAMES = {"neighbor": MODE_NEIGHBOR, "walk": MODE_WALK, "mdrw": MODE_MDRW}
 
 
 def make_params(mode, bias, n_samples, frontier_size=1, neighbor_size=1, depth=1, fanout=None, seed=0,
-                schedule=SCHED_PLAIN):
+                schedule=SCHED_PLAIN, sample_base=0):
     p = _lib.Params()
     p.mode = MODE_NAMES.get(mode, mode)
     p.bias = BIAS_NAMES.get(bias, bias)
@@ -34,6 +34,7 @@ def make_params(mode, bias, n_samples, frontier_size=1, neighbor_size=1, depth=1
     for i, n in enumerate(fanout or []):
         p.fanout[i] = n
     p.seed = seed
+    p.sample_base = sample_base
     return p
 
 
@@ -89,6 +90,9 @@ class Graph:
         s = _lib.Stats()
         check(lib().csaw_graph_stats(self.h, ctypes.byref(s)))
         return {f: getattr(s, f) for f, _ in _lib.Stats._fields_}
+
+    def set_option(self, option, value):
+        check(lib().csaw_graph_set_option(self.h, option, int(value)))
 
     def profile(self, enable=True):
         check(lib().csaw_graph_profile(self.h, int(enable)))

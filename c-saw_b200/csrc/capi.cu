@@ -14,6 +14,8 @@
 #include <cstring>
 #include <string>
 #include <array>
+#include <map>
+#include <set>
 #include <vector>
 
 #include "csaw.h"
@@ -64,8 +66,13 @@ struct DevBuf {
     size_t n = 0;
 };
 
+// Bumped whenever a device buffer is (re)allocated: cached CUDA graphs that
+// captured older addresses are dropped.
+uint64_t g_alloc_epoch = 1;
+
 int ensure(DevBuf &b, size_t bytes) {
     if (b.n >= bytes) return 0;
+    ++g_alloc_epoch;
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
     b.n = 0;
@@ -121,6 +128,14 @@ struct csaw_graph_s {
     unsigned long long kbytes[KK_COUNT] = {}, kitems[KK_COUNT] = {};
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
     std::vector<cudaEvent_t> event_pool;
+    // CUDA-graph replay of repeated batches: a batch key seen once runs
+    // eagerly (allocating what it needs), the second time it is captured,
+    // afterwards it is replayed as one graph launch.
+    bool use_graphs = true;
+    uint64_t graph_epoch = 0;
+    std::set<std::string> warm;
+    std::map<std::string, cudaGraphExec_t> graphs;
+    std::map<std::string, int64_t> graph_kernels;   // kernel launches per replay
 };
 
 namespace {
@@ -201,6 +216,7 @@ int grid_for(K kernel, int threads, size_t dyn_smem, int sm_count) {
 // (E * (sizeof(rowptr) + 4) bytes of HBM).
 int ensure_nbr(csaw_graph_s *g, cudaStream_t st) {
     if (g->nbr_beg || g->E == 0) return 0;
+    ++g_alloc_epoch;
     const size_t bsz = g->idx64 ? 8 : 4;
     CK(cudaMalloc(&g->nbr_beg, bsz * (size_t)g->E));
     CK(cudaMalloc((void **)&g->nbr_deg, sizeof(int32_t) * (size_t)g->E));
@@ -222,6 +238,8 @@ int check_params(const csaw_graph_s *g, const csaw_params *p, int fan[CSAW_MAX_D
     if (p->schedule < CSAW_SCHED_PLAIN || p->schedule > CSAW_SCHED_LEARNED)
         return fail(CSAW_ERR_INVALID, "unknown schedule");
     if (p->n_samples < 0) return fail(CSAW_ERR_INVALID, "n_samples < 0");
+    if (p->sample_base < 0 || p->sample_base + p->n_samples > INT32_MAX)
+        return fail(CSAW_ERR_INVALID, "sample ids must fit int32 (sample_base + n_samples)");
     if (p->depth < 0 || p->depth > (p->mode == CSAW_MODE_NEIGHBOR ? CSAW_MAX_DEPTH : (1 << 24) - 64))
         return fail(CSAW_ERR_INVALID, "depth out of range");
     if (p->frontier_size < 1) return fail(CSAW_ERR_INVALID, "frontier_size < 1");
@@ -296,11 +314,11 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
             LaunchScope ls(g, KK_INIT, st);
             if (plain)
                 k_init_queue<<<(n0 + 255) / 256, 256, 0, st>>>(
-                    seeds + s0 * F, n0, F, (int)s0, g->V, (int32_t *)c->q[0][0].p, (int32_t *)c->q[0][1].p,
+                    seeds + s0 * F, n0, F, (int)(p->sample_base + s0), g->V, (int32_t *)c->q[0][0].p, (int32_t *)c->q[0][1].p,
                     (uint32_t *)c->q[0][2].p, &c->ctr->nq[0], &c->ctr->err);
             else
                 k_init_queue_fast<I><<<(n0 + 255) / 256, 256, 0, st>>>(
-                    dg, seeds + s0 * F, n0, F, (int)s0, (int32_t *)c->q[0][0].p, (int32_t *)c->q[0][1].p,
+                    dg, seeds + s0 * F, n0, F, (int)(p->sample_base + s0), (int32_t *)c->q[0][0].p, (int32_t *)c->q[0][1].p,
                     (uint32_t *)c->q[0][2].p, (I *)c->q[0][3].p, (int32_t *)c->q[0][4].p, &c->ctr->nq[0],
                     &c->ctr->err);
         }
@@ -372,6 +390,7 @@ int run_walk_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int32_t *
     a.n = p->n_samples;
     a.len = p->depth;
     a.F = 1;
+    a.base = (int)p->sample_base;
     a.o_src = o.src;
     a.o_dst = o.dst;
     a.o_smp = o.smp;
@@ -420,6 +439,7 @@ int run_mdrw_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int32_t *
     a.n = p->n_samples;
     a.len = p->depth;
     a.F = p->frontier_size;
+    a.base = (int)p->sample_base;
     a.o_src = o.src;
     a.o_dst = o.dst;
     a.o_smp = o.smp;
@@ -688,6 +708,7 @@ extern "C" int csaw_graph_destroy(csaw_graph g) {
     cudaFree(g->nbr_beg);
     cudaFree(g->nbr_deg);
     cudaFree(g->nonisolated);
+    for (auto &kv : g->graphs) cudaGraphExecDestroy(kv.second);
     for (JobCtx *c : g->jobs) free_job(c);
     for (auto &pe : g->pending) {
         cudaEventDestroy(pe.second.first);
@@ -809,47 +830,116 @@ extern "C" int csaw_sample_host(csaw_graph g, const csaw_params *p, const int32_
     return rc;
 }
 
-extern "C" int csaw_sample_batch(csaw_graph g, csaw_job *jobs, int n_jobs, void *stream) {
-    if (!g) return fail(CSAW_ERR_INVALID, "graph is NULL");
-    if (n_jobs < 0 || (n_jobs > 0 && !jobs)) return fail(CSAW_ERR_INVALID, "bad job array");
-    if (n_jobs == 0) return 0;
-    CK(cudaSetDevice(g->device));
-    cudaStream_t st = (cudaStream_t)stream;
-    reset_last(g);
-    // fork: every job stream waits for work already queued on the caller's stream
+// Forks the jobs from `st` onto their context streams, enqueues them and
+// joins them back into `st`.
+static int enqueue_batch(csaw_graph_s *g, csaw_job *jobs, int n_jobs, cudaStream_t st, std::vector<JobCtx *> &ctx,
+                         std::vector<std::array<int32_t *, 4>> &dev_out) {
     JobCtx *c0 = g->jobs[0];
     CK(cudaEventRecord(c0->done, st));
-    std::vector<JobCtx *> ctx((size_t)n_jobs);
-    std::vector<std::array<int32_t *, 4>> dev_out((size_t)n_jobs);
     int first_rc = 0;
     for (int i = 0; i < n_jobs; ++i) {
         csaw_job &j = jobs[i];
-        j.n_out = 0;
-        j.status = 0;
         int rc = get_job(g, (size_t)i + 1, &ctx[i]);
         if (!rc) rc = cudaStreamWaitEvent(ctx[i]->stream, c0->done, 0) == cudaSuccess ? 0 :
                       fail(CSAW_ERR_CUDA, "cudaStreamWaitEvent failed");
         if (!rc) {
-            if (j.host_buffers) {
-                rc = enqueue_host_job(g, ctx[i], &j, ctx[i]->stream, dev_out[i].data());
-            } else {
-                rc = enqueue_job(g, ctx[i], j.params, j.seeds, j.out_src, j.out_dst, j.out_sample, j.out_depth,
-                                 j.capacity, ctx[i]->stream);
-            }
+            if (j.host_buffers) rc = enqueue_host_job(g, ctx[i], &j, ctx[i]->stream, dev_out[i].data());
+            else rc = enqueue_job(g, ctx[i], j.params, j.seeds, j.out_src, j.out_dst, j.out_sample, j.out_depth,
+                                  j.capacity, ctx[i]->stream);
         }
         j.status = rc;
         if (rc && !first_rc) first_rc = rc;
     }
-    // join
     for (int i = 0; i < n_jobs; ++i) {
         if (!ctx[i]) continue;
         cudaEventRecord(ctx[i]->done, ctx[i]->stream);
         cudaStreamWaitEvent(st, ctx[i]->done, 0);
     }
+    return first_rc;
+}
+
+static std::string batch_key(const csaw_job *jobs, int n_jobs) {
+    std::string k;
+    for (int i = 0; i < n_jobs; ++i) {
+        const csaw_job &j = jobs[i];
+        k.append((const char *)j.params, sizeof(csaw_params));
+        const void *ptrs[6] = {j.seeds, j.out_src, j.out_dst, j.out_sample, j.out_depth, (const void *)(intptr_t)j.capacity};
+        k.append((const char *)ptrs, sizeof(ptrs));
+    }
+    return k;
+}
+
+extern "C" int csaw_sample_batch(csaw_graph g, csaw_job *jobs, int n_jobs, void *stream) {
+    if (!g) return fail(CSAW_ERR_INVALID, "graph is NULL");
+    if (n_jobs < 0 || (n_jobs > 0 && !jobs)) return fail(CSAW_ERR_INVALID, "bad job array");
+    if (n_jobs == 0) return 0;
+    for (int i = 0; i < n_jobs; ++i)
+        if (!jobs[i].params) return fail(CSAW_ERR_INVALID, "job params is NULL");
+    CK(cudaSetDevice(g->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    reset_last(g);
+    std::vector<JobCtx *> ctx((size_t)n_jobs);
+    std::vector<std::array<int32_t *, 4>> dev_out((size_t)n_jobs);
+    bool graphable = g->use_graphs && !g->prof;
+    for (int i = 0; i < n_jobs && graphable; ++i) graphable = !jobs[i].host_buffers;
+    if (g->graph_epoch != g_alloc_epoch) {   // workspace moved: cached graphs are stale
+        for (auto &kv : g->graphs) cudaGraphExecDestroy(kv.second);
+        g->graphs.clear();
+        g->graph_kernels.clear();
+        g->warm.clear();
+        g->graph_epoch = g_alloc_epoch;
+    }
+    std::string key = graphable ? batch_key(jobs, n_jobs) : std::string();
+    for (int i = 0; i < n_jobs; ++i) {
+        jobs[i].n_out = 0;
+        jobs[i].status = 0;
+    }
+    int first_rc = 0;
+    bool launched = false;
+    if (graphable) {
+        auto it = g->graphs.find(key);
+        if (it == g->graphs.end() && g->warm.count(key)) {
+            cudaGraph_t graph = nullptr;
+            cudaGraphExec_t exec = nullptr;
+            if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                const int64_t l0 = g->launches;
+                int rc = enqueue_batch(g, jobs, n_jobs, st, ctx, dev_out);
+                cudaError_t e = cudaStreamEndCapture(st, &graph);
+                const int64_t nk = g->launches - l0;
+                g->launches = l0;   // captured, not run: counted at each replay
+                if (!rc && e == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+                    it = g->graphs.emplace(key, exec).first;
+                    g->graph_kernels[key] = nk;
+                }
+                if (graph) cudaGraphDestroy(graph);
+            }
+            cudaGetLastError();
+            if (g->graph_epoch != g_alloc_epoch) {   // something allocated during capture: do not keep it
+                if (it != g->graphs.end()) {
+                    cudaGraphExecDestroy(it->second);
+                    g->graph_kernels.erase(it->first);
+                    g->graphs.erase(it);
+                }
+                it = g->graphs.end();
+                g->graph_epoch = g_alloc_epoch;
+            }
+        }
+        if (it != g->graphs.end()) {
+            for (int i = 0; i < n_jobs; ++i) {
+                ctx[i] = g->jobs[(size_t)i + 1];
+                jobs[i].status = 0;
+            }
+            CK(cudaGraphLaunch(it->second, st));
+            g->launches += g->graph_kernels[key];
+            launched = true;
+        }
+    }
+    if (!launched) first_rc = enqueue_batch(g, jobs, n_jobs, st, ctx, dev_out);
     cudaError_t e = cudaStreamSynchronize(st);
     drain_profile(g);
     if (e != cudaSuccess) return fail(CSAW_ERR_CUDA, std::string("stream sync: ") + cudaGetErrorString(e));
     std::string first_msg;
+    if (first_rc) first_msg = g_err;
     for (int i = 0; i < n_jobs; ++i) {
         csaw_job &j = jobs[i];
         if (j.status) continue;
@@ -863,8 +953,23 @@ extern "C" int csaw_sample_batch(csaw_graph g, csaw_job *jobs, int n_jobs, void 
     }
     for (int i = 0; i < n_jobs; ++i)
         if (jobs[i].host_buffers && ctx[i]) CK(cudaStreamSynchronize(ctx[i]->stream));
-    if (first_rc && !first_msg.empty()) g_err = first_msg;
+    if (first_rc) {
+        g_err = first_msg;
+    } else if (graphable && !launched) {
+        g->warm.insert(key);
+    }
     return first_rc;
+}
+
+extern "C" int csaw_graph_set_option(csaw_graph g, int option, int64_t value) {
+    if (!g) return fail(CSAW_ERR_INVALID, "graph is NULL");
+    switch (option) {
+        case CSAW_OPT_CUDA_GRAPHS:
+            g->use_graphs = value != 0;
+            return 0;
+        default:
+            return fail(CSAW_ERR_INVALID, "unknown option");
+    }
 }
 
 // Reference file format: beg.bin = int64[V+1], csr.bin = int64[E]

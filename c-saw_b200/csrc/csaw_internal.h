@@ -92,6 +92,7 @@ struct WalkArgs {
     int n;                    // walks (or samples for MDRW)
     int len;                  // steps
     int F;                    // MDRW frontier size
+    int base;                 // id of the first walk / sample
     int32_t *o_src, *o_dst, *o_smp, *o_dep;
     unsigned long long *o_count;
     int64_t cap;

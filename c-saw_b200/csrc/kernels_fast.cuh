@@ -98,72 +98,160 @@ __device__ __forceinline__ void preload_bias(const DevGraph &g, int64_t beg, int
     __syncwarp();
 }
 
-// Selection for N < d <= 32 entirely in registers.
-template <typename I, int BIAS>
-__device__ __forceinline__ int select_reg(const DevGraph &g, int64_t beg, int d, int N, const DrawCtx &dc,
-                                          int lane) {
-    float w = lane < d ? edge_bias<I, BIAS>(g, beg + lane) : 0.f;
-    float P = tile_prefix(w, d, lane);
-    float T = __shfl_sync(FULL, P, 31);
+// Speculative resolver of the batched kernels (same result as resolve_slots).
+// A rejection phase allows REJECT_ATTEMPTS = 4 draws per slot, and the four
+// words of one Philox block are exactly the next four draws of a slot, so
+// every pending lane computes the candidates of its next four draws at once
+// (four independent searches, overlapped) and a rejected draw costs one
+// shuffle and one ballot instead of a serial search.
+struct Spec4 {
+    int j = 0, a = 1;   // warp uniform: current slot, draws it used in this window
+    int base = 0;       // lane: draw index of c0 (a multiple of 4)
+    int sel = -1;
+    int c0 = -1, c1 = -1, c2 = -1, c3 = -1;
+    __device__ __forceinline__ int pick(int k) const { return k == 0 ? c0 : (k == 1 ? c1 : (k == 2 ? c2 : c3)); }
+};
+
+// Windows of lanes [from, N): lane `from` starts at draw from_base, later
+// lanes at draw 0, all on the current prefix.  Warp-uniform.
+template <typename CandFn>
+__device__ __forceinline__ void spec_fill(Spec4 &st, int from, int N, int lane, const DrawCtx &dc, SlotRng &rng,
+                                          CandFn cand_of, int from_base) {
+    const bool act = lane >= from && lane < N;
+    const int base = lane == from ? from_base : 0;
+    uint32_t x0 = 0, x1 = 0, x2 = 0, x3 = 0;
+    if (act) {
+        x0 = rng.word(dc, lane, base);
+        x1 = rng.word(dc, lane, base + 1);
+        x2 = rng.word(dc, lane, base + 2);
+        x3 = rng.word(dc, lane, base + 3);
+    }
+    const int n0 = cand_of(x0, act), n1 = cand_of(x1, act), n2 = cand_of(x2, act), n3 = cand_of(x3, act);
+    if (act) {
+        st.base = base;
+        st.c0 = n0;
+        st.c1 = n1;
+        st.c2 = n2;
+        st.c3 = n3;
+    }
+    st.a = 1;
+}
+
+__device__ __forceinline__ void fill_smallest(Spec4 &st, int j, int lane) {
+    int i = 0;
+    while (__ballot_sync(FULL, lane < j && st.sel == i)) ++i;
+    if (lane == j) st.sel = i;
+}
+
+// 0: all N slots accepted; 1: slot st.j needs a phase rebuild.
+__device__ __forceinline__ int resolve4(Spec4 &st, int N, int lane) {
+    while (st.j < N) {
+        const int j = st.j, a = st.a;
+        const int c = __shfl_sync(FULL, st.pick(a - 1), j);
+        if (!__ballot_sync(FULL, lane < j && st.sel == c)) {
+            if (lane == j) st.sel = c;
+            st.j = j + 1;
+            st.a = 1;
+            continue;
+        }
+        if (__shfl_sync(FULL, st.base, j) + a == MAX_SLOT_DRAWS) {
+            fill_smallest(st, j, lane);
+            st.j = j + 1;
+            st.a = 1;
+            continue;
+        }
+        if (a == REJECT_ATTEMPTS) return 1;
+        st.a = a + 1;
+    }
+    return 0;
+}
+
+// Generic driver: cand_of(x, act) maps a draw word to a candidate (warp-
+// uniform call); rebuild(st, j) zeroes the selections of slots < j out of the
+// prefix and returns false when no positive mass is left.
+template <typename CandFn, typename RebuildFn>
+__device__ __forceinline__ int select_spec(int N, int lane, const DrawCtx &dc, bool zero, CandFn cand_of,
+                                           RebuildFn rebuild) {
     SlotRng rng;
-    SelState st;
-    auto cand_of = [&](uint32_t x, bool act) -> int {
-        float t = act ? its_target(x, T) : 0.f;
-        return shfl_search(P, t);
-    };
-    bool zero = !(T > 0.f);
-    if (!zero) draw_pending(st, 0, N, lane, dc, rng, cand_of);
+    Spec4 st;
+    if (!zero) spec_fill(st, 0, N, lane, dc, rng, cand_of, 0);
     for (;;) {
         if (zero) {
-            zero_fill(st, N, lane);
+            for (int jj = st.j; jj < N; ++jj) fill_smallest(st, jj, lane);
             break;
         }
-        if (resolve_slots(st, N, lane, dc, rng, cand_of) == 0) break;
+        if (resolve4(st, N, lane) == 0) break;
         const int j = st.j;
-        const unsigned zm = __reduce_or_sync(FULL, lane < j ? (1u << st.sel) : 0u);
-        P = tile_prefix(((zm >> lane) & 1u) ? 0.f : w, d, lane);
-        T = __shfl_sync(FULL, P, 31);
-        if (!(T > 0.f)) {
+        const int next = __shfl_sync(FULL, st.base, j) + REJECT_ATTEMPTS;
+        if (!rebuild(st, j)) {
             zero = true;
             continue;
         }
-        draw_pending(st, j, N, lane, dc, rng, cand_of);
+        spec_fill(st, j, N, lane, dc, rng, cand_of, next);
     }
     return st.sel;
 }
 
-// Selection for 32 < d <= WF with the biases preloaded into W (shared).
+// Selection for N < d <= 32 entirely in registers.
+template <typename I, int BIAS>
+__device__ __forceinline__ int select_reg(const DevGraph &g, int64_t beg, int d, int N, const DrawCtx &dc,
+                                          int lane) {
+    const float w = lane < d ? edge_bias<I, BIAS>(g, beg + lane) : 0.f;
+    float P = tile_prefix(w, d, lane);
+    float T = __shfl_sync(FULL, P, 31);
+    auto cand_of = [&](uint32_t x, bool act) -> int {
+        const float t = act ? its_target(x, T) : 0.f;
+        return shfl_search(P, t);
+    };
+    auto rebuild = [&](const Spec4 &st, int j) -> bool {
+        const unsigned zm = __reduce_or_sync(FULL, lane < j ? (1u << st.sel) : 0u);
+        P = tile_prefix(((zm >> lane) & 1u) ? 0.f : w, d, lane);
+        T = __shfl_sync(FULL, P, 31);
+        return T > 0.f;
+    };
+    return select_spec(N, lane, dc, !(T > 0.f), cand_of, rebuild);
+}
+
+// Selection for 32 < d with the canonical prefix in P (shared or a cached
+// CDF); W holds the raw biases for rebuilds (shared), zb a rebuild bitmap.
 __device__ __forceinline__ int select_smem(const float *W, int d, int N, const DrawCtx &dc, float *P,
                                            uint32_t *zb, int lane) {
     auto wfn = [&](int64_t i) { return W[i]; };
     float T = warp_canon_prefix(wfn, d, P, nullptr, lane);
-    SlotRng rng;
-    SelState st;
     auto cand_of = [&](uint32_t x, bool act) -> int {
         return act ? (int)search_upper(P, d, its_target(x, T)) : -1;
     };
-    bool zero = !(T > 0.f);
-    if (!zero) draw_pending(st, 0, N, lane, dc, rng, cand_of);
-    for (;;) {
-        if (zero) {
-            zero_fill(st, N, lane);
-            break;
-        }
-        if (resolve_slots(st, N, lane, dc, rng, cand_of) == 0) break;
-        const int j = st.j;
+    auto rebuild = [&](const Spec4 &st, int j) -> bool {
         const int nwords = (d + 31) >> 5;
         for (int w = lane; w < nwords; w += 32) zb[w] = 0u;
         __syncwarp();
         if (lane < j) atomicOr(&zb[st.sel >> 5], 1u << (st.sel & 31));
         __syncwarp();
         T = warp_canon_prefix(wfn, d, P, zb, lane);
-        if (!(T > 0.f)) {
-            zero = true;
-            continue;
+        return T > 0.f;
+    };
+    return select_spec(N, lane, dc, !(T > 0.f), cand_of, rebuild);
+}
+
+// Unbiased selection (no prefix): index ranks over the non-excluded range.
+__device__ __forceinline__ int select_unbiased(int64_t d, int N, const DrawCtx &dc, int *zs, int lane) {
+    int nZ = 0;
+    auto cand_of = [&](uint32_t x, bool act) -> int {
+        return act ? kth_not_excluded(mulhi(x, (uint32_t)(d - nZ)), zs, nZ) : -1;
+    };
+    auto rebuild = [&](const Spec4 &st, int j) -> bool {
+        int rank = 0;
+        for (int m = 0; m < j; ++m) {
+            const int sm = __shfl_sync(FULL, st.sel, m);
+            if (sm < st.sel) ++rank;
         }
-        draw_pending(st, j, N, lane, dc, rng, cand_of);
-    }
-    return st.sel;
+        __syncwarp();
+        if (lane < j) zs[rank] = st.sel;
+        __syncwarp();
+        nZ = j;
+        return true;
+    };
+    return select_spec(N, lane, dc, false, cand_of, rebuild);
 }
 
 // Seeds -> level-0 queue with row begin and degree.
@@ -346,7 +434,7 @@ k_select_fast(DevGraph g, LevelArgs a) {
         const DrawCtx dc{a.k0, a.k1, p, (uint32_t)s, (uint32_t)a.depth};
         int sel;
         if constexpr (!BIASED) {
-            sel = select_warp<I, BIAS>(g, beg, d, N, dc, nullptr, nullptr, zs, lane);
+            sel = select_unbiased(d, N, dc, zs, lane);
         } else {
             if (cached) {
                 sel = select_warp<I, BIAS>(g, beg, d, N, dc, P, zb, zs, lane);
@@ -413,7 +501,7 @@ k_walk_fast(DevGraph g, WalkArgs a) {
             if (lane < nrec && pos < a.cap) {
                 a.o_src[pos] = rs;
                 a.o_dst[pos] = rd;
-                if (a.o_smp) a.o_smp[pos] = w;
+                if (a.o_smp) a.o_smp[pos] = a.base + w;
                 if (a.o_dep) a.o_dep[pos] = t0 + lane;
             }
             nrec = 0;
@@ -422,7 +510,7 @@ k_walk_fast(DevGraph g, WalkArgs a) {
             if ((t & 31) == 0) {
                 flush();
                 t0 = t;
-                xw = philox(make_uint4(0u, (uint32_t)w, (TAG_SAMPLE << 24) | (uint32_t)(t + lane), 0u), a.k0,
+                xw = philox(make_uint4(0u, (uint32_t)(a.base + w), (TAG_SAMPLE << 24) | (uint32_t)(t + lane), 0u), a.k0,
                             a.k1).x;
             }
             if (d <= 0) break;
@@ -452,10 +540,13 @@ k_walk_fast(DevGraph g, WalkArgs a) {
                         dl = __ldg(g.nbr_deg + beg + lane);
                     }
                 }
-                const float P = tile_prefix(wl, d, lane);
-                const float T = __shfl_sync(FULL, P, 31);
-                int idx = shfl_search(P, T > 0.f ? its_target(x, T) : 0.f);
-                if (!(T > 0.f)) idx = 0;
+                // canonical prefix of one tile; the first lane above t is the
+                // same with or without the running max, and T is the max
+                const float v = warp_ks_sum(wl, lane);
+                const float P = lane < d ? __fadd_rn(0.f, __fadd_rn(0.f, v)) : 0.f;
+                const float T = __uint_as_float(__reduce_max_sync(FULL, __float_as_uint(P)));
+                int idx = 0;
+                if (T > 0.f) idx = __ffs(__ballot_sync(FULL, P > its_target(x, T))) - 1;
                 e = beg + idx;
                 u = __shfl_sync(FULL, ul, idx);
                 nb = __shfl_sync(FULL, bl, idx);
@@ -552,7 +643,7 @@ k_walk_thread_fast(DevGraph g, WalkArgs a) {
             if (alive) {
                 uint32_t idx = 0;
                 if (d > 1) {
-                    uint4 b = philox(make_uint4(0u, (uint32_t)w, (TAG_SAMPLE << 24) | (uint32_t)t, 0u), a.k0, a.k1);
+                    uint4 b = philox(make_uint4(0u, (uint32_t)(a.base + w), (TAG_SAMPLE << 24) | (uint32_t)t, 0u), a.k0, a.k1);
                     idx = mulhi(b.x, (uint32_t)d);
                 }
                 const int64_t e = beg + idx;
@@ -569,7 +660,7 @@ k_walk_thread_fast(DevGraph g, WalkArgs a) {
                 d = nd;
                 ++steps;
             }
-            stg.push(oa, alive, v, dst, w, t, lane);
+            stg.push(oa, alive, v, dst, a.base + w, t, lane);
             if (alive) v = dst;
         }
     }

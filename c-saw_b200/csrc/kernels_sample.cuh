@@ -342,7 +342,7 @@ k_walk_thread(DevGraph g, WalkArgs a) {
                 } else {
                     uint32_t idx = 0;
                     if (d > 1) {
-                        uint4 b = philox(make_uint4(0u, (uint32_t)w, (TAG_SAMPLE << 24) | (uint32_t)t, 0u),
+                        uint4 b = philox(make_uint4(0u, (uint32_t)(a.base + w), (TAG_SAMPLE << 24) | (uint32_t)t, 0u),
                                          a.k0, a.k1);
                         idx = mulhi(b.x, (uint32_t)d);
                     }
@@ -355,7 +355,7 @@ k_walk_thread(DevGraph g, WalkArgs a) {
                     ++steps;
                 }
             }
-            stg.push(oa, act, v, dst, w, t, lane);
+            stg.push(oa, act, v, dst, a.base + w, t, lane);
             if (act) v = dst;
         }
     }
@@ -426,7 +426,7 @@ k_walk_warp(DevGraph g, WalkArgs a) {
                                  : (4ull + 2ull * sizeof(I)) * d;
                 }
                 if (T > 0.f) {
-                    uint4 b = philox(make_uint4(0u, (uint32_t)w, (TAG_SAMPLE << 24) | (uint32_t)t, 0u),
+                    uint4 b = philox(make_uint4(0u, (uint32_t)(a.base + w), (TAG_SAMPLE << 24) | (uint32_t)t, 0u),
                                      a.k0, a.k1);
                     idx = search_upper(PP, d, its_target(b.x, T));
                 }
@@ -436,7 +436,7 @@ k_walk_warp(DevGraph g, WalkArgs a) {
                 if (lane == 0) atomicOr(a.err, ERR_UPDATE_RANGE);
                 dst = 0;
             }
-            stg.push(oa, lane == 0, v, dst, w, t, lane);
+            stg.push(oa, lane == 0, v, dst, a.base + w, t, lane);
             v = dst;
             ++steps;
         }
@@ -480,7 +480,7 @@ __global__ void k_mdrw(DevGraph g, WalkArgs a) {
         }
         __syncwarp();
         for (int t = 0; t < a.len; ++t) {
-            uint4 b = philox(make_uint4(0u, (uint32_t)s, (TAG_MDRW << 24) | (uint32_t)t, 0u), a.k0, a.k1);
+            uint4 b = philox(make_uint4(0u, (uint32_t)(a.base + s), (TAG_MDRW << 24) | (uint32_t)t, 0u), a.k0, a.k1);
             int slot = 0;
             if (F > 1) {
                 auto wfn = [&](int64_t i) -> float {
@@ -501,7 +501,7 @@ __global__ void k_mdrw(DevGraph g, WalkArgs a) {
                     if (lane == 0) atomicOr(a.err, ERR_UPDATE_RANGE);
                     dst = 0;
                 }
-                stg.push(oa, lane == 0, v, dst, s, t, lane);
+                stg.push(oa, lane == 0, v, dst, a.base + s, t, lane);
                 bytes += 4 + obytes;
                 ++steps;
                 __syncwarp();

@@ -88,7 +88,7 @@ void launch_levels(const DevGraph &dg, const csaw_params *p, const int fan[], co
         }
     const int S = p->n_samples, F = p->frontier_size, D = p->depth;
     const uint32_t n0 = (uint32_t)((int64_t)S * F);
-    k_init_queue<<<(n0 + 255) / 256, 256, 0, st>>>(seeds, n0, F, 0, dg.v.n_vertices, q[0][0], q[0][1],
+    k_init_queue<<<(n0 + 255) / 256, 256, 0, st>>>(seeds, n0, F, (int)p->sample_base, dg.v.n_vertices, q[0][0], q[0][1],
                                                    (uint32_t *)q[0][2], &c->nq[0], &c->err);
     for (int l = 0; l < D; ++l) {
         const int s = l & 1, t = s ^ 1;

@@ -67,6 +67,9 @@ typedef struct {
     int32_t depth;          /* Depth (hops), walk length, or MDRW steps */
     int32_t fanout[CSAW_MAX_DEPTH]; /* per-hop NeighborSize (0 = neighbor_size) */
     uint64_t seed;          /* Philox key: the whole output is a function of it */
+    int64_t sample_base;    /* id of the first sample (keys and output ids are
+                               sample_base + i), so shards of one job run on
+                               several GPUs give exactly the single-GPU output */
 } csaw_params;
 
 typedef struct csaw_graph_s *csaw_graph;
@@ -163,6 +166,16 @@ typedef struct {
  * per-job status in jobs[i].status.
  */
 int csaw_sample_batch(csaw_graph g, csaw_job *jobs, int n_jobs, void *stream);
+
+/* Graph options. */
+enum {
+    /* 1 (default): a batch of device-buffer jobs seen before with the same
+     * parameters and buffers is captured once into a CUDA graph and replayed
+     * as one launch afterwards; 0: always launch kernel by kernel.  Off while
+     * profiling is on. */
+    CSAW_OPT_CUDA_GRAPHS = 1
+};
+int csaw_graph_set_option(csaw_graph g, int option, int64_t value);
 
 /*
  * Neighbor sampling that allocates no device memory.  No counterpart in the

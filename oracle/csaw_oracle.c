@@ -312,8 +312,9 @@ typedef struct {
     int status;
 } job_t;
 
-static void run_neighbor(job_t *jb, int s) {
+static void run_neighbor(job_t *jb, int sl) {
     const oracle_params *p = jb->p;
+    const int s = (int)(p->sample_base + sl);
     ctx_t *c = &jb->c;
     int64_t cap = 64, n = 0;
     int32_t *cv = (int32_t *)malloc(sizeof(int32_t) * (size_t)cap);
@@ -324,7 +325,7 @@ static void run_neighbor(job_t *jb, int s) {
             cv = (int32_t *)realloc(cv, sizeof(int32_t) * (size_t)cap);
             cp = (uint32_t *)realloc(cp, sizeof(uint32_t) * (size_t)cap);
         }
-        cv[n] = jb->seeds[(int64_t)s * p->frontier_size + f];
+        cv[n] = jb->seeds[(int64_t)sl * p->frontier_size + f];
         cp[n] = (uint32_t)f;
         ++n;
     }
@@ -361,10 +362,11 @@ static void run_neighbor(job_t *jb, int s) {
     free(cv); free(cp);
 }
 
-static void run_walk(job_t *jb, int s) {
+static void run_walk(job_t *jb, int sl) {
     const oracle_params *p = jb->p;
     ctx_t *c = &jb->c;
-    int32_t v = jb->seeds[s];
+    const int s = (int)(p->sample_base + sl);
+    int32_t v = jb->seeds[sl];
     int64_t sel[1];
     for (int t = 0; t < p->depth; ++t) {
         int64_t beg = c->rowptr[v], d = c->rowptr[v + 1] - beg;
@@ -376,14 +378,15 @@ static void run_walk(job_t *jb, int s) {
     }
 }
 
-static void run_mdrw(job_t *jb, int s) {
+static void run_mdrw(job_t *jb, int sl) {
     const oracle_params *p = jb->p;
+    const int s = (int)(p->sample_base + sl);
     ctx_t *c = &jb->c;
     int F = p->frontier_size;
     int32_t *f = (int32_t *)malloc(sizeof(int32_t) * (size_t)F);
     float *b = (float *)malloc(sizeof(float) * (size_t)F);
     float *P = (float *)malloc(sizeof(float) * (size_t)F);
-    memcpy(f, jb->seeds + (int64_t)s * F, sizeof(int32_t) * (size_t)F);
+    memcpy(f, jb->seeds + (int64_t)sl * F, sizeof(int32_t) * (size_t)F);
     uint32_t key[2] = {(uint32_t)c->seed, (uint32_t)(c->seed >> 32)};
     for (int t = 0; t < p->depth; ++t) {
         for (int i = 0; i < F; ++i)
@@ -443,7 +446,7 @@ int oracle_run(const int64_t *rowptr, const int32_t *col, const float *weight,
                int32_t *src, int32_t *dst, int32_t *sample, int32_t *depth,
                int64_t cap, int64_t *n_out, int n_threads) {
     (void)E;
-    if (!p || !rowptr || !col || !seeds || !n_out || p->n_samples < 0 ||
+    if (!p || !rowptr || !col || !seeds || !n_out || p->n_samples < 0 || p->sample_base < 0 ||
         p->depth < 0 || p->depth > ORACLE_MAX_DEPTH || p->frontier_size < 1)
         return 1;
     if (p->bias == ORACLE_EDGE_WEIGHT && !weight) return 1;

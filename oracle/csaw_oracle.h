@@ -47,6 +47,7 @@ typedef struct {
     int32_t depth;          /* hops (neighbor), walk length, MDRW steps */
     int32_t fanout[ORACLE_MAX_DEPTH]; /* N per hop (neighbor mode) */
     uint64_t seed;          /* Philox key */
+    int64_t sample_base;    /* id of the first sample (keys and output ids) */
 } oracle_params;
 
 /* Philox4x32-10 (Salmon et al., SC11). */

@@ -210,3 +210,45 @@ def test_batch_jobs_equal_solo_runs(csaw, powerlaw_small, rmat12_pareto):
     hjobs = [csaw.BatchJob(j.params, j.seeds.cpu().numpy(), host=True) for j in jobs]
     for r, s in zip(g.sample_batch(hjobs), solo):
         assert_parity(r, s)
+
+
+@pytest.mark.parametrize("mode,fan", [(0, [6, 4, 2]), (1, None), (2, None)])
+def test_shards_union_equals_full_run(csaw, powerlaw_small, mode, fan):
+    """Three shards (global sample ids via sample_base) give the full job's edges."""
+    import torch
+    from csaw import dist as cdist
+    g = csaw.Graph(powerlaw_small)
+    F = 1 if mode == 1 else 3
+    n, depth = 120, (3 if mode == 0 else 25)
+    seeds = oracle.make_seeds(powerlaw_small.rowptr, n * F, 9)
+    full = csaw.make_params(mode, 1, n, F, (fan or [1])[0], depth, fan, seed=31, schedule=1)
+    ref = g.sample(full, torch.from_numpy(seeds).cuda())
+    parts = []
+    for r in range(3):
+        p, sl = cdist.shard_params(full, r, 3)
+        parts.append([x.cpu().numpy() for x in g.sample(p, torch.from_numpy(seeds[sl]).cuda())])
+    union = [np.concatenate([pp[i] for pp in parts]) for i in range(4)]
+    assert_parity(union, [x.cpu().numpy() for x in ref])
+
+
+@pytest.mark.parametrize("graphs", [1, 0])
+def test_repeated_batches_replay_identically(csaw, powerlaw_small, graphs):
+    """The second identical batch is captured into a CUDA graph, later ones
+    replay it; every repetition returns the same edges (and the same as with
+    graphs off)."""
+    import torch
+    from csaw import _lib
+    g = csaw.Graph(powerlaw_small)
+    g.set_option(_lib.OPT_CUDA_GRAPHS, graphs)
+    sa = torch.from_numpy(oracle.make_seeds(powerlaw_small.rowptr, 400, 1)).cuda()
+    sb = torch.from_numpy(oracle.make_seeds(powerlaw_small.rowptr, 300, 2)).cuda()
+    jobs = [csaw.BatchJob(csaw.make_params(0, 1, 100, 4, 20, 3, [20, 20, 20], seed=5, schedule=1), sa),
+            csaw.BatchJob(csaw.make_params(1, 1, 300, 1, 1, 40, None, seed=6, schedule=1), sb)]
+    outs = []
+    for _ in range(4):
+        outs.append([[x.cpu().numpy() for x in r] for r in g.sample_batch(jobs)])
+    for o in outs[1:]:
+        for a, b in zip(o, outs[0]):
+            assert_parity(a, b)
+    ref = oracle_run(powerlaw_small, 0, 1, 100, 4, 3, [20, 20, 20], 5, sa.cpu().numpy())
+    assert_parity(outs[-1][0], ref)
