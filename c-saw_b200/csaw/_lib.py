@@ -22,7 +22,8 @@ EXPORTS = [
     "csaw_last_error", "csaw_version", "csaw_graph_create", "csaw_graph_destroy",
     "csaw_graph_stats", "csaw_graph_profile", "csaw_graph_kernel_stats", "csaw_make_seeds",
     "csaw_sample", "csaw_sample_host", "csaw_sample_batch", "csaw_sample_noalloc", "csaw_sampler_compat",
-    "csaw_graph_set_option",
+    "csaw_graph_set_option", "csaw_stream_graph_create", "csaw_stream_graph_destroy", "csaw_stream_sample",
+    "csaw_stream_stats",
 ]
 OPT_CUDA_GRAPHS = 1
 
@@ -63,6 +64,12 @@ class Job(ctypes.Structure):
     ]
 
 
+class StreamInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in (
+        "n_partitions", "n_slots", "partition_loads", "partition_hits", "bytes_h2d", "kernel_launches",
+        "host_pinned_in_place")]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int64) for n in (
         "n_vertices", "n_edges", "max_degree", "device_bytes", "workspace_bytes",
@@ -96,6 +103,10 @@ def lib():
     L.csaw_sample_noalloc.argtypes = sig
     L.csaw_sample_batch.argtypes = [p, ctypes.POINTER(Job), i32, p]
     L.csaw_graph_set_option.argtypes = [p, i32, i64]
+    L.csaw_stream_graph_create.argtypes = [p, i32, p, p, i64, i64, i32, i64, ctypes.POINTER(p)]
+    L.csaw_stream_graph_destroy.argtypes = [p]
+    L.csaw_stream_sample.argtypes = sig
+    L.csaw_stream_stats.argtypes = [p, ctypes.POINTER(StreamInfo)]
     L.csaw_sampler_compat.argtypes = [ctypes.c_char_p, ctypes.c_char_p, i32, i32, i32, i32, i32, i32,
                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
     for name in EXPORTS:

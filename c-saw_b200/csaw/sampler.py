@@ -184,6 +184,60 @@ class Graph:
                 out[2 + with_sample, :k] if with_depth else None)
 
 
+class StreamGraph:
+    """A graph whose adjacency stays in host memory and is paged to the device
+    by partitions of 2^partition_bits vertices (csaw_stream_graph_create);
+    slot_budget_bytes bounds the device memory for resident partitions.  The
+    CSR arrays are kept referenced (they are page-locked in place)."""
+
+    def __init__(self, csr, partition_bits=20, slot_budget_bytes=32 << 30, rowptr64=None):
+        L = lib()
+        if rowptr64 is None:
+            rowptr64 = csr.n_edges >= 2**31
+        self.rowptr_host = csr.rowptr if rowptr64 else csr.rowptr32()
+        self.csr = csr
+        h = ctypes.c_void_p()
+        w = None if csr.weight is None else csr.weight.ctypes.data_as(ctypes.c_void_p)
+        check(L.csaw_stream_graph_create(self.rowptr_host.ctypes.data_as(ctypes.c_void_p), int(rowptr64),
+                                         csr.col.ctypes.data_as(ctypes.c_void_p), w, csr.n_vertices, csr.n_edges,
+                                         partition_bits, slot_budget_bytes, ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().csaw_stream_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self):
+        s = _lib.StreamInfo()
+        check(lib().csaw_stream_stats(self.h, ctypes.byref(s)))
+        return {f: getattr(s, f) for f, _ in _lib.StreamInfo._fields_}
+
+    def sample(self, params, seeds, capacity=None, out=None, with_sample=True, with_depth=True, stream=None):
+        torch = _torch()
+        if capacity is None:
+            capacity = edge_bound(params)
+        if out is None:
+            out = torch.empty((2 + with_sample + with_depth, max(capacity, 1)), dtype=torch.int32, device="cuda")
+        ptrs = [ctypes.c_void_p(out[i].data_ptr()) for i in range(out.shape[0])]
+        n = ctypes.c_int64()
+        st = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        seeds = seeds.to(device="cuda", dtype=torch.int32).contiguous()
+        check(lib().csaw_stream_sample(self.h, ctypes.byref(params), ctypes.c_void_p(seeds.data_ptr()), ptrs[0],
+                                       ptrs[1], ptrs[2] if with_sample else None,
+                                       ptrs[2 + with_sample] if with_depth else None, capacity, ctypes.byref(n),
+                                       ctypes.c_void_p(st)))
+        k = n.value
+        return (out[0, :k], out[1, :k], out[2, :k] if with_sample else None,
+                out[2 + with_sample, :k] if with_depth else None)
+
+
 class BatchJob:
     """One job of Graph.sample_batch: params, seeds and output buffers (device
     tensors, or numpy arrays with host=True)."""
@@ -246,4 +300,4 @@ def Sampler(beg, csr, n_blocks, n_threads, n_subgraph, FrontierSize, NeighborSiz
     return out
 
 
-__all__ = ["Graph", "Sampler", "Arguments", "BatchJob", "make_params", "edge_bound", "CsawError"]
+__all__ = ["Graph", "StreamGraph", "Sampler", "Arguments", "BatchJob", "make_params", "edge_bound", "CsawError"]

@@ -197,6 +197,35 @@ int csaw_sample_noalloc(csaw_graph g, const csaw_params *p, const int32_t *seeds
                         int32_t *out_depth, int64_t capacity, int64_t *n_out, void *stream);
 
 /*
+ * Streaming (partitioned) sampling for graphs whose adjacency exceeds the
+ * device budget (replaces streaming/streaming_sampling.cu:427-728).  The row
+ * offsets are copied to the device; col (and weights) stay in the caller's
+ * host arrays, page-locked in place, and are paged in as partitions of
+ * 2^partition_bits vertices into as many device slots as slot_budget_bytes
+ * allows (at least 2).  The host arrays must outlive the handle.
+ * csaw_stream_sample runs neighbor sampling or walks (MDRW is not offered;
+ * walk Depth <= 64) and gives exactly the csaw_sample output.
+ */
+typedef struct csaw_stream_graph_s *csaw_stream_graph;
+typedef struct {
+    int64_t n_partitions, n_slots;
+    int64_t partition_loads;   /* partitions copied to the device */
+    int64_t partition_hits;    /* partition uses served by a resident slot */
+    int64_t bytes_h2d;         /* adjacency bytes copied */
+    int64_t kernel_launches;
+    int64_t host_pinned_in_place; /* bit 0: col, bit 1: weights registered */
+} csaw_stream_info;
+int csaw_stream_graph_create(const void *rowptr, int rowptr_is_64, const int32_t *col,
+                             const float *weights, int64_t n_vertices, int64_t n_edges,
+                             int partition_bits, int64_t slot_budget_bytes,
+                             csaw_stream_graph *out);
+int csaw_stream_graph_destroy(csaw_stream_graph g);
+int csaw_stream_sample(csaw_stream_graph g, const csaw_params *p, const int32_t *seeds,
+                       int32_t *out_src, int32_t *out_dst, int32_t *out_sample,
+                       int32_t *out_depth, int64_t capacity, int64_t *n_out, void *stream);
+int csaw_stream_stats(csaw_stream_graph g, csaw_stream_info *out);
+
+/*
  * Reference-compatible entry (Sampler, non-stream/main.cu:196-308): loads
  * int64 beg.bin / csr.bin (graph.hpp:18-34 format), draws FrontierSize seeds
  * per sample, runs neighbor sampling (FrontierSize == 1) or MDRW

@@ -1,0 +1,73 @@
+"""Streaming (partitioned) sampling: adjacency in page-locked host memory,
+paged into a few device slots; the output must equal the in-memory path and
+the oracle exactly, whatever the partition order and evictions."""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import sort_edges
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def csaw():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("gpu test without a CUDA device")
+    import csaw as c
+    c.lib()
+    return c
+
+
+def _same(a, b):
+    sa, sb = sort_edges(*a), sort_edges(*b)
+    assert sa.shape == sb.shape and np.array_equal(sa, sb)
+
+
+@pytest.mark.parametrize("bias", [0, 1, 2, 3])
+@pytest.mark.parametrize("pbits,slots", [(8, 2), (6, 3), (10, 100)])
+def test_stream_neighbor_equals_in_memory(csaw, rmat12_pareto, bias, pbits, slots):
+    import torch
+    g = rmat12_pareto
+    per_slot = int(np.max(g.rowptr[np.minimum(np.arange(0, g.n_vertices + (1 << pbits), 1 << pbits), g.n_vertices)][1:]
+                          - g.rowptr[np.minimum(np.arange(0, g.n_vertices + (1 << pbits), 1 << pbits), g.n_vertices)][:-1]))
+    budget = slots * per_slot * 8
+    sg = csaw.StreamGraph(g, partition_bits=pbits, slot_budget_bytes=budget)
+    G = csaw.Graph(g)
+    seeds = oracle.make_seeds(g.rowptr, 200 * 2, 3 + bias)
+    p = csaw.make_params(0, bias, 200, 2, 10, 3, [10, 5, 3], seed=41 + bias)
+    a = [x.cpu().numpy() for x in sg.sample(p, torch.from_numpy(seeds).cuda())]
+    b = [x.cpu().numpy() for x in G.sample(p, torch.from_numpy(seeds).cuda())]
+    _same(a, b)
+    info = sg.info()
+    assert info["n_slots"] == min(slots, info["n_partitions"])
+    if info["n_slots"] < info["n_partitions"]:
+        assert info["partition_loads"] > info["n_slots"]     # evictions and reloads happened
+    assert info["bytes_h2d"] > 0 and info["host_pinned_in_place"] & 1
+    if bias in (0, 1, 2):
+        _same(a, oracle.run(g.rowptr, g.col, g.weight, seeds, 0, bias, 200, 2, 3, [10, 5, 3], seed=41 + bias,
+                            n_threads=8))
+
+
+@pytest.mark.parametrize("bias", [0, 1, 2])
+def test_stream_walk_equals_in_memory(csaw, powerlaw_small, bias):
+    import torch
+    g = powerlaw_small
+    sg = csaw.StreamGraph(g, partition_bits=11, slot_budget_bytes=4 * 8 * int(np.diff(g.rowptr[::2048]).max() + 2048))
+    seeds = oracle.make_seeds(g.rowptr, 300, 6)
+    p = csaw.make_params(1, bias, 300, 1, 1, 40, None, seed=9)
+    a = [x.cpu().numpy() for x in sg.sample(p, torch.from_numpy(seeds).cuda())]
+    b = oracle.run(g.rowptr, g.col, g.weight, seeds, 1, bias, 300, 1, 40, seed=9, n_threads=8)
+    _same(a, b)
+
+
+def test_stream_rejects_mdrw_and_tiny_budget(csaw, powerlaw_small):
+    import torch
+    g = powerlaw_small
+    with pytest.raises(csaw.CsawError):
+        csaw.StreamGraph(g, partition_bits=11, slot_budget_bytes=16)
+    sg = csaw.StreamGraph(g, partition_bits=11, slot_budget_bytes=1 << 26)
+    p = csaw.make_params(2, 1, 10, 4, 1, 5, None, seed=1)
+    with pytest.raises(csaw.CsawError):
+        sg.sample(p, torch.zeros(40, dtype=torch.int32, device="cuda"))
