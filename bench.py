@@ -12,9 +12,12 @@ e2e = the same metric through the host-buffer entry points (csaw_sample_host
 for the plain form, csaw_sample_batch with host buffers for the batched form):
 host seeds in, host edge list (src, dst, sample) out, copies inside the timed
 region.
-Both forms run: "plain" (one warp per item, level by level, gathered degree
-bias) and "batched" (the default product path); value is the batched form,
-forms.plain the plain one, on the same graph, seeds and keys.
+Three forms run on the same graph, seeds and keys: "plain" (one warp per
+item, level by level, gathered degree bias, jobs one after the other),
+"batched" (load-balanced expansion, neighbor records, concurrent jobs,
+CUDA-graph replay, degree-rule granularity) and "learned" (batched with the
+learned granularity scheduler, trained on the GPU on profiles recorded on a
+few warm-up steps).  value is the last form of --forms (default: learned).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl csaw|reference]
 
@@ -178,6 +181,50 @@ def cpu_baseline(g):
             "sample": f"{reps} x ({na} of 4000 samples of (a) + {nb} of 4000 walks of (b)), {dt:.1f} s"}
 
 
+def learned_gain(args):
+    """Degree rule vs learned granularity on a heavy-tailed graph: R-MAT
+    (a=.6, b=.2, c=.15) scale 20, edge factor 16, Pareto(1.5) weights,
+    edge-weight-biased sampling, 8192 samples, F 8, N 10, D 3 (the shape of
+    the scale-25 learned-scheduler configuration at 1/32 of its vertices).
+    Prints one JSON line with both times; identical edges are asserted."""
+    import torch
+    import csaw
+    from csaw import graphgen
+    g = graphgen.rmat(20, 16, a=0.6, b=0.2, c=0.15, seed=25, weight="pareto:1.5")
+    G = csaw.Graph(g)
+    seeds = G.make_seeds(8192 * 8, 0x25)
+    out = torch.empty((3, 8192 * 8 * (10 + 100 + 1000)), dtype=torch.int32, device="cuda")
+    res = {}
+    for form, sch in (("batched", csaw.SCHED_BATCHED), ("learned", csaw.SCHED_LEARNED)):
+        p = csaw.make_params(0, 2, 8192, 8, 10, 3, seed=0x25, schedule=sch)
+        job = [csaw.BatchJob(p, seeds, out.shape[1], out, with_depth=False)]
+        if form == "learned":
+            G.sched_record(400_000)
+            for _ in range(3):
+                G.sample_batch(job)
+            res["train_loss"] = G.sched_train(epochs=400, lr=3e-3, seed=1)
+        for _ in range(args.warmup):
+            G.sample_batch(job)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        n = 0
+        for _ in range(args.steps):
+            n += G.sample_batch(job)[0][0].numel()
+        e1.record()
+        torch.cuda.synchronize()
+        res[form] = {"ms_per_step": e0.elapsed_time(e1) / args.steps, "edges_per_step": n / args.steps}
+        G.profile(True)
+        G.sample_batch(job)
+        res[form]["cta_items"] = G.kernel_stats("heavy")["items"]
+        res[form]["warp_items"] = G.kernel_stats("select")["items"]
+        G.profile(False)
+    assert res["batched"]["edges_per_step"] == res["learned"]["edges_per_step"]
+    res["learned_speedup"] = res["batched"]["ms_per_step"] / res["learned"]["ms_per_step"]
+    res["graph"] = {"V": g.n_vertices, "E": g.n_edges, "max_degree": int(np.diff(g.rowptr).max())}
+    print(json.dumps({"learned_gain": res}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -185,13 +232,18 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="csaw", choices=["csaw", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--forms", default="plain,batched",
+    ap.add_argument("--learned-gain", action="store_true",
+                    help="time the degree rule vs the learned scheduler on a heavy-tailed R-MAT graph instead")
+    ap.add_argument("--forms", default="plain,batched,learned",
                     help="forms to time; the last one is reported as value (profiling runs use one form)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.learned_gain:
+        learned_gain(args)
         return
 
     import torch
@@ -212,15 +264,17 @@ def main():
     # replicas (weak scaling): same job shape, rank-disjoint global sample ids
     params = {f: (cdist.replica_params(csaw.make_params(**WORK_A, seed=SEED_A, schedule=sch), rank),
                   cdist.replica_params(csaw.make_params(**WORK_B, seed=SEED_B, schedule=sch), rank))
-              for f, sch in (("plain", csaw.SCHED_PLAIN), ("batched", csaw.SCHED_BATCHED))}
+              for f, sch in (("plain", csaw.SCHED_PLAIN), ("batched", csaw.SCHED_BATCHED),
+                             ("learned", csaw.SCHED_LEARNED))}
     pa, pb = params["batched"]
     cap_a, cap_b = csaw.edge_bound(pa), csaw.edge_bound(pb)
     out_a = torch.empty((3, cap_a), dtype=torch.int32, device="cuda")
     out_b = torch.empty((3, cap_b), dtype=torch.int32, device="cuda")
     flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.int32, device="cuda")
 
-    batch_jobs = [csaw.BatchJob(params["batched"][0], seeds_a, cap_a, out_a, with_depth=False),
-                  csaw.BatchJob(params["batched"][1], seeds_b, cap_b, out_b, with_depth=False)]
+    batch_jobs = {f: [csaw.BatchJob(params[f][0], seeds_a, cap_a, out_a, with_depth=False),
+                      csaw.BatchJob(params[f][1], seeds_b, cap_b, out_b, with_depth=False)]
+                  for f in ("batched", "learned")}
 
     def step(form):
         if form == "plain":   # one job after the other, as the reference runs them
@@ -228,7 +282,7 @@ def main():
             a = G.sample(qa, seeds_a, capacity=cap_a, out=out_a, with_depth=False)
             b = G.sample(qb, seeds_b, capacity=cap_b, out=out_b, with_depth=False)
             return a[0].numel() + b[0].numel()
-        res = G.sample_batch(batch_jobs)   # both workloads as one batch
+        res = G.sample_batch(batch_jobs[form])   # both workloads as one batch
         return res[0][0].numel() + res[1][0].numel()
 
     def barrier():
@@ -265,8 +319,21 @@ def main():
     forms = [f.strip() for f in args.forms.split(",") if f.strip()]
     main_form = forms[-1]
     plain_ms, plain_k = None, {}
+    other = {}
     if "plain" in forms and main_form != "plain":
         plain_edges, plain_ms, plain_k, _, _ = timed("plain", profile=True)
+    if "batched" in forms and main_form != "batched":
+        other["batched"] = timed("batched")[1]
+    sched = None
+    if "learned" in forms:
+        # the learned scheduler: record execution profiles, train on the GPU
+        G.sched_record(400_000)
+        for _ in range(3):
+            step("learned")
+        t0 = time.perf_counter()
+        loss = G.sched_train(epochs=400, lr=3e-3, seed=rank)
+        sched = {"records": G.sched_info()["records"], "train_loss": loss,
+                 "train_s": time.perf_counter() - t0}
     # per-kernel events for the roofline come from a profiled pass of the same
     # steps; the reported value is the unprofiled pass (graph replay allowed)
     _, prof_ms, kstats, _, _ = timed(main_form, profile=True)
@@ -347,6 +414,9 @@ def main():
                 "profiled_pass_ms_per_step": prof_ms / args.steps,
                 "forms": {main_form: value, "plain": all_edges / plain_t if plain_t else None,
                           "speedup_vs_plain": plain_t / t_max if plain_t else None,
+                          **{f: all_edges / (ms_f / 1e3) for f, ms_f in other.items()},
+                          **({"learned_vs_batched": (other["batched"] / ms)} if "batched" in other else {}),
+                          "scheduler": sched,
                           "plain_kernels": {k: v for k, v in plain_k.items() if v["launches"]}},
                 "edges_per_step": all_edges / args.steps / world}
         if not args.no_cpu_baseline:

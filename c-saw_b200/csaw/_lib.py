@@ -13,7 +13,7 @@ OK, ERR_INVALID, ERR_CUDA, ERR_CAPACITY, ERR_NOMEM, ERR_DEVICE = range(6)
 MODE_NEIGHBOR, MODE_WALK, MODE_MDRW = 0, 1, 2
 BIAS_UNBIASED, BIAS_DEGREE, BIAS_EDGE_WEIGHT, BIAS_HOOK = 0, 1, 2, 3
 SCHED_PLAIN, SCHED_BATCHED, SCHED_LEARNED = 0, 1, 2
-GRAPH_DEGREE_BIAS, GRAPH_CDF_CACHE = 1, 2
+GRAPH_DEGREE_BIAS, GRAPH_CDF_CACHE, GRAPH_NO_CDF_CACHE = 1, 2, 4
 MAX_DEPTH = 64
 KERNEL_KINDS = {"expand": 0, "heavy": 1, "walk": 2, "mdrw": 3, "setup": 4, "select": 5}
 
@@ -23,9 +23,12 @@ EXPORTS = [
     "csaw_graph_stats", "csaw_graph_profile", "csaw_graph_kernel_stats", "csaw_make_seeds",
     "csaw_sample", "csaw_sample_host", "csaw_sample_batch", "csaw_sample_noalloc", "csaw_sampler_compat",
     "csaw_graph_set_option", "csaw_stream_graph_create", "csaw_stream_graph_destroy", "csaw_stream_sample",
-    "csaw_stream_stats",
+    "csaw_stream_stats", "csaw_sched_info", "csaw_sched_get_records", "csaw_sched_train", "csaw_sched_get_model", "csaw_sched_set_model",
+    "csaw_mlp_grad_host",
 ]
 OPT_CUDA_GRAPHS = 1
+OPT_SCHED_RECORD = 2
+MLP_NPARAM, MLP_NORM = 1542, 18
 
 
 class CsawError(RuntimeError):
@@ -107,6 +110,13 @@ def lib():
     L.csaw_stream_graph_destroy.argtypes = [p]
     L.csaw_stream_sample.argtypes = sig
     L.csaw_stream_stats.argtypes = [p, ctypes.POINTER(StreamInfo)]
+    PF = ctypes.POINTER(ctypes.c_float)
+    L.csaw_sched_info.argtypes = [p, P64, ctypes.POINTER(ctypes.c_int), PF]
+    L.csaw_sched_train.argtypes = [p, i32, ctypes.c_float, u64, PF]
+    L.csaw_sched_get_records.argtypes = [p, p, i64, P64]
+    L.csaw_sched_get_model.argtypes = [p, p, p]
+    L.csaw_sched_set_model.argtypes = [p, p, p]
+    L.csaw_mlp_grad_host.argtypes = [p, p, p, i32, p, PF]
     L.csaw_sampler_compat.argtypes = [ctypes.c_char_p, ctypes.c_char_p, i32, i32, i32, i32, i32, i32,
                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
     for name in EXPORTS:

@@ -59,15 +59,22 @@ def _torch():
 
 
 class Graph:
-    """A CSR resident on the current CUDA device (csaw_graph_create)."""
+    """A CSR resident on the current CUDA device (csaw_graph_create).
 
-    def __init__(self, csr, rowptr64=None, degree_bias=False, cdf_cache=False):
+    cdf_cache: None builds the per-vertex bias prefix cache when a batched or
+    learned biased job meets a vertex above 512 edges; True builds it for every
+    schedule (the plain one included); False never builds it.
+    """
+
+    def __init__(self, csr, rowptr64=None, degree_bias=False, cdf_cache=None):
         L = lib()
         if rowptr64 is None:
             rowptr64 = csr.n_edges >= 2**31
         self.rowptr_host = csr.rowptr if rowptr64 else csr.rowptr32()
         self.csr = csr
-        flags = (_lib.GRAPH_DEGREE_BIAS if degree_bias else 0) | (_lib.GRAPH_CDF_CACHE if cdf_cache else 0)
+        flags = _lib.GRAPH_DEGREE_BIAS if degree_bias else 0
+        if cdf_cache is not None:
+            flags |= _lib.GRAPH_CDF_CACHE if cdf_cache else _lib.GRAPH_NO_CDF_CACHE
         h = ctypes.c_void_p()
         w = None if csr.weight is None else csr.weight.ctypes.data_as(ctypes.c_void_p)
         check(L.csaw_graph_create(self.rowptr_host.ctypes.data_as(ctypes.c_void_p), int(rowptr64),
@@ -93,6 +100,38 @@ class Graph:
 
     def set_option(self, option, value):
         check(lib().csaw_graph_set_option(self.h, option, int(value)))
+
+    # ---- learned scheduler
+    def sched_record(self, n_records):
+        """Record up to n execution profiles on the next learned-schedule runs."""
+        self.set_option(_lib.OPT_SCHED_RECORD, n_records)
+
+    def sched_info(self):
+        n, t, l = ctypes.c_int64(), ctypes.c_int(), ctypes.c_float()
+        check(lib().csaw_sched_info(self.h, ctypes.byref(n), ctypes.byref(t), ctypes.byref(l)))
+        return {"records": n.value, "trained": bool(t.value), "loss": l.value}
+
+    def sched_records(self, max_n=1 << 20):
+        out = np.zeros(max_n, dtype=PROF_DTYPE)
+        n = ctypes.c_int64()
+        check(lib().csaw_sched_get_records(self.h, out.ctypes.data_as(ctypes.c_void_p), max_n, ctypes.byref(n)))
+        return out[:n.value]
+
+    def sched_train(self, epochs=300, lr=3e-3, seed=0):
+        loss = ctypes.c_float()
+        check(lib().csaw_sched_train(self.h, epochs, lr, seed, ctypes.byref(loss)))
+        return loss.value
+
+    def sched_model(self):
+        w = np.zeros(_lib.MLP_NPARAM, dtype=np.float32)
+        nrm = np.zeros(_lib.MLP_NORM, dtype=np.float32)
+        check(lib().csaw_sched_get_model(self.h, w.ctypes.data_as(ctypes.c_void_p), nrm.ctypes.data_as(ctypes.c_void_p)))
+        return w, nrm
+
+    def sched_set_model(self, w, nrm):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        nrm = np.ascontiguousarray(nrm, dtype=np.float32)
+        check(lib().csaw_sched_set_model(self.h, w.ctypes.data_as(ctypes.c_void_p), nrm.ctypes.data_as(ctypes.c_void_p)))
 
     def profile(self, enable=True):
         check(lib().csaw_graph_profile(self.h, int(enable)))
@@ -182,6 +221,23 @@ class Graph:
         k = n.value
         return (out[0, :k], out[1, :k], out[2, :k] if with_sample else None,
                 out[2 + with_sample, :k] if with_depth else None)
+
+
+PROF_DTYPE = np.dtype([("x", np.float32, 8), ("cls", np.int32), ("cycles", np.float32)])
+
+
+def mlp_grad(params, norm, records):
+    """Mean loss and gradient of the scheduler MLP on `records` (PROF_DTYPE
+    array), computed by the library's GPU kernel."""
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    norm = np.ascontiguousarray(norm, dtype=np.float32)
+    records = np.ascontiguousarray(records, dtype=PROF_DTYPE)
+    grad = np.zeros(_lib.MLP_NPARAM, dtype=np.float32)
+    loss = ctypes.c_float()
+    check(lib().csaw_mlp_grad_host(params.ctypes.data_as(ctypes.c_void_p), norm.ctypes.data_as(ctypes.c_void_p),
+                                   records.ctypes.data_as(ctypes.c_void_p), len(records),
+                                   grad.ctypes.data_as(ctypes.c_void_p), ctypes.byref(loss)))
+    return loss.value, grad
 
 
 class StreamGraph:
@@ -300,4 +356,4 @@ def Sampler(beg, csr, n_blocks, n_threads, n_subgraph, FrontierSize, NeighborSiz
     return out
 
 
-__all__ = ["Graph", "StreamGraph", "Sampler", "Arguments", "BatchJob", "make_params", "edge_bound", "CsawError"]
+__all__ = ["mlp_grad", "PROF_DTYPE", "Graph", "StreamGraph", "Sampler", "Arguments", "BatchJob", "make_params", "edge_bound", "CsawError"]

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <algorithm>
 #include <array>
 #include <map>
 #include <set>
@@ -21,6 +22,7 @@
 #include "csaw.h"
 #include "csaw_internal.h"
 #include "kernels_fast.cuh"
+#include "sched_mlp.cuh"
 
 using namespace csaw;
 
@@ -58,6 +60,8 @@ struct Counters {
     uint32_t nq[2];
     uint32_t n_heavy;
     uint32_t n_sel;
+    uint32_t n_cta[4];
+    uint32_t n_retry;
     int err;
 };
 
@@ -96,10 +100,12 @@ constexpr int MDRW_MAX_F = 4096;
 // Job 0 serves csaw_sample; csaw_sample_batch runs job i on context i, each
 // on its own stream, so independent jobs overlap on the device.
 struct JobCtx {
-    DevBuf q[2][5], heavy, sel, hlist, hscratch, wscratch, seeds_in, out_dev;
+    DevBuf q[2][5], heavy, sel, hlist, hscratch, wscratch, seeds_in, out_dev, cta[4], retry;
     Counters *ctr = nullptr, *hctr = nullptr;
     cudaStream_t stream = nullptr;   // owned (batch jobs); job 0 uses the caller's
     cudaEvent_t done = nullptr;
+    cudaStream_t side = nullptr;     // CTA-granularity pass, concurrent with the warp pass
+    cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 }  // namespace
@@ -115,6 +121,10 @@ struct csaw_graph_s {
     bool ebias_flag = false;   // materialised at creation (visible to every schedule)
     float *cdf = nullptr;
     int cdf_bias = -1;
+    bool cdf_flag = false;        // CSAW_GRAPH_CDF_CACHE: visible to the plain schedule too
+    bool cdf_off = false;         // CSAW_GRAPH_NO_CDF_CACHE
+    int32_t *big_verts = nullptr; // vertices above CDF_BIG (the cache builds them one CTA each)
+    int64_t n_big = 0;
     void *nbr_beg = nullptr;      // per-edge neighbor records (batched schedules)
     int32_t *nbr_deg = nullptr;
     int32_t *nonisolated = nullptr;
@@ -136,6 +146,20 @@ struct csaw_graph_s {
     std::set<std::string> warm;
     std::map<std::string, cudaGraphExec_t> graphs;
     std::map<std::string, int64_t> graph_kernels;   // kernel launches per replay
+    // learned scheduler
+    float2 *vstats = nullptr;         // per-vertex bias statistics
+    int vstats_bias = -1;
+    float *mlp_w = nullptr, *mlp_m = nullptr, *mlp_v = nullptr, *mlp_norm = nullptr, *mlp_grad = nullptr,
+          *mlp_loss = nullptr;
+    __nv_bfloat16 *mlp_wq = nullptr;
+    ProfRec *rec = nullptr;
+    uint32_t *n_rec = nullptr;
+    int64_t max_rec = 0;
+    bool recording = false, trained = false;
+    float last_loss = -1.f;
+    SchedArgs *d_sched = nullptr;     // device copy read by the kernels
+    SchedArgs sched_host{};           // what d_sched holds
+    bool sched_valid = false;
 };
 
 namespace {
@@ -151,9 +175,9 @@ DevGraph dev_view(const csaw_graph_s *g, int schedule = CSAW_SCHED_BATCHED) {
     d.v.n_vertices = g->V;
     d.v.n_edges = g->E;
     d.ebias = (schedule != CSAW_SCHED_PLAIN || g->ebias_flag) ? g->ebias : nullptr;
-    d.cdf = g->cdf;
-    d.cdf_bias = g->cdf_bias;
     const bool fast = schedule != CSAW_SCHED_PLAIN;
+    d.cdf = (fast || g->cdf_flag) ? g->cdf : nullptr;
+    d.cdf_bias = g->cdf_bias;
     d.nbr_beg = fast ? g->nbr_beg : nullptr;
     d.nbr_deg = fast ? g->nbr_deg : nullptr;
     return d;
@@ -229,6 +253,92 @@ int ensure_nbr(csaw_graph_s *g, cudaStream_t st) {
     return 0;
 }
 
+constexpr int64_t CDF_BIG = 4096;   // vertices above are built by one CTA each
+
+// Per-vertex CDF cache: the canonical prefix of every vertex's biases for bias
+// kind BIAS (4E bytes), built on first biased use by a batched schedule on a
+// graph with vertices above the per-warp shared capacity, or when the graph
+// was created with CSAW_GRAPH_CDF_CACHE; never with CSAW_GRAPH_NO_CDF_CACHE.
+template <typename I, int BIAS>
+int ensure_cdf(csaw_graph_s *g, cudaStream_t st) {
+    if (g->cdf && g->cdf_bias == BIAS) return 0;
+    if (g->E == 0 || g->cdf_off) return 0;
+    if (!g->cdf) {
+        ++g_alloc_epoch;
+        CK(cudaMalloc((void **)&g->cdf, sizeof(float) * (size_t)g->E));
+        g->dev_bytes += 4 * g->E;
+    }
+    g->cdf_bias = -1;
+    DevGraph dg = dev_view(g);
+    dg.cdf = nullptr;
+    {
+        LaunchScope ls(g, KK_INIT, st);
+        k_cdf_build<I, BIAS><<<g->sm_count * 8, 256, 0, st>>>(dg, g->cdf, CDF_BIG);
+    }
+    if (g->n_big > 0) {
+        const int64_t stride = ((g->maxdeg >> 5) + 1 + (g->maxdeg >> 10) + 1 + 8 + 63) & ~63ll;
+        float *scratch = nullptr;
+        const int blocks = (int)std::min<int64_t>(g->n_big, g->sm_count * 2);
+        CK(cudaMallocAsync((void **)&scratch, sizeof(float) * stride * blocks, st));
+        LaunchScope ls(g, KK_INIT, st);
+        k_cdf_build_big<I, BIAS><<<blocks, 1024, 0, st>>>(dg, g->cdf, g->big_verts, (int)g->n_big, scratch, stride);
+        CK(cudaFreeAsync(scratch, st));
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    g->cdf_bias = BIAS;
+    ++g_alloc_epoch;
+    return 0;
+}
+
+// Per-vertex bias statistics for the learned scheduler (built once per bias).
+template <typename I, int BIAS>
+int ensure_vstats(csaw_graph_s *g, cudaStream_t st) {
+    if (g->vstats && g->vstats_bias == BIAS) return 0;
+    if (!g->vstats) {
+        ++g_alloc_epoch;
+        CK(cudaMalloc((void **)&g->vstats, sizeof(float2) * (size_t)g->V));
+        g->dev_bytes += 8 * g->V;
+    }
+    DevGraph dg = dev_view(g);
+    LaunchScope ls(g, KK_INIT, st);
+    k_vertex_stats<I, BIAS><<<g->sm_count * 8, 256, 0, st>>>(dg, g->vstats);
+    CK(cudaGetLastError());
+    g->vstats_bias = BIAS;
+    return 0;
+}
+
+// Device SchedArgs for a run of schedule `schedule` with bias `bias`.
+int sched_for(csaw_graph_s *g, int schedule, int bias, int warp_slots, cudaStream_t st, const SchedArgs **out) {
+    *out = nullptr;
+    if (schedule != CSAW_SCHED_LEARNED || bias == CSAW_BIAS_UNBIASED) return 0;
+    SchedArgs h{};
+    h.mode = g->recording ? SCHED_RECORD : (g->trained ? SCHED_MLP : SCHED_THRESHOLD);
+    h.wq = g->mlp_wq;
+    h.norm = g->mlp_norm;
+    h.vstats = g->vstats;
+    h.rec = g->rec;
+    h.n_rec = g->n_rec;
+    h.max_rec = (uint32_t)g->max_rec;
+    h.bias_kind = bias;
+    h.warp_slots = warp_slots;
+    if (!g->d_sched) {
+        ++g_alloc_epoch;
+        CK(cudaMalloc((void **)&g->d_sched, sizeof(SchedArgs)));
+    }
+    // upload only on change (a change also drops cached graphs, so this never
+    // runs inside a stream capture)
+    if (!g->sched_valid || memcmp(&h, &g->sched_host, sizeof(SchedArgs)) != 0) {
+        CK(cudaStreamSynchronize(st));
+        CK(cudaMemcpy(g->d_sched, &h, sizeof(SchedArgs), cudaMemcpyHostToDevice));
+        g->sched_host = h;
+        g->sched_valid = true;
+        ++g_alloc_epoch;
+    }
+    *out = g->d_sched;
+    return 0;
+}
+
 int check_params(const csaw_graph_s *g, const csaw_params *p, int fan[CSAW_MAX_DEPTH]) {
     if (!p) return fail(CSAW_ERR_INVALID, "params is NULL");
     if (p->mode < CSAW_MODE_NEIGHBOR || p->mode > CSAW_MODE_MDRW)
@@ -286,27 +396,40 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
             TRY(ensure(c->q[k][4], sizeof(int32_t) * qcap));
         }
     }
+    const SchedArgs *sched = nullptr;
+    const int sgrid = plain ? 0 : grid_for(k_select_fast<I, BIAS>, FAST_THREADS, 0, g->sm_count);
+    if (BIASED && ((!plain && g->maxdeg > WF) || g->cdf_flag)) TRY((ensure_cdf<I, BIAS>(g, st)));
+    const bool cached = BIASED && g->cdf && g->cdf_bias == BIAS && (!plain || g->cdf_flag);
     if (!plain) {
         TRY(ensure_nbr(g, st));
         TRY(ensure(c->sel, sizeof(SelEntry) * qcap));
-        TRY(ensure(c->hlist, sizeof(SelEntry) * qcap));
+        if (cached && g->maxdeg > WF) TRY(ensure(c->retry, sizeof(SelEntry) * qcap));
+        if (p->schedule == CSAW_SCHED_LEARNED && BIASED) TRY((ensure_vstats<I, BIAS>(g, st)));
+        TRY(sched_for(g, p->schedule, BIAS, sgrid * (FAST_THREADS / 32), st, &sched));
+        for (int k = 0; k < 4; ++k)
+            if (sched || k == 1) TRY(ensure(c->cta[k], sizeof(SelEntry) * qcap));
     }
     const int64_t smem_cap = plain ? WBUF : WF;
     int hblocks = 0;
     int64_t hstride = 0;
-    if (BIASED && g->maxdeg > smem_cap && !(g->cdf && g->cdf_bias == BIAS)) {
+    int cta_grid[4] = {0, 0, 0, 0};
+    if (BIASED && (g->maxdeg > smem_cap || sched)) {
         TRY(ensure(c->heavy, sizeof(uint32_t) * qcap));
         hstride = g->maxdeg + 2 * ((g->maxdeg >> 5) + 1) + (g->maxdeg >> 10) + 1 + 8;
         hstride = (hstride + 63) & ~63ll;
         hblocks = g->sm_count * 2;
-        while (hblocks > 1 && (int64_t)hblocks * hstride * 4 > SCRATCH_BUDGET) hblocks /= 2;
+        const int64_t cap_blocks = std::max<int64_t>(1, SCRATCH_BUDGET / (hstride * 4));
+        for (int k = 0; k < 4; ++k) {   // fill the GPU at each CTA width, within the scratch budget
+            cta_grid[k] = (int)std::min<int64_t>(grid_for(k_expand_heavy<I, BIAS>, 128 << k, 0, g->sm_count), cap_blocks);
+            hblocks = std::max(hblocks, cta_grid[k]);
+        }
+        hblocks = (int)std::min<int64_t>(hblocks, cap_blocks);
         TRY(ensure(c->hscratch, sizeof(float) * hstride * hblocks));
     }
     const DevGraph dg = dev_view(g, p->schedule);
     const uint64_t seed = p->seed;
     const int grid = plain ? grid_for(k_expand_warp<I, BIAS>, EXPAND_THREADS, 0, g->sm_count)
                            : grid_for(k_coop_fast<I, BIAS>, FAST_THREADS, 0, g->sm_count);
-    const int sgrid = plain ? 0 : grid_for(k_select_fast<I, BIAS>, FAST_THREADS, 0, g->sm_count);
     for (int64_t s0 = 0; s0 < S; s0 += B) {
         const int64_t nb = (S - s0 < B) ? S - s0 : B;
         const uint32_t n0 = (uint32_t)(nb * F);
@@ -325,7 +448,7 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
         for (int l = 0; l < D; ++l) {
             const int cur = l & 1, nxt = cur ^ 1;
             CK(cudaMemsetAsync(&c->ctr->nq[nxt], 0, sizeof(uint32_t), st));
-            CK(cudaMemsetAsync(&c->ctr->n_heavy, 0, 2 * sizeof(uint32_t), st));  // n_heavy, n_sel
+            CK(cudaMemsetAsync(&c->ctr->n_heavy, 0, 7 * sizeof(uint32_t), st));  // n_heavy, n_sel, n_cta[4], n_retry
             LevelArgs a;
             a.in_v = (const int32_t *)c->q[cur][0].p;
             a.in_s = (const int32_t *)c->q[cur][1].p;
@@ -343,7 +466,12 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
             a.n_heavy = &c->ctr->n_heavy;
             a.sel_list = plain ? nullptr : (SelEntry *)c->sel.p;
             a.n_sel = &c->ctr->n_sel;
-            a.heavy_list = plain ? nullptr : (SelEntry *)c->hlist.p;
+            a.heavy_list = nullptr;
+            for (int k = 0; k < 4; ++k) a.cta_list[k] = (SelEntry *)c->cta[k].p;
+            a.n_cta = c->ctr->n_cta;
+            a.sched = sched;
+            a.retry_list = (SelEntry *)c->retry.p;
+            a.n_retry = &c->ctr->n_retry;
             a.heavy_scratch = (float *)c->hscratch.p;
             a.heavy_stride = hstride;
             a.o_src = o.src;
@@ -365,14 +493,42 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
                 if (plain) k_expand_warp<I, BIAS><<<grid, EXPAND_THREADS, 0, st>>>(dg, a);
                 else k_coop_fast<I, BIAS><<<grid, FAST_THREADS, 0, st>>>(dg, a);
             }
+            const bool side = hblocks && !plain && (sched || !cached);
+            if (side) {
+                // CTA-granularity items on the side stream, concurrent with the
+                // warp-granularity pass (disjoint lists, reserved output slots);
+                // one launch per CTA width that can hold items (degree rule: 256)
+                CK(cudaEventRecord(c->fork, st));
+                CK(cudaStreamWaitEvent(c->side, c->fork, 0));
+                for (int k = 0; k < 4; ++k) {
+                    if (!sched && k != 1) continue;
+                    LevelArgs ak = a;
+                    ak.heavy_list = (SelEntry *)c->cta[k].p;
+                    ak.n_heavy = &c->ctr->n_cta[k];
+                    ak.cta_class = k;
+                    LaunchScope ls(g, KK_HEAVY, c->side);
+                    k_expand_heavy<I, BIAS><<<cta_grid[k], 128 << k, 0, c->side>>>(dg, ak);
+                }
+                CK(cudaEventRecord(c->join, c->side));
+            }
             if (!plain) {
                 LaunchScope ls(g, KK_SELECT, st);
                 k_select_fast<I, BIAS><<<sgrid, FAST_THREADS, 0, st>>>(dg, a);
             }
-            if (hblocks) {
+            if (hblocks && plain) {
                 LaunchScope ls(g, KK_HEAVY, st);
                 k_expand_heavy<I, BIAS><<<hblocks, HEAVY_THREADS, 0, st>>>(dg, a);
             }
+            if (!plain && cached && g->maxdeg > WF) {
+                // cached hubs the warp pass could not rebuild in shared memory
+                LevelArgs ar = a;
+                ar.heavy_list = (SelEntry *)c->retry.p;
+                ar.n_heavy = &c->ctr->n_retry;
+                ar.cta_class = 1;
+                LaunchScope ls(g, KK_HEAVY, st);
+                k_expand_heavy<I, BIAS><<<cta_grid[1], 256, 0, st>>>(dg, ar);
+            }
+            if (side) CK(cudaStreamWaitEvent(st, c->join, 0));
         }
     }
     CK(cudaGetLastError());
@@ -384,6 +540,7 @@ int run_walk_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int32_t *
                cudaStream_t st) {
     const bool plain = p->schedule == CSAW_SCHED_PLAIN;
     if (!plain) TRY(ensure_nbr(g, st));
+    if (BIAS != CSAW_BIAS_UNBIASED && ((!plain && g->maxdeg > WF) || g->cdf_flag)) TRY((ensure_cdf<I, BIAS>(g, st)));
     const DevGraph dg = dev_view(g, p->schedule);
     WalkArgs a{};
     a.seeds = seeds;
@@ -494,6 +651,9 @@ int new_job(JobCtx **out, bool own_stream) {
     if (e == cudaSuccess) e = cudaMallocHost((void **)&c->hctr, sizeof(Counters));
     if (e == cudaSuccess && own_stream) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         cudaGetLastError();
         cudaFree(c->ctr);
@@ -509,12 +669,16 @@ void free_job(JobCtx *c) {
     if (!c) return;
     for (auto &qq : c->q)
         for (auto &b : qq) cudaFree(b.p);
-    for (DevBuf *b : {&c->heavy, &c->sel, &c->hlist, &c->hscratch, &c->wscratch, &c->seeds_in, &c->out_dev})
+    for (DevBuf *b : {&c->heavy, &c->sel, &c->hlist, &c->hscratch, &c->wscratch, &c->seeds_in, &c->out_dev, &c->cta[0],
+                      &c->cta[1], &c->cta[2], &c->cta[3], &c->retry})
         cudaFree(b->p);
     cudaFree(c->ctr);
     if (c->hctr) cudaFreeHost(c->hctr);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->done) cudaEventDestroy(c->done);
+    if (c->side) cudaStreamDestroy(c->side);
+    if (c->fork) cudaEventDestroy(c->fork);
+    if (c->join) cudaEventDestroy(c->join);
     delete c;
 }
 
@@ -522,7 +686,8 @@ int64_t job_workspace(const JobCtx *c) {
     int64_t ws = 0;
     for (auto &qq : c->q)
         for (auto &b : qq) ws += (int64_t)b.n;
-    for (const DevBuf *b : {&c->heavy, &c->sel, &c->hlist, &c->hscratch, &c->wscratch, &c->seeds_in, &c->out_dev})
+    for (const DevBuf *b : {&c->heavy, &c->sel, &c->hlist, &c->hscratch, &c->wscratch, &c->seeds_in, &c->out_dev,
+                            &c->cta[0], &c->cta[1], &c->cta[2], &c->cta[3], &c->retry})
         ws += (int64_t)b->n;
     return ws;
 }
@@ -631,6 +796,9 @@ extern "C" int csaw_graph_create(const void *rowptr, int rowptr_is_64, const int
         if (d > 0) non.push_back((int32_t)v);
     }
     n_non = (int64_t)non.size();
+    std::vector<int32_t> big;
+    for (int64_t v = 0; v < n_vertices; ++v)
+        if (rp(v + 1) - rp(v) > CDF_BIG) big.push_back((int32_t)v);
     for (int64_t e = 0; e < n_edges; ++e)
         if (col[e] < 0 || col[e] >= n_vertices) return fail(CSAW_ERR_INVALID, "col entry out of range");
     if (weights)
@@ -670,6 +838,13 @@ extern "C" int csaw_graph_create(const void *rowptr, int rowptr_is_64, const int
             CKG(cudaMemcpy(g->weight, weights, sizeof(float) * (size_t)n_edges, cudaMemcpyHostToDevice));
         g->dev_bytes += 4 * n_edges;
     }
+    g->cdf_off = (flags & CSAW_GRAPH_NO_CDF_CACHE) != 0;
+    g->cdf_flag = !g->cdf_off && (flags & CSAW_GRAPH_CDF_CACHE) != 0;
+    g->n_big = (int64_t)big.size();
+    if (!big.empty()) {
+        CKG(cudaMalloc((void **)&g->big_verts, sizeof(int32_t) * big.size()));
+        CKG(cudaMemcpy(g->big_verts, big.data(), sizeof(int32_t) * big.size(), cudaMemcpyHostToDevice));
+    }
     CKG(cudaMalloc((void **)&g->nonisolated, sizeof(int32_t) * (size_t)(n_non > 0 ? n_non : 1)));
     if (n_non > 0)
         CKG(cudaMemcpy(g->nonisolated, non.data(), sizeof(int32_t) * (size_t)n_non, cudaMemcpyHostToDevice));
@@ -705,11 +880,16 @@ extern "C" int csaw_graph_destroy(csaw_graph g) {
     cudaFree(g->weight);
     cudaFree(g->ebias);
     cudaFree(g->cdf);
+    cudaFree(g->big_verts);
     cudaFree(g->nbr_beg);
     cudaFree(g->nbr_deg);
     cudaFree(g->nonisolated);
     for (auto &kv : g->graphs) cudaGraphExecDestroy(kv.second);
     for (JobCtx *c : g->jobs) free_job(c);
+    for (void *q : {(void *)g->vstats, (void *)g->mlp_w, (void *)g->mlp_m, (void *)g->mlp_v, (void *)g->mlp_norm,
+                    (void *)g->mlp_grad, (void *)g->mlp_loss, (void *)g->mlp_wq, (void *)g->rec, (void *)g->n_rec,
+                    (void *)g->d_sched})
+        cudaFree(q);
     for (auto &pe : g->pending) {
         cudaEventDestroy(pe.second.first);
         cudaEventDestroy(pe.second.second);
@@ -961,15 +1141,172 @@ extern "C" int csaw_sample_batch(csaw_graph g, csaw_job *jobs, int n_jobs, void 
     return first_rc;
 }
 
+static int ensure_mlp(csaw_graph_s *g) {
+    if (g->mlp_w) return 0;
+    ++g_alloc_epoch;
+    CK(cudaMalloc((void **)&g->mlp_w, sizeof(float) * MLP_NPARAM));
+    CK(cudaMalloc((void **)&g->mlp_m, sizeof(float) * MLP_NPARAM));
+    CK(cudaMalloc((void **)&g->mlp_v, sizeof(float) * MLP_NPARAM));
+    CK(cudaMalloc((void **)&g->mlp_grad, sizeof(float) * MLP_NPARAM));
+    CK(cudaMalloc((void **)&g->mlp_norm, sizeof(float) * MLP_NORM));
+    CK(cudaMalloc((void **)&g->mlp_loss, sizeof(float)));
+    CK(cudaMalloc((void **)&g->mlp_wq, sizeof(__nv_bfloat16) * MLP_NPARAM));
+    CK(cudaMalloc((void **)&g->n_rec, sizeof(uint32_t)));
+    CK(cudaMemset(g->n_rec, 0, sizeof(uint32_t)));
+    return 0;
+}
+
 extern "C" int csaw_graph_set_option(csaw_graph g, int option, int64_t value) {
     if (!g) return fail(CSAW_ERR_INVALID, "graph is NULL");
+    CK(cudaSetDevice(g->device));
     switch (option) {
         case CSAW_OPT_CUDA_GRAPHS:
             g->use_graphs = value != 0;
             return 0;
+        case CSAW_OPT_SCHED_RECORD:
+            if (value < 0) return fail(CSAW_ERR_INVALID, "record capacity < 0");
+            TRY(ensure_mlp(g));
+            if (value > g->max_rec) {
+                ++g_alloc_epoch;
+                cudaFree(g->rec);
+                g->rec = nullptr;
+                CK(cudaMalloc((void **)&g->rec, sizeof(ProfRec) * (size_t)value));
+                g->max_rec = value;
+            }
+            if (value > 0) CK(cudaMemset(g->n_rec, 0, sizeof(uint32_t)));
+            g->recording = value > 0;
+            ++g_alloc_epoch;   // launch sets differ by mode: drop cached graphs
+            return 0;
         default:
             return fail(CSAW_ERR_INVALID, "unknown option");
     }
+}
+
+extern "C" int csaw_sched_info(csaw_graph g, int64_t *n_records, int *trained, float *last_loss) {
+    if (!g) return fail(CSAW_ERR_INVALID, "graph is NULL");
+    uint32_t n = 0;
+    if (g->n_rec) CK(cudaMemcpy(&n, g->n_rec, sizeof(n), cudaMemcpyDeviceToHost));
+    if (n_records) *n_records = std::min<int64_t>(n, g->max_rec);
+    if (trained) *trained = g->trained ? 1 : 0;
+    if (last_loss) *last_loss = g->last_loss;
+    return 0;
+}
+
+// Full-batch Adam on the recorded profiles; initial weights are He-scaled
+// uniform from a 64-bit LCG keyed by `seed`.
+extern "C" int csaw_sched_train(csaw_graph g, int epochs, float lr, uint64_t seed, float *final_loss) {
+    if (!g) return fail(CSAW_ERR_INVALID, "graph is NULL");
+    if (epochs < 1 || !(lr > 0.f)) return fail(CSAW_ERR_INVALID, "epochs >= 1 and lr > 0 required");
+    CK(cudaSetDevice(g->device));
+    TRY(ensure_mlp(g));
+    int64_t n = 0;
+    TRY(csaw_sched_info(g, &n, nullptr, nullptr));
+    if (n < 16) return fail(CSAW_ERR_INVALID, "fewer than 16 recorded profiles: run the learned schedule with "
+                                              "CSAW_OPT_SCHED_RECORD first");
+    std::vector<float> w(MLP_NPARAM, 0.f);
+    uint64_t st = seed * 6364136223846793005ull + 1442695040888963407ull;
+    auto uni = [&]() {
+        st = st * 6364136223846793005ull + 1442695040888963407ull;
+        return (float)((st >> 40) * (1.0 / 16777216.0)) * 2.f - 1.f;
+    };
+    for (int i = 0; i < MLP_H * MLP_IN; ++i) w[MLP_W1 + i] = uni() * sqrtf(6.f / MLP_IN);
+    for (int i = 0; i < MLP_H * MLP_H; ++i) w[MLP_W2 + i] = uni() * sqrtf(6.f / MLP_H);
+    for (int i = 0; i < MLP_OUT * MLP_H; ++i) w[MLP_W3 + i] = uni() * sqrtf(3.f / MLP_H);
+    CK(cudaMemcpy(g->mlp_w, w.data(), sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice));
+    CK(cudaMemset(g->mlp_m, 0, sizeof(float) * MLP_NPARAM));
+    CK(cudaMemset(g->mlp_v, 0, sizeof(float) * MLP_NPARAM));
+    k_mlp_norm<<<1, 1024>>>(g->rec, (int)n, g->mlp_norm);
+    const int gb = (int)std::min<int64_t>(g->sm_count * 2, (n + MLP_GRAD_THREADS - 1) / MLP_GRAD_THREADS);
+    for (int e = 1; e <= epochs; ++e) {
+        cudaMemsetAsync(g->mlp_grad, 0, sizeof(float) * MLP_NPARAM);
+        k_mlp_grad<<<gb, MLP_GRAD_THREADS>>>(g->mlp_w, g->mlp_norm, g->rec, (int)n, g->mlp_grad, g->mlp_loss);
+        k_mlp_adam<<<(MLP_NPARAM + 255) / 256, 256>>>(g->mlp_w, g->mlp_grad, g->mlp_m, g->mlp_v, lr, e, (int)n);
+    }
+    cudaMemsetAsync(g->mlp_grad, 0, sizeof(float) * MLP_NPARAM);
+    cudaMemsetAsync(g->mlp_loss, 0, sizeof(float));
+    k_mlp_grad<<<gb, MLP_GRAD_THREADS>>>(g->mlp_w, g->mlp_norm, g->rec, (int)n, g->mlp_grad, g->mlp_loss);
+    k_mlp_to_bf16<<<(MLP_NPARAM + 255) / 256, 256>>>(g->mlp_w, g->mlp_wq);
+    g->launches += 2 * epochs + 3;
+    CK(cudaGetLastError());
+    float loss = 0.f;
+    CK(cudaMemcpy(&loss, g->mlp_loss, sizeof(float), cudaMemcpyDeviceToHost));
+    loss /= (float)n;
+    g->last_loss = loss;
+    g->trained = true;
+    g->recording = false;
+    ++g_alloc_epoch;
+    if (final_loss) *final_loss = loss;
+    return 0;
+}
+
+extern "C" int csaw_sched_get_records(csaw_graph g, void *out, int64_t max_n, int64_t *n) {
+    if (!g || !n || (max_n > 0 && !out)) return fail(CSAW_ERR_INVALID, "bad arguments");
+    int64_t have = 0;
+    TRY(csaw_sched_info(g, &have, nullptr, nullptr));
+    *n = std::min(have, max_n);
+    if (*n > 0) CK(cudaMemcpy(out, g->rec, sizeof(ProfRec) * (size_t)*n, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+extern "C" int csaw_sched_get_model(csaw_graph g, float *params, float *norm) {
+    if (!g || !g->trained) return fail(CSAW_ERR_INVALID, "no trained model");
+    if (params) CK(cudaMemcpy(params, g->mlp_w, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost));
+    if (norm) CK(cudaMemcpy(norm, g->mlp_norm, sizeof(float) * MLP_NORM, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+extern "C" int csaw_sched_set_model(csaw_graph g, const float *params, const float *norm) {
+    if (!g || !params || !norm) return fail(CSAW_ERR_INVALID, "NULL argument");
+    CK(cudaSetDevice(g->device));
+    TRY(ensure_mlp(g));
+    CK(cudaMemcpy(g->mlp_w, params, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(g->mlp_norm, norm, sizeof(float) * MLP_NORM, cudaMemcpyHostToDevice));
+    k_mlp_to_bf16<<<(MLP_NPARAM + 255) / 256, 256>>>(g->mlp_w, g->mlp_wq);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    g->trained = true;
+    g->recording = false;
+    ++g_alloc_epoch;
+    return 0;
+}
+
+extern "C" int csaw_mlp_grad_host(const float *params, const float *norm, const void *records, int n, float *grad,
+                                  float *loss) {
+    if (!params || !norm || !records || n < 1 || !grad) return fail(CSAW_ERR_INVALID, "bad arguments");
+    float *dw = nullptr, *dn = nullptr, *dg = nullptr, *dl = nullptr;
+    ProfRec *dr = nullptr;
+    int rc = 0;
+    if (cudaMalloc((void **)&dw, sizeof(float) * MLP_NPARAM) != cudaSuccess ||
+        cudaMalloc((void **)&dn, sizeof(float) * MLP_NORM) != cudaSuccess ||
+        cudaMalloc((void **)&dg, sizeof(float) * MLP_NPARAM) != cudaSuccess ||
+        cudaMalloc((void **)&dl, sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void **)&dr, sizeof(ProfRec) * (size_t)n) != cudaSuccess) {
+        cudaGetLastError();
+        rc = fail(CSAW_ERR_NOMEM, "allocation failed");
+    }
+    if (!rc) {
+        cudaMemcpy(dw, params, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice);
+        cudaMemcpy(dn, norm, sizeof(float) * MLP_NORM, cudaMemcpyHostToDevice);
+        cudaMemcpy(dr, records, sizeof(ProfRec) * (size_t)n, cudaMemcpyHostToDevice);
+        cudaMemset(dg, 0, sizeof(float) * MLP_NPARAM);
+        cudaMemset(dl, 0, sizeof(float));
+        k_mlp_grad<<<std::min(64, (n + MLP_GRAD_THREADS - 1) / MLP_GRAD_THREADS), MLP_GRAD_THREADS>>>(dw, dn, dr, n,
+                                                                                                   dg, dl);
+        cudaMemcpy(grad, dg, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost);
+        for (int i = 0; i < MLP_NPARAM; ++i) grad[i] /= (float)n;
+        if (loss) {
+            cudaMemcpy(loss, dl, sizeof(float), cudaMemcpyDeviceToHost);
+            *loss /= (float)n;
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = fail(CSAW_ERR_CUDA, cudaGetErrorString(e));
+    }
+    cudaFree(dw);
+    cudaFree(dn);
+    cudaFree(dg);
+    cudaFree(dl);
+    cudaFree(dr);
+    return rc;
 }
 
 // Reference file format: beg.bin = int64[V+1], csr.bin = int64[E]

@@ -96,6 +96,26 @@ __device__ __forceinline__ int64_t search_upper(const float *P, int64_t d, float
     return lo;
 }
 
+// The same index for one warp-uniform target, found by the whole warp with a
+// 32-way search: each round probes the last element of 32 equal chunks of the
+// remaining range and keeps the first chunk whose probe exceeds t, so a
+// degree-d search takes about log32(d) dependent loads instead of log2(d).
+__device__ __forceinline__ int64_t warp_search_upper(const float *P, int64_t d, float t, int lane) {
+    int64_t lo = 0, hi = d;   // the answer lies in [lo, hi)
+    while (hi - lo > 32) {
+        const int64_t step = (hi - lo + 31) >> 5;
+        const int64_t idx = lo + (int64_t)(lane + 1) * step - 1;
+        const bool up = idx >= hi - 1 || __ldg(P + idx) > t;
+        const int k = __ffs(__ballot_sync(FULL, up)) - 1;
+        const int64_t nlo = lo + (int64_t)k * step;
+        hi = nlo + step < hi ? nlo + step : hi;
+        lo = nlo;
+    }
+    const int64_t idx = lo + lane;
+    const bool up = idx >= hi - 1 || __ldg(P + idx) > t;
+    return lo + (__ffs(__ballot_sync(FULL, up)) - 1);
+}
+
 // ------------------------------------------------------------ warp scans
 __device__ __forceinline__ float warp_ks_sum(float v, int lane) {
 #pragma unroll

@@ -54,7 +54,11 @@ struct SelEntry {
     uint32_t p;
     int32_t d;
     long long beg;
+    int32_t cls;      // execution granularity chosen for the item
+    int32_t pad;
 };
+
+struct SchedArgs;
 
 // One level of neighbor sampling: input queue -> output edges + next queue.
 struct LevelArgs {
@@ -75,6 +79,12 @@ struct LevelArgs {
     SelEntry *sel_list;       // batched: warp-granularity items (d > N)
     uint32_t *n_sel;
     SelEntry *heavy_list;     // batched: CTA-granularity items (count n_heavy)
+    SelEntry *cta_list[4];    // batched: items per CTA class (128/256/512/1024)
+    uint32_t *n_cta;          //   and their counts
+    int cta_class;            // class of the CTA launch (0..3), for profiles
+    SelEntry *retry_list;     // batched: cached hubs the warp pass handed back
+    uint32_t *n_retry;
+    const SchedArgs *sched;   // learned scheduler, or null (degree rule)
     float *heavy_scratch;     // per-CTA scratch for the heavy kernel
     int64_t heavy_stride;     // floats per CTA
     int32_t *o_src, *o_dst, *o_smp, *o_dep;

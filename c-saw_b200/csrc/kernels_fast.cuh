@@ -316,6 +316,7 @@ k_coop_fast(DevGraph g, LevelArgs a) {
     const uint32_t n = *a.n_in;
     const int N = a.N;
     const bool cached = BIASED && g.cdf && g.cdf_bias == BIAS;
+    const bool routed = BIASED && a.sched && a.sched->mode != SCHED_THRESHOLD;
     const int nout = 2 + (a.o_smp != nullptr) + (a.o_dep != nullptr);
     const unsigned long long per_edge = 4ull + 4ull * nout + (a.push ? 12ull + 2 * (sizeof(I) + 4) : 0ull);
     uint32_t bs = (n + nw - 1) / nw;
@@ -336,7 +337,28 @@ k_coop_fast(DevGraph g, LevelArgs a) {
         }
         const int k = (valid && d > 0) ? (int)(d < N ? d : N) : 0;
         const bool drawn = k > 0 && d > N;
-        const bool heavy = drawn && BIASED && !cached && d > WF;
+        // execution class of items that need draws: degree rule, or learned
+        int cls = 1;
+        if (drawn && BIASED) cls = threshold_class(d, WF, cached);
+        if (routed) {
+            float2 st = make_float2(0.f, 0.f);
+            if (drawn) st = a.sched->vstats[v];
+            unsigned dm = __ballot_sync(FULL, drawn);
+            while (dm) {
+                const int b = __ffs(dm) - 1;
+                dm &= dm - 1;
+                const int64_t db = __shfl_sync(FULL, d, b);
+                const float2 sb = make_float2(__shfl_sync(FULL, st.x, b), __shfl_sync(FULL, st.y, b));
+                uint32_t hb = (uint32_t)__shfl_sync(FULL, s, b) * 0x9E3779B1u ^ __shfl_sync(FULL, p, b) * 0x85EBCA77u ^
+                              (uint32_t)a.depth * 0xC2B2AE3Du ^ a.k0;
+                hb ^= hb >> 15;
+                hb *= 0x2C1B3C6Du;
+                hb ^= hb >> 13;
+                const int c = choose_class(a.sched, a.sched->wq, db, N, sb, n, a.depth, hb, WF, cached, lane);
+                if (lane == b) cls = c;
+            }
+        }
+        const bool heavy = drawn && cls >= 2;
         const int incl = warp_incl_scan(k, lane);
         const int excl = incl - k;
         const int K = __shfl_sync(FULL, incl, 31);
@@ -358,16 +380,20 @@ k_coop_fast(DevGraph g, LevelArgs a) {
             pos = __shfl_sync(FULL, pos, 0);
             if (drawn && !heavy)
                 a.sel_list[pos + __popc(sm & ((1u << lane) - 1u))] =
-                    SelEntry{it, qb + (uint32_t)excl, ob + excl, v, s, p, (int32_t)d, (long long)beg};
+                    SelEntry{it, qb + (uint32_t)excl, ob + excl, v, s, p, (int32_t)d, (long long)beg, cls, 0};
         }
-        const unsigned hm = __ballot_sync(FULL, heavy);
-        if (hm) {
-            uint32_t pos = 0;
-            if (lane == 0) pos = atomicAdd(a.n_heavy, (uint32_t)__popc(hm));
-            pos = __shfl_sync(FULL, pos, 0);
-            if (heavy)
-                a.heavy_list[pos + __popc(hm & ((1u << lane) - 1u))] =
-                    SelEntry{it, qb + (uint32_t)excl, ob + excl, v, s, p, (int32_t)d, (long long)beg};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const bool mine = heavy && cls == 2 + c;
+            const unsigned hm = __ballot_sync(FULL, mine);
+            if (hm) {
+                uint32_t pos = 0;
+                if (lane == 0) pos = atomicAdd(&a.n_cta[c], (uint32_t)__popc(hm));
+                pos = __shfl_sync(FULL, pos, 0);
+                if (mine)
+                    a.cta_list[c][pos + __popc(hm & ((1u << lane) - 1u))] =
+                        SelEntry{it, qb + (uint32_t)excl, ob + excl, v, s, p, (int32_t)d, (long long)beg, cls, 0};
+            }
         }
         if (valid) {
             my_items++;
@@ -422,6 +448,7 @@ k_select_fast(DevGraph g, LevelArgs a) {
     uint32_t *zb = s_z + (BIASED ? wib * (WF / 32) : 0);
     int *zs = s_zs + wib * 32;
     const uint32_t n = *a.n_sel;
+    const uint32_t n_level = *a.n_in;
     const int N = a.N;
     const bool cached = BIASED && g.cdf && g.cdf_bias == BIAS;
     const int nout = 2 + (a.o_smp != nullptr) + (a.o_dep != nullptr);
@@ -432,14 +459,21 @@ k_select_fast(DevGraph g, LevelArgs a) {
         const uint32_t p = en.p;
         const int64_t beg = en.beg, d = en.d;
         const DrawCtx dc{a.k0, a.k1, p, (uint32_t)s, (uint32_t)a.depth};
+        const bool rec = a.sched && a.sched->mode == SCHED_RECORD;
+        long long t0 = 0;
+        if (rec) t0 = clock64();
         int sel;
         if constexpr (!BIASED) {
             sel = select_unbiased(d, N, dc, zs, lane);
         } else {
-            if (cached) {
-                sel = select_warp<I, BIAS>(g, beg, d, N, dc, P, zb, zs, lane);
-            } else if (d <= 32) {
+            if (en.cls == 0) {
                 sel = select_reg<I, BIAS>(g, beg, (int)d, N, dc, lane);
+            } else if (d > WF) {   // cached prefix (only cached items above WF reach here)
+                sel = select_warp<I, BIAS>(g, beg, d, N, dc, P, zb, zs, lane, WF);
+                if (sel == -2) {   // needs a rebuild that does not fit: retried by the CTA pass
+                    if (lane == 0) a.retry_list[atomicAdd(a.n_retry, 1u)] = en;
+                    continue;
+                }
             } else {
                 preload_bias<I, BIAS>(g, beg, (int)d, W, lane);
                 sel = select_smem(W, (int)d, N, dc, P, zb, lane);
@@ -448,9 +482,13 @@ k_select_fast(DevGraph g, LevelArgs a) {
         if (lane < N)
             emit_edge<I>(g, a, beg + sel, v, s, p * (uint32_t)N + (uint32_t)lane, (int64_t)en.ob + lane,
                          en.q + (uint32_t)lane);
+        if (rec) {
+            __syncwarp();
+            if (lane == 0) record_profile(a.sched, d, N, a.sched->vstats[v], n_level, a.depth, en.cls, clock64() - t0);
+        }
         if (lane == 0) {
             my_items++;
-            my_bytes += 16 + (BIASED && !cached ? 4ull * d : 0ull) +
+            my_bytes += 16 + (BIASED && !(cached && d > WF) ? 4ull * d : 0ull) +
                         (unsigned long long)N * (4ull + 4ull * nout + (a.push ? 12ull + 2 * (sizeof(I) + 4) : 0ull));
         }
     }
@@ -523,11 +561,6 @@ k_walk_fast(DevGraph g, WalkArgs a) {
             if (d == 1) {
             } else if (BIAS == CSAW_BIAS_UNBIASED) {
                 e = beg + mulhi(x, (uint32_t)d);
-            } else if (cached) {
-                const float *cp = g.cdf + beg;
-                const float T = cp[d - 1];
-                e = beg + (T > 0.f ? search_upper(cp, d, its_target(x, T)) : 0);
-                bytes += 4ull * (64 - __clzll((unsigned long long)d));
             } else if (d <= 32) {
                 float wl = 0.f;
                 int32_t ul = 0, dl = 0;
@@ -553,6 +586,11 @@ k_walk_fast(DevGraph g, WalkArgs a) {
                 nd = __shfl_sync(FULL, dl, idx);
                 have = g.nbr_beg != nullptr;
                 bytes += (mat ? 4ull : 4ull + 2ull * sizeof(I)) * d + rec * (d - 1);
+            } else if (cached) {
+                const float *cp = g.cdf + beg;
+                const float T = __ldg(cp + d - 1);
+                e = beg + (T > 0.f ? warp_search_upper(cp, d, its_target(x, T), lane) : 0);
+                bytes += 4ull * 32 * ((68 - __clzll((unsigned long long)d)) / 5);   // 32 probes per round
             } else if (d <= WF) {
                 preload_bias<I, BIAS>(g, beg, d, W, lane);
                 auto wfn = [&](int64_t i) { return W[i]; };

@@ -10,6 +10,7 @@
 #pragma once
 
 #include "csaw_device.cuh"
+#include "sched_mlp.cuh"
 
 namespace csaw {
 
@@ -52,11 +53,15 @@ static __global__ void k_init_queue(const int32_t *seeds, uint32_t n, int F, int
 
 // ------------------------------------------------------- warp selection
 // Selection for one item with d > N by one warp; returns the lane's slot
-// selection (lanes < N).  P/zb/zs: the warp's shared buffers (d <= WBUF).
+// selection (lanes < N).  P/zb/zs: the warp's shared buffers, P holding `cap`
+// floats.  With a CDF cache the first phase searches the cached prefix, so d
+// may exceed cap; if such an item needs a phase rebuild (which must write a
+// prefix of d floats) every lane returns -2 and the caller hands the whole
+// item to the CTA path, which recomputes it with the same keys.
 template <typename I, int BIAS>
 __device__ __forceinline__ int select_warp(const DevGraph &g, int64_t beg, int64_t d, int N,
                                            const DrawCtx &dc, float *P, uint32_t *zb, int *zs,
-                                           int lane) {
+                                           int lane, int64_t cap) {
     constexpr bool BIASED = BIAS != CSAW_BIAS_UNBIASED;
     auto wfn = [&](int64_t i) { return edge_bias<I, BIAS>(g, beg + i); };
     float T = 0.f;
@@ -87,6 +92,7 @@ __device__ __forceinline__ int select_warp(const DevGraph &g, int64_t beg, int64
         if (resolve_slots(st, N, lane, dc, rng, cand_of) == 0) break;
         const int j = st.j;
         if constexpr (BIASED) {
+            if (d > cap) return -2;
             const int nwords = (int)((d + 31) >> 5);
             for (int w = lane; w < nwords; w += 32) zb[w] = 0u;
             __syncwarp();
@@ -159,7 +165,15 @@ k_expand_warp(DevGraph g, LevelArgs a) {
         if (d > N) {
             scanned = BIASED && !(g.cdf && g.cdf_bias == BIAS);
             const DrawCtx dc{a.k0, a.k1, p, (uint32_t)s, (uint32_t)a.depth};
-            sel = select_warp<I, BIAS>(g, beg, d, N, dc, P, zb, zs, lane);
+            sel = select_warp<I, BIAS>(g, beg, d, N, dc, P, zb, zs, lane, WBUF);
+            if (sel == -2) {   // cached hub that needs a rebuild: the CTA path redoes it
+                my_items--;
+                if (lane == 0) {
+                    uint32_t h = atomicAdd(a.n_heavy, 1u);
+                    a.heavy[h] = it;
+                }
+                continue;
+            }
         }
         bool act = lane < k;
         int32_t dst = 0;
@@ -195,7 +209,7 @@ k_expand_warp(DevGraph g, LevelArgs a) {
 // global scratch (same canonical order, so bit-identical to the warp path);
 // warp 0 runs the slot resolver; every rebuild is a CTA-wide rescan.
 template <typename I, int BIAS>
-__global__ void __launch_bounds__(HEAVY_THREADS)
+__global__ void __launch_bounds__(1024)
 k_expand_heavy(DevGraph g, LevelArgs a) {
     __shared__ int s_flag, s_j;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -205,6 +219,9 @@ k_expand_heavy(DevGraph g, LevelArgs a) {
     unsigned long long my_bytes = 0, my_items = 0;
     for (uint32_t h = blockIdx.x; h < nh; h += gridDim.x) {
         const uint32_t it = a.heavy_list ? a.heavy_list[h].it : a.heavy[h];
+        const bool rec = a.sched && a.sched->mode == SCHED_RECORD;
+        long long t0 = 0;
+        if (rec && threadIdx.x == 0) t0 = clock64();
         const int32_t v = a.in_v[it];
         const int32_t s = a.in_s[it];
         const uint32_t p = a.in_p[it];
@@ -218,12 +235,14 @@ k_expand_heavy(DevGraph g, LevelArgs a) {
         float *gcar = tsum + (d >> 5) + 1;
         uint32_t *zb = (uint32_t *)(gcar + (d >> 10) + 1);
         auto wfn = [&](int64_t i) { return edge_bias<I, BIAS>(g, beg + i); };
-        float T = cta_canon_prefix(wfn, d, P, tsum, gcar, nullptr);
+        const bool cached = g.cdf && g.cdf_bias == BIAS;
+        const float *PP = cached ? g.cdf + beg : P;
+        float T = cached ? PP[d - 1] : cta_canon_prefix(wfn, d, P, tsum, gcar, nullptr);
         const DrawCtx dc{a.k0, a.k1, p, (uint32_t)s, (uint32_t)a.depth};
         SlotRng rng;
         SelState st;
         auto cand_of = [&](uint32_t x, bool act) -> int {
-            return act ? (int)search_upper(P, d, its_target(x, T)) : -1;
+            return act ? (int)search_upper(PP, d, its_target(x, T)) : -1;
         };
         bool zero = !(T > 0.f);
         if (warp == 0 && !zero) draw_pending(st, 0, N, lane, dc, rng, cand_of);
@@ -246,6 +265,7 @@ k_expand_heavy(DevGraph g, LevelArgs a) {
             if (warp == 0 && lane < j) atomicOr(&zb[st.sel >> 5], 1u << (st.sel & 31));
             __syncthreads();
             T = cta_canon_prefix(wfn, d, P, tsum, gcar, zb);
+            PP = P;
             if (warp == 0) {
                 if (!(T > 0.f)) zero = true;
                 else draw_pending(st, j, N, lane, dc, rng, cand_of);
@@ -297,6 +317,8 @@ k_expand_heavy(DevGraph g, LevelArgs a) {
         my_items++;
         my_bytes += expansion_bytes<I, BIAS>(g, d, N, true, a);
         __syncthreads();
+        if (rec && threadIdx.x == 0)
+            record_profile(a.sched, d, N, a.sched->vstats[v], *a.n_in, a.depth, 2 + a.cta_class, clock64() - t0);
     }
     if (threadIdx.x == 0) {
         atomicAdd(&a.bytes[1], my_bytes);
@@ -514,6 +536,37 @@ __global__ void k_mdrw(DevGraph g, WalkArgs a) {
     if (lane == 0) {
         atomicAdd(&a.bytes[3], bytes);
         atomicAdd(&a.items[3], steps);
+    }
+}
+
+// -------------------------------------------------------------- CDF cache
+// Canonical prefix of every vertex's edge biases, written in place of the
+// per-edge array cdf[E] (same canonical order, so searching it equals
+// scanning on the fly).  One warp per vertex up to big_deg; vertices above go
+// to k_cdf_build_big, one CTA each.
+template <typename I, int BIAS>
+__global__ void k_cdf_build(DevGraph g, float *cdf, int64_t big_deg) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t v = gw; v < g.v.n_vertices; v += nw) {
+        const int64_t beg = row_begin<I>(g, v), d = row_begin<I>(g, v + 1) - beg;
+        if (d <= 0 || d > big_deg) continue;
+        auto wfn = [&](int64_t i) { return edge_bias<I, BIAS>(g, beg + i); };
+        warp_canon_prefix(wfn, d, cdf + beg, nullptr, lane);
+    }
+}
+
+template <typename I, int BIAS>
+__global__ void k_cdf_build_big(DevGraph g, float *cdf, const int32_t *verts, int n, float *scratch,
+                                int64_t stride) {
+    float *tsum = scratch + (int64_t)blockIdx.x * stride;
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+        const int32_t v = verts[k];
+        const int64_t beg = row_begin<I>(g, v), d = row_begin<I>(g, v + 1) - beg;
+        float *gcar = tsum + (d >> 5) + 1;
+        auto wfn = [&](int64_t i) { return edge_bias<I, BIAS>(g, beg + i); };
+        cta_canon_prefix(wfn, d, cdf + beg, tsum, gcar, nullptr);
     }
 }
 

@@ -76,8 +76,13 @@ typedef struct csaw_graph_s *csaw_graph;
 
 /* graph creation flags */
 enum {
-    CSAW_GRAPH_DEGREE_BIAS = 1, /* materialise per-edge neighbor degree (4E B) */
-    CSAW_GRAPH_CDF_CACHE = 2    /* precompute per-vertex bias prefix (4E B) */
+    CSAW_GRAPH_DEGREE_BIAS = 1,  /* materialise per-edge neighbor degree (4E B) */
+    CSAW_GRAPH_CDF_CACHE = 2,    /* per-vertex bias prefix (4E B) for every schedule,
+                                    the plain one included */
+    CSAW_GRAPH_NO_CDF_CACHE = 4  /* never build the prefix cache.  Without either
+                                    flag the batched and learned schedules build it
+                                    on first biased use when the maximum degree
+                                    exceeds 512 */
 };
 
 typedef struct {
@@ -173,9 +178,34 @@ enum {
      * parameters and buffers is captured once into a CUDA graph and replayed
      * as one launch afterwards; 0: always launch kernel by kernel.  Off while
      * profiling is on. */
-    CSAW_OPT_CUDA_GRAPHS = 1
+    CSAW_OPT_CUDA_GRAPHS = 1,
+    /* n > 0: the next CSAW_SCHED_LEARNED runs record up to n execution
+     * profiles (features, granularity, cycles) with a random valid
+     * granularity per item; 0: stop recording. */
+    CSAW_OPT_SCHED_RECORD = 2
 };
 int csaw_graph_set_option(csaw_graph g, int option, int64_t value);
+
+/*
+ * Learned execution-granularity scheduler (CSAW_SCHED_LEARNED).  Replaces
+ * the reference's fixed warp-per-vertex schedule (main.cu:60-91); it never
+ * changes the output.  An MLP 8 -> 32 -> 32 -> 6 predicts, per item that
+ * needs draws, the latency of six granularities (warp in registers, warp in
+ * shared memory, CTA of 128/256/512/1024 threads); without a trained model
+ * the degree rule is used.  csaw_sched_train fits it on the GPU (FP32 forward
+ * and backward kernels, full-batch Adam) to the recorded profiles;
+ * csaw_mlp_grad_host exposes the mean loss and gradient for checking.
+ * Parameter layout: W1[32][8] b1[32] W2[32][32] b2[32] W3[6][32] b3[6]
+ * (1542 floats); norm: x mean[8], x std[8], y mean, y std (18 floats).
+ * Profile record: float x[8], int32 class, float cycles (40 bytes).
+ */
+int csaw_sched_info(csaw_graph g, int64_t *n_records, int *trained, float *last_loss);
+int csaw_sched_get_records(csaw_graph g, void *out, int64_t max_n, int64_t *n);
+int csaw_sched_train(csaw_graph g, int epochs, float lr, uint64_t seed, float *final_loss);
+int csaw_sched_get_model(csaw_graph g, float *params, float *norm);
+int csaw_sched_set_model(csaw_graph g, const float *params, const float *norm);
+int csaw_mlp_grad_host(const float *params, const float *norm, const void *records, int n,
+                       float *grad, float *loss);
 
 /*
  * Neighbor sampling that allocates no device memory.  No counterpart in the
