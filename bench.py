@@ -185,44 +185,180 @@ def learned_gain(args):
     """Degree rule vs learned granularity on a heavy-tailed graph: R-MAT
     (a=.6, b=.2, c=.15) scale 20, edge factor 16, Pareto(1.5) weights,
     edge-weight-biased sampling, 8192 samples, F 8, N 10, D 3 (the shape of
-    the scale-25 learned-scheduler configuration at 1/32 of its vertices).
-    Prints one JSON line with both times; identical edges are asserted."""
+    the scale-25 learned-scheduler configuration at 1/32 of its vertices),
+    with the per-vertex prefix cache (the default for this graph) and without
+    it.  Prints one JSON line with both times per variant; identical edges
+    are asserted."""
     import torch
     import csaw
     from csaw import graphgen
     g = graphgen.rmat(20, 16, a=0.6, b=0.2, c=0.15, seed=25, weight="pareto:1.5")
-    G = csaw.Graph(g)
-    seeds = G.make_seeds(8192 * 8, 0x25)
     out = torch.empty((3, 8192 * 8 * (10 + 100 + 1000)), dtype=torch.int32, device="cuda")
-    res = {}
-    for form, sch in (("batched", csaw.SCHED_BATCHED), ("learned", csaw.SCHED_LEARNED)):
-        p = csaw.make_params(0, 2, 8192, 8, 10, 3, seed=0x25, schedule=sch)
-        job = [csaw.BatchJob(p, seeds, out.shape[1], out, with_depth=False)]
-        if form == "learned":
-            G.sched_record(400_000)
-            for _ in range(3):
+    res = {"graph": {"V": g.n_vertices, "E": g.n_edges, "max_degree": int(np.diff(g.rowptr).max())}}
+    for variant, cache in (("cache", None), ("no_cache", False)):
+        G = csaw.Graph(g, cdf_cache=cache)
+        seeds = G.make_seeds(8192 * 8, 0x25)
+        r = {}
+        for form, sch in (("batched", csaw.SCHED_BATCHED), ("learned", csaw.SCHED_LEARNED)):
+            p = csaw.make_params(0, 2, 8192, 8, 10, 3, seed=0x25, schedule=sch)
+            job = [csaw.BatchJob(p, seeds, out.shape[1], out, with_depth=False)]
+            if form == "learned":
+                G.sched_record(400_000)
+                for _ in range(3):
+                    G.sample_batch(job)
+                r["train_loss"] = G.sched_train(epochs=400, lr=3e-3, seed=1)
+                r["class_mask"] = G.sched_info()["class_mask"]
+            for _ in range(args.warmup):
                 G.sample_batch(job)
-            res["train_loss"] = G.sched_train(epochs=400, lr=3e-3, seed=1)
-        for _ in range(args.warmup):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            n = 0
+            for _ in range(args.steps):
+                n += G.sample_batch(job)[0][0].numel()
+            e1.record()
+            torch.cuda.synchronize()
+            r[form] = {"ms_per_step": e0.elapsed_time(e1) / args.steps, "edges_per_step": n / args.steps}
+            G.profile(True)
             G.sample_batch(job)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        n = 0
-        for _ in range(args.steps):
-            n += G.sample_batch(job)[0][0].numel()
-        e1.record()
-        torch.cuda.synchronize()
-        res[form] = {"ms_per_step": e0.elapsed_time(e1) / args.steps, "edges_per_step": n / args.steps}
-        G.profile(True)
-        G.sample_batch(job)
-        res[form]["cta_items"] = G.kernel_stats("heavy")["items"]
-        res[form]["warp_items"] = G.kernel_stats("select")["items"]
-        G.profile(False)
-    assert res["batched"]["edges_per_step"] == res["learned"]["edges_per_step"]
-    res["learned_speedup"] = res["batched"]["ms_per_step"] / res["learned"]["ms_per_step"]
-    res["graph"] = {"V": g.n_vertices, "E": g.n_edges, "max_degree": int(np.diff(g.rowptr).max())}
+            r[form]["kernels"] = {k: G.kernel_stats(k) for k in ("expand", "select", "heavy", "setup")}
+            G.profile(False)
+        assert r["batched"]["edges_per_step"] == r["learned"]["edges_per_step"]
+        r["learned_speedup"] = r["batched"]["ms_per_step"] / r["learned"]["ms_per_step"]
+        res[variant] = r
+        G.close()
     print(json.dumps({"learned_gain": res}))
+
+
+SERVE_GRAPH = dict(scale=22, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=22, weight="uniform")
+SERVE_RATE = 2000.0          # requests per second, Poisson
+SERVE_SEEDS = (512, 1.0, 64, 8192)   # lognormal median, sigma, clip
+
+
+def serve_requests(csaw, g, n, rng, kind=None, n_seeds=None):
+    """Requests of the serving mix: 2-hop [25,10] and 3-hop [15,10,5]
+    edge-weight-biased neighbor sampling and edge-weight-biased walks of
+    length U{10..80}, in equal shares; seeds per request lognormal (median
+    512, sigma 1) clipped to [64, 8192], uniform over non-isolated vertices."""
+    med, sig, lo, hi = SERVE_SEEDS
+    deg = np.diff(g.rowptr)
+    non = np.flatnonzero(deg > 0).astype(np.int32)
+    out = []
+    for i in range(n):
+        k = kind if kind is not None else int(rng.integers(0, 3))
+        m = n_seeds or int(np.clip(np.round(med * np.exp(sig * rng.standard_normal())), lo, hi))
+        seeds = non[rng.integers(0, non.size, m)]
+        if k == 0:
+            p = csaw.make_params(0, 2, m, 1, 25, 2, [25, 10], seed=1 + i, schedule=csaw.SCHED_BATCHED)
+        elif k == 1:
+            p = csaw.make_params(0, 2, m, 1, 15, 3, [15, 10, 5], seed=1 + i, schedule=csaw.SCHED_BATCHED)
+        else:
+            p = csaw.make_params(1, 2, m, 1, 1, int(rng.integers(10, 81)), seed=1 + i,
+                                 schedule=csaw.SCHED_BATCHED)
+        out.append((k, m, p, seeds))
+    return out
+
+
+def run_stream(csaw, S, reqs, rate, rng, pool):
+    """Open-loop Poisson arrivals at `rate`: a submitter thread issues each
+    request at its arrival time, a waiter collects results in order.  Output
+    buffers are page-locked (direct device-to-host copies), from a pool by
+    size class.  Latency is measured inside the library (submit to result in
+    host memory)."""
+    import threading
+    gaps = rng.exponential(1.0 / rate, len(reqs))
+    tickets = [None] * len(reqs)
+    ready = threading.Semaphore(0)
+    lat = [0.0] * len(reqs)
+    edges = [0] * len(reqs)
+
+    def waiter():
+        for i in range(len(reqs)):
+            ready.acquire()
+            t, buf, cls = tickets[i]
+            n, ms, _ = S.wait(t)
+            lat[i], edges[i] = ms, n
+            pool.put(cls, buf)
+
+    th = threading.Thread(target=waiter)
+    th.start()
+    t0 = time.perf_counter()
+    due = t0
+    for i, (k, m, p, seeds) in enumerate(reqs):
+        due += gaps[i]
+        cap = csaw.edge_bound(p)
+        cls, buf = pool.get(cap)
+        while True:
+            left = due - time.perf_counter()
+            if left <= 0:
+                break
+            if left > 3e-4:
+                time.sleep(left - 3e-4)
+        tickets[i] = (S.submit(p, seeds, out=buf, capacity=cap, with_sample=False, with_depth=False), buf, cls)
+        ready.release()
+    th.join()
+    wall = time.perf_counter() - t0
+    return np.array(lat), np.array(edges), wall
+
+
+class PinnedPool:
+    """Page-locked (2, cap) int32 buffers by power-of-two size class."""
+
+    def __init__(self):
+        self.free = {}
+
+    def get(self, cap):
+        import torch
+        cls = max(1 << 12, 1 << int(np.ceil(np.log2(max(cap, 1)))))
+        lst = self.free.setdefault(cls, [])
+        if lst:
+            return cls, lst.pop()
+        return cls, torch.empty((2, cls), dtype=torch.int32).pin_memory()
+
+    def put(self, cls, buf):
+        self.free[cls].append(buf)
+
+
+def serving(args, n_slots=8):
+    """Serving workload: R-MAT scale 22, edge factor 16, U(0,1] weights (4.19M
+    vertices, generated on the GPU), a Poisson stream of mixed requests at
+    2000 req/s, plus a stream of 1024-seed 2-hop requests at the same rate.
+    Returns p50/p99 latency and throughput of each."""
+    import torch
+    import csaw
+    from csaw import graphgen
+    sys.setswitchinterval(2e-4)   # the waiter thread returns buffers promptly
+    g = graphgen.rmat_device(**SERVE_GRAPH)
+    torch.cuda.empty_cache()
+    G = csaw.Graph(g)
+    S = csaw.Server(G, n_slots=n_slots, device_budget=2 << 30)
+    rng = np.random.default_rng(2000)
+    pool = PinnedPool()
+    res = {"graph": {"workload": f"rmat{SERVE_GRAPH['scale']}_ef{SERVE_GRAPH['edge_factor']}",
+                     "n_vertices": g.n_vertices, "n_edges": g.n_edges,
+                     "max_degree": int(np.diff(g.rowptr).max())},
+           "rate_per_s": SERVE_RATE, "n_slots": n_slots, "device_budget": 2 << 30}
+    # warm-up: every request kind at the largest sizes (job scratch, staging, caches)
+    for k in range(3):   # n_slots largest requests at once: every slot grows its scratch once
+        run_stream(csaw, S, serve_requests(csaw, g, n_slots, rng, kind=k, n_seeds=8192), 1e6, rng, pool)
+    run_stream(csaw, S, serve_requests(csaw, g, 400, rng), SERVE_RATE, rng, pool)
+    S.stats(reset=True)
+    for name, rate, reqs in (
+            ("mixed", SERVE_RATE, serve_requests(csaw, g, args.serve_requests, rng)),
+            ("twohop_1024", SERVE_RATE, serve_requests(csaw, g, args.serve_requests, rng, kind=0, n_seeds=1024)),
+            # every request at once: the loop's capacity (latency is then queueing)
+            ("mixed_saturated", 1e7, serve_requests(csaw, g, args.serve_requests, rng))):
+        lat, edges, wall = run_stream(csaw, S, reqs, rate, rng, pool)
+        st = S.stats(reset=True)
+        res[name] = {"requests": len(reqs), "p50_ms": st["p50_ms"], "p90_ms": st["p90_ms"], "p99_ms": st["p99_ms"],
+                     "max_ms": st["max_ms"], "mean_ms": st["mean_ms"], "p99_queue_ms": st["p99_queue_ms"],
+                     "p99_launch_ms": st["p99_launch_ms"], "p99_gpu_ms": st["p99_gpu_ms"], "edges": int(edges.sum()),
+                     "seps": float(edges.sum()) / (st["last_done_s"] - st["first_submit_s"]),
+                     "offered_rate": len(reqs) / wall, "failed": st["failed"],
+                     "peak_device_bytes": st["peak_device_bytes"]}
+    S.close()
+    G.close()
+    return res
 
 
 def main():
@@ -234,6 +370,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--learned-gain", action="store_true",
                     help="time the degree rule vs the learned scheduler on a heavy-tailed R-MAT graph instead")
+    ap.add_argument("--serve", action="store_true", help="run only the serving (request loop) workload")
+    ap.add_argument("--serve-requests", type=int, default=4000, help="requests per serving stream")
     ap.add_argument("--forms", default="plain,batched,learned",
                     help="forms to time; the last one is reported as value (profiling runs use one form)")
     args = ap.parse_args()
@@ -244,6 +382,11 @@ def main():
         return
     if args.learned_gain:
         learned_gain(args)
+        return
+    if args.serve:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps({"serving": serving(args)}))
         return
 
     import torch

@@ -6,10 +6,10 @@ ABI, include/csaw.h); this package is its host-side binding.
 from . import graphgen
 from ._lib import (BIAS_DEGREE, BIAS_EDGE_WEIGHT, BIAS_HOOK, BIAS_UNBIASED, MODE_MDRW, MODE_NEIGHBOR,
                    MODE_WALK, SCHED_BATCHED, SCHED_LEARNED, SCHED_PLAIN, CsawError, lib)
-from .sampler import Arguments, BatchJob, Graph, Sampler, StreamGraph, edge_bound, make_params
+from .sampler import Arguments, BatchJob, Graph, Sampler, Server, StreamGraph, edge_bound, make_params
 
 __all__ = [
-    "graphgen", "lib", "Graph", "StreamGraph", "Sampler", "Arguments", "BatchJob", "make_params", "edge_bound", "CsawError",
+    "graphgen", "lib", "Graph", "StreamGraph", "Server", "Sampler", "Arguments", "BatchJob", "make_params", "edge_bound", "CsawError",
     "MODE_NEIGHBOR", "MODE_WALK", "MODE_MDRW", "BIAS_UNBIASED", "BIAS_DEGREE", "BIAS_EDGE_WEIGHT",
     "BIAS_HOOK", "SCHED_PLAIN", "SCHED_BATCHED", "SCHED_LEARNED",
 ]

@@ -9,7 +9,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libcsaw_b200.so")
 
-OK, ERR_INVALID, ERR_CUDA, ERR_CAPACITY, ERR_NOMEM, ERR_DEVICE = range(6)
+OK, ERR_INVALID, ERR_CUDA, ERR_CAPACITY, ERR_NOMEM, ERR_DEVICE, PENDING = range(7)
 MODE_NEIGHBOR, MODE_WALK, MODE_MDRW = 0, 1, 2
 BIAS_UNBIASED, BIAS_DEGREE, BIAS_EDGE_WEIGHT, BIAS_HOOK = 0, 1, 2, 3
 SCHED_PLAIN, SCHED_BATCHED, SCHED_LEARNED = 0, 1, 2
@@ -23,8 +23,9 @@ EXPORTS = [
     "csaw_graph_stats", "csaw_graph_profile", "csaw_graph_kernel_stats", "csaw_make_seeds",
     "csaw_sample", "csaw_sample_host", "csaw_sample_batch", "csaw_sample_noalloc", "csaw_sampler_compat",
     "csaw_graph_set_option", "csaw_stream_graph_create", "csaw_stream_graph_destroy", "csaw_stream_sample",
-    "csaw_stream_stats", "csaw_sched_info", "csaw_sched_get_records", "csaw_sched_train", "csaw_sched_get_model", "csaw_sched_set_model",
-    "csaw_mlp_grad_host",
+    "csaw_stream_stats", "csaw_sched_info", "csaw_sched_get_records", "csaw_sched_train", "csaw_sched_classes", "csaw_sched_get_model", "csaw_sched_set_model",
+    "csaw_mlp_grad_host", "csaw_server_create", "csaw_server_destroy", "csaw_server_submit", "csaw_server_wait",
+    "csaw_server_get_stats",
 ]
 OPT_CUDA_GRAPHS = 1
 OPT_SCHED_RECORD = 2
@@ -50,6 +51,17 @@ class Params(ctypes.Structure):
         ("seed", ctypes.c_uint64),
         ("sample_base", ctypes.c_int64),
     ]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("n_slots", ctypes.c_int32), ("max_wait_us", ctypes.c_int32), ("device_budget", ctypes.c_int64)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(f, ctypes.c_int64) for f in ("submitted", "completed", "failed", "queued", "in_flight", "edges",
+                                               "peak_device_bytes", "workspace_bytes")] + \
+               [(f, ctypes.c_double) for f in ("p50_ms", "p90_ms", "p99_ms", "max_ms", "mean_ms", "p99_queue_ms",
+                                                "p99_launch_ms", "p99_gpu_ms", "first_submit_s", "last_done_s")]
 
 
 class Job(ctypes.Structure):
@@ -113,10 +125,16 @@ def lib():
     PF = ctypes.POINTER(ctypes.c_float)
     L.csaw_sched_info.argtypes = [p, P64, ctypes.POINTER(ctypes.c_int), PF]
     L.csaw_sched_train.argtypes = [p, i32, ctypes.c_float, u64, PF]
+    L.csaw_sched_classes.argtypes = [p, ctypes.POINTER(ctypes.c_uint32)]
     L.csaw_sched_get_records.argtypes = [p, p, i64, P64]
     L.csaw_sched_get_model.argtypes = [p, p, p]
     L.csaw_sched_set_model.argtypes = [p, p, p]
     L.csaw_mlp_grad_host.argtypes = [p, p, p, i32, p, PF]
+    L.csaw_server_create.argtypes = [p, ctypes.POINTER(ServerConfig), ctypes.POINTER(p)]
+    L.csaw_server_destroy.argtypes = [p]
+    L.csaw_server_submit.argtypes = [p, ctypes.POINTER(Params), p, p, p, p, p, i64, ctypes.POINTER(ctypes.c_uint64)]
+    L.csaw_server_wait.argtypes = [p, ctypes.c_uint64, i64, P64, ctypes.POINTER(ctypes.c_double)]
+    L.csaw_server_get_stats.argtypes = [p, i32, ctypes.POINTER(ServerStats)]
     L.csaw_sampler_compat.argtypes = [ctypes.c_char_p, ctypes.c_char_p, i32, i32, i32, i32, i32, i32,
                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
     for name in EXPORTS:

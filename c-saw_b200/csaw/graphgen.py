@@ -95,6 +95,61 @@ def rmat(scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=0, symmetrize=True, we
     return CSR(rowptr, col, w, name=f"rmat{scale}_ef{edge_factor}")
 
 
+def rmat_device(scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=0, symmetrize=True, weight="uniform",
+                device="cuda", chunk=1 << 26):
+    """R-MAT as rmat() (same quadrant rule, self-loops and duplicates removed),
+    generated with torch on a CUDA device, so scales 22-25 take seconds rather
+    than minutes.  Draws come from a torch Philox generator seeded with `seed`:
+    the same distribution as rmat(), not the same graph."""
+    import torch
+    V = 1 << scale
+    E = edge_factor * V
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    ab, abc = a + b, a + b + c
+    keys = []
+    for off in range(0, E, chunk):
+        n = min(chunk, E - off)
+        s = torch.zeros(n, dtype=torch.int64, device=device)
+        d = torch.zeros(n, dtype=torch.int64, device=device)
+        for bit in range(scale):
+            r = torch.rand(n, generator=gen, device=device)
+            s |= (r >= ab).to(torch.int64) << bit
+            d |= (((r >= a) & (r < ab)) | (r >= abc)).to(torch.int64) << bit
+            del r
+        keep = s != d
+        s, d = s[keep], d[keep]
+        keys.append(torch.unique(s * V + d))
+        if symmetrize:
+            keys.append(torch.unique(d * V + s))
+        del s, d, keep
+    key = torch.unique(torch.cat(keys))
+    del keys
+    src = key // V
+    col = (key % V).to(torch.int32)
+    del key
+    rowptr = torch.zeros(V + 1, dtype=torch.int64, device=device)
+    rowptr[1:] = torch.cumsum(torch.bincount(src, minlength=V), 0)
+    del src
+    m = col.numel()
+    wgen = torch.Generator(device=device)
+    wgen.manual_seed(seed + 1)
+    if weight == "uniform":
+        w = 1.0 - torch.rand(m, generator=wgen, device=device)                      # (0, 1]
+    elif weight == "lognormal":
+        w = torch.exp(torch.randn(m, generator=wgen, device=device))
+    elif weight.startswith("pareto"):
+        alpha = float(weight.split(":")[1]) if ":" in weight else 1.5
+        w = torch.pow(1.0 - torch.rand(m, generator=wgen, device=device), -1.0 / alpha)   # Pareto, x_m = 1
+    elif weight == "none":
+        w = None
+    else:
+        raise ValueError(weight)
+    out = CSR(rowptr.cpu().numpy(), col.cpu().numpy(), None if w is None else w.float().cpu().numpy(),
+              name=f"rmat{scale}_ef{edge_factor}_dev")
+    return out
+
+
 def powerlaw_directed(n_vertices=875_713, n_edges=5_105_039, gamma=2.1, max_degree=460, zipf=0.6,
                       seed=0, weight="lognormal"):
     """Directed graph whose out-degrees follow P(d) ~ d^-gamma on [1, max_degree]."""

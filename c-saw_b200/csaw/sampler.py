@@ -109,7 +109,9 @@ class Graph:
     def sched_info(self):
         n, t, l = ctypes.c_int64(), ctypes.c_int(), ctypes.c_float()
         check(lib().csaw_sched_info(self.h, ctypes.byref(n), ctypes.byref(t), ctypes.byref(l)))
-        return {"records": n.value, "trained": bool(t.value), "loss": l.value}
+        m = ctypes.c_uint32()
+        check(lib().csaw_sched_classes(self.h, ctypes.byref(m)))
+        return {"records": n.value, "trained": bool(t.value), "loss": l.value, "class_mask": m.value}
 
     def sched_records(self, max_n=1 << 20):
         out = np.zeros(max_n, dtype=PROF_DTYPE)
@@ -333,6 +335,78 @@ class BatchJob:
         o = self.out
         return (o[0, :k], o[1, :k], o[2, :k] if self.with_sample else None,
                 o[2 + self.with_sample, :k] if self.with_depth else None)
+
+
+class Server:
+    """Request loop with continuous batching on a resident Graph
+    (csaw_server_*): a native worker thread admits requests as slots and the
+    device budget free up and runs them concurrently; results land in host
+    buffers (numpy arrays, or page-locked torch CPU tensors for a direct
+    copy).  submit/wait may be called from several threads."""
+
+    def __init__(self, graph, n_slots=8, device_budget=1 << 30, max_wait_us=2000):
+        cfg = _lib.ServerConfig(n_slots, max_wait_us, device_budget)
+        h = ctypes.c_void_p()
+        check(lib().csaw_server_create(graph.h, ctypes.byref(cfg), ctypes.byref(h)))
+        self.h = h
+        self.graph = graph
+        self._live = {}
+
+    def close(self):
+        if self.h:
+            lib().csaw_server_destroy(self.h)
+            self.h = None
+            self._live.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _addr(x):
+        if isinstance(x, np.ndarray):
+            return x.ctypes.data_as(ctypes.c_void_p).value
+        return x.data_ptr()
+
+    def submit(self, params, seeds, out=None, capacity=None, with_sample=True, with_depth=True):
+        """Queues one request; returns its ticket.  seeds: host int32 array
+        (copied); out: (2 + with_sample + with_depth, capacity) int32 host
+        buffer, kept referenced until wait() reports the ticket."""
+        seeds = np.ascontiguousarray(seeds, dtype=np.int32)
+        if capacity is None:
+            capacity = edge_bound(params) if out is None else out.shape[1]
+        rows = 2 + with_sample + with_depth
+        if out is None:
+            out = np.empty((rows, max(capacity, 1)), dtype=np.int32)
+        ptr = [self._addr(out[i]) for i in range(rows)]
+        t = ctypes.c_uint64()
+        check(lib().csaw_server_submit(self.h, ctypes.byref(params), seeds.ctypes.data_as(ctypes.c_void_p), ptr[0],
+                                       ptr[1], ptr[2] if with_sample else None,
+                                       ptr[2 + with_sample] if with_depth else None, capacity, ctypes.byref(t)))
+        self._live[t.value] = (out, with_sample, with_depth)
+        return t.value
+
+    def wait(self, ticket, timeout_us=-1):
+        """(edges, latency_ms, (src, dst, sample, depth) views) once the request
+        is done; None while it is pending after timeout_us.  Raises CsawError
+        for a failed request."""
+        n, lat = ctypes.c_int64(), ctypes.c_double()
+        rc = lib().csaw_server_wait(self.h, ticket, timeout_us, ctypes.byref(n), ctypes.byref(lat))
+        if rc == _lib.PENDING:
+            return None
+        live = self._live.pop(ticket, None)
+        check(rc)
+        out, ws, wd = live
+        k = n.value
+        res = (out[0, :k], out[1, :k], out[2, :k] if ws else None, out[2 + ws, :k] if wd else None)
+        return k, lat.value, res
+
+    def stats(self, reset=False):
+        st = _lib.ServerStats()
+        check(lib().csaw_server_get_stats(self.h, int(reset), ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in _lib.ServerStats._fields_}
 
 
 class Arguments:

@@ -74,14 +74,23 @@ struct DevBuf {
 // captured older addresses are dropped.
 uint64_t g_alloc_epoch = 1;
 
-int ensure(DevBuf &b, size_t bytes) {
+// Grows b to at least `bytes`.  With a stream that is not capturing, the old
+// buffer is released and the new one taken stream-ordered (after the work
+// already queued on st, without synchronising the device), so a job context
+// growing under load does not stall other streams.
+int ensure(DevBuf &b, size_t bytes, cudaStream_t st = nullptr) {
     if (b.n >= bytes) return 0;
     ++g_alloc_epoch;
-    if (b.p) cudaFree(b.p);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    const bool ordered = st && cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone;
+    if (b.p) {
+        if (ordered) cudaFreeAsync(b.p, st);
+        else cudaFree(b.p);
+    }
     b.p = nullptr;
     b.n = 0;
     if (bytes == 0) return 0;
-    cudaError_t e = cudaMalloc(&b.p, bytes);
+    cudaError_t e = ordered ? cudaMallocAsync(&b.p, bytes, st) : cudaMalloc(&b.p, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
         b.p = nullptr;
@@ -100,7 +109,7 @@ constexpr int MDRW_MAX_F = 4096;
 // Job 0 serves csaw_sample; csaw_sample_batch runs job i on context i, each
 // on its own stream, so independent jobs overlap on the device.
 struct JobCtx {
-    DevBuf q[2][5], heavy, sel, hlist, hscratch, wscratch, seeds_in, out_dev, cta[4], retry;
+    DevBuf q[2][5], heavy, sel, hlist, hscratch, wscratch, seeds_in, out_dev, cta[4], retry, stab;
     Counters *ctr = nullptr, *hctr = nullptr;
     cudaStream_t stream = nullptr;   // owned (batch jobs); job 0 uses the caller's
     cudaEvent_t done = nullptr;
@@ -119,10 +128,10 @@ struct csaw_graph_s {
     float *weight = nullptr;
     float *ebias = nullptr;
     bool ebias_flag = false;   // materialised at creation (visible to every schedule)
-    float *cdf = nullptr;
-    int cdf_bias = -1;
+    float *cdf[4] = {};           // per bias kind: canonical per-vertex prefix, or null
     bool cdf_flag = false;        // CSAW_GRAPH_CDF_CACHE: visible to the plain schedule too
     bool cdf_off = false;         // CSAW_GRAPH_NO_CDF_CACHE
+    uint32_t class_mask = 0x3f;   // classes the trained model picks (bit c)
     int32_t *big_verts = nullptr; // vertices above CDF_BIG (the cache builds them one CTA each)
     int64_t n_big = 0;
     void *nbr_beg = nullptr;      // per-edge neighbor records (batched schedules)
@@ -164,9 +173,10 @@ struct csaw_graph_s {
 
 namespace {
 
-// The plain schedule sees the per-edge degree array only when the caller asked
-// for it at creation; the batched schedules materialise it on first use.
-DevGraph dev_view(const csaw_graph_s *g, int schedule = CSAW_SCHED_BATCHED) {
+// The plain schedule sees the per-edge degree array and the prefix cache only
+// when the caller asked for them at creation; the batched schedules
+// materialise them on first use.  `bias` selects the prefix cache (-1: none).
+DevGraph dev_view(const csaw_graph_s *g, int schedule = CSAW_SCHED_BATCHED, int bias = -1) {
     DevGraph d;
     d.v.rowptr = g->rowptr;
     d.v.rowptr_is_64 = g->idx64;
@@ -176,8 +186,8 @@ DevGraph dev_view(const csaw_graph_s *g, int schedule = CSAW_SCHED_BATCHED) {
     d.v.n_edges = g->E;
     d.ebias = (schedule != CSAW_SCHED_PLAIN || g->ebias_flag) ? g->ebias : nullptr;
     const bool fast = schedule != CSAW_SCHED_PLAIN;
-    d.cdf = (fast || g->cdf_flag) ? g->cdf : nullptr;
-    d.cdf_bias = g->cdf_bias;
+    d.cdf = ((fast || g->cdf_flag) && bias > 0 && bias < 4) ? g->cdf[bias] : nullptr;
+    d.cdf_bias = bias;
     d.nbr_beg = fast ? g->nbr_beg : nullptr;
     d.nbr_deg = fast ? g->nbr_deg : nullptr;
     return d;
@@ -261,19 +271,15 @@ constexpr int64_t CDF_BIG = 4096;   // vertices above are built by one CTA each
 // was created with CSAW_GRAPH_CDF_CACHE; never with CSAW_GRAPH_NO_CDF_CACHE.
 template <typename I, int BIAS>
 int ensure_cdf(csaw_graph_s *g, cudaStream_t st) {
-    if (g->cdf && g->cdf_bias == BIAS) return 0;
+    if (g->cdf[BIAS]) return 0;
     if (g->E == 0 || g->cdf_off) return 0;
-    if (!g->cdf) {
-        ++g_alloc_epoch;
-        CK(cudaMalloc((void **)&g->cdf, sizeof(float) * (size_t)g->E));
-        g->dev_bytes += 4 * g->E;
-    }
-    g->cdf_bias = -1;
-    DevGraph dg = dev_view(g);
-    dg.cdf = nullptr;
+    float *cdf = nullptr;
+    ++g_alloc_epoch;
+    CK(cudaMalloc((void **)&cdf, sizeof(float) * (size_t)g->E));
+    const DevGraph dg = dev_view(g);
     {
         LaunchScope ls(g, KK_INIT, st);
-        k_cdf_build<I, BIAS><<<g->sm_count * 8, 256, 0, st>>>(dg, g->cdf, CDF_BIG);
+        k_cdf_build<I, BIAS><<<g->sm_count * 8, 256, 0, st>>>(dg, cdf, CDF_BIG);
     }
     if (g->n_big > 0) {
         const int64_t stride = ((g->maxdeg >> 5) + 1 + (g->maxdeg >> 10) + 1 + 8 + 63) & ~63ll;
@@ -281,12 +287,13 @@ int ensure_cdf(csaw_graph_s *g, cudaStream_t st) {
         const int blocks = (int)std::min<int64_t>(g->n_big, g->sm_count * 2);
         CK(cudaMallocAsync((void **)&scratch, sizeof(float) * stride * blocks, st));
         LaunchScope ls(g, KK_INIT, st);
-        k_cdf_build_big<I, BIAS><<<blocks, 1024, 0, st>>>(dg, g->cdf, g->big_verts, (int)g->n_big, scratch, stride);
+        k_cdf_build_big<I, BIAS><<<blocks, 1024, 0, st>>>(dg, cdf, g->big_verts, (int)g->n_big, scratch, stride);
         CK(cudaFreeAsync(scratch, st));
     }
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));
-    g->cdf_bias = BIAS;
+    g->cdf[BIAS] = cdf;
+    g->dev_bytes += 4 * g->E;
     ++g_alloc_epoch;
     return 0;
 }
@@ -313,7 +320,9 @@ int sched_for(csaw_graph_s *g, int schedule, int bias, int warp_slots, cudaStrea
     *out = nullptr;
     if (schedule != CSAW_SCHED_LEARNED || bias == CSAW_BIAS_UNBIASED) return 0;
     SchedArgs h{};
-    h.mode = g->recording ? SCHED_RECORD : (g->trained ? SCHED_MLP : SCHED_THRESHOLD);
+    // a trained model that picks no CTA class routes exactly as the degree rule
+    const bool routes = g->trained && (g->class_mask & 0x3cu);
+    h.mode = g->recording ? SCHED_RECORD : (routes ? SCHED_MLP : SCHED_THRESHOLD);
     h.wq = g->mlp_wq;
     h.norm = g->mlp_norm;
     h.vstats = g->vstats;
@@ -322,6 +331,7 @@ int sched_for(csaw_graph_s *g, int schedule, int bias, int warp_slots, cudaStrea
     h.max_rec = (uint32_t)g->max_rec;
     h.bias_kind = bias;
     h.warp_slots = warp_slots;
+    h.class_mask = g->class_mask;
     if (!g->d_sched) {
         ++g_alloc_epoch;
         CK(cudaMalloc((void **)&g->d_sched, sizeof(SchedArgs)));
@@ -390,31 +400,43 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
     const int64_t qcap = (int64_t)(B * per_sample) + 32;
     const bool plain = p->schedule == CSAW_SCHED_PLAIN;
     for (int k = 0; k < 2; ++k) {
-        for (int a = 0; a < 3; ++a) TRY(ensure(c->q[k][a], sizeof(int32_t) * qcap));
+        for (int a = 0; a < 3; ++a) TRY(ensure(c->q[k][a], sizeof(int32_t) * qcap, st));
         if (!plain) {
-            TRY(ensure(c->q[k][3], sizeof(int64_t) * qcap));
-            TRY(ensure(c->q[k][4], sizeof(int32_t) * qcap));
+            TRY(ensure(c->q[k][3], sizeof(int64_t) * qcap, st));
+            TRY(ensure(c->q[k][4], sizeof(int32_t) * qcap, st));
         }
     }
     const SchedArgs *sched = nullptr;
     const int sgrid = plain ? 0 : grid_for(k_select_fast<I, BIAS>, FAST_THREADS, 0, g->sm_count);
     if (BIASED && ((!plain && g->maxdeg > WF) || g->cdf_flag)) TRY((ensure_cdf<I, BIAS>(g, st)));
-    const bool cached = BIASED && g->cdf && g->cdf_bias == BIAS && (!plain || g->cdf_flag);
+    const bool cached = BIASED && g->cdf[BIAS] && (!plain || g->cdf_flag);
     if (!plain) {
         TRY(ensure_nbr(g, st));
-        TRY(ensure(c->sel, sizeof(SelEntry) * qcap));
-        if (cached && g->maxdeg > WF) TRY(ensure(c->retry, sizeof(SelEntry) * qcap));
+        TRY(ensure(c->sel, sizeof(SelEntry) * qcap, st));
+        if (cached && g->maxdeg > WF) TRY(ensure(c->retry, sizeof(SelEntry) * qcap, st));
         if (p->schedule == CSAW_SCHED_LEARNED && BIASED) TRY((ensure_vstats<I, BIAS>(g, st)));
         TRY(sched_for(g, p->schedule, BIAS, sgrid * (FAST_THREADS / 32), st, &sched));
         for (int k = 0; k < 4; ++k)
-            if (sched || k == 1) TRY(ensure(c->cta[k], sizeof(SelEntry) * qcap));
+            if (sched || k == 1) TRY(ensure(c->cta[k], sizeof(SelEntry) * qcap, st));
+        if (sched && g->sched_host.mode == SCHED_MLP) TRY(ensure(c->stab, 2 * TAB_N, st));
     }
+    const bool tabled = sched && g->sched_host.mode == SCHED_MLP;
+    // CTA classes launched: those the model may pick, and CTA-256 wherever the
+    // degree rule needs it (hubs above WF without a cached prefix)
+    const bool need256 = g->maxdeg > WF && !cached;
+    auto launch_class = [&](int k) {
+        if (!sched || g->sched_host.mode == SCHED_THRESHOLD) return k == 1 && need256;
+        if (g->sched_host.mode == SCHED_RECORD) return true;
+        return ((g->sched_host.class_mask >> (k + 2)) & 1u) || (k == 1 && need256);
+    };
+    bool any_class = false;
+    for (int k = 0; k < 4; ++k) any_class |= launch_class(k);
     const int64_t smem_cap = plain ? WBUF : WF;
     int hblocks = 0;
     int64_t hstride = 0;
     int cta_grid[4] = {0, 0, 0, 0};
     if (BIASED && (g->maxdeg > smem_cap || sched)) {
-        TRY(ensure(c->heavy, sizeof(uint32_t) * qcap));
+        TRY(ensure(c->heavy, sizeof(uint32_t) * qcap, st));
         hstride = g->maxdeg + 2 * ((g->maxdeg >> 5) + 1) + (g->maxdeg >> 10) + 1 + 8;
         hstride = (hstride + 63) & ~63ll;
         hblocks = g->sm_count * 2;
@@ -424,9 +446,9 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
             hblocks = std::max(hblocks, cta_grid[k]);
         }
         hblocks = (int)std::min<int64_t>(hblocks, cap_blocks);
-        TRY(ensure(c->hscratch, sizeof(float) * hstride * hblocks));
+        TRY(ensure(c->hscratch, sizeof(float) * hstride * hblocks, st));
     }
-    const DevGraph dg = dev_view(g, p->schedule);
+    const DevGraph dg = dev_view(g, p->schedule, BIAS);
     const uint64_t seed = p->seed;
     const int grid = plain ? grid_for(k_expand_warp<I, BIAS>, EXPAND_THREADS, 0, g->sm_count)
                            : grid_for(k_coop_fast<I, BIAS>, FAST_THREADS, 0, g->sm_count);
@@ -470,6 +492,7 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
             for (int k = 0; k < 4; ++k) a.cta_list[k] = (SelEntry *)c->cta[k].p;
             a.n_cta = c->ctr->n_cta;
             a.sched = sched;
+            a.sched_tab = tabled ? (const uint8_t *)c->stab.p : nullptr;
             a.retry_list = (SelEntry *)c->retry.p;
             a.n_retry = &c->ctr->n_retry;
             a.heavy_scratch = (float *)c->hscratch.p;
@@ -488,12 +511,16 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
             a.depth = l;
             a.N = fan[l];
             a.push = l + 1 < D;
+            if (tabled) {
+                LaunchScope ls(g, KK_INIT, st);
+                k_sched_table<<<TAB_N * 32 / 256, 256, 0, st>>>(sched, a.n_in, a.N, l, (uint8_t *)c->stab.p);
+            }
             {
                 LaunchScope ls(g, KK_EXPAND, st);
                 if (plain) k_expand_warp<I, BIAS><<<grid, EXPAND_THREADS, 0, st>>>(dg, a);
                 else k_coop_fast<I, BIAS><<<grid, FAST_THREADS, 0, st>>>(dg, a);
             }
-            const bool side = hblocks && !plain && (sched || !cached);
+            const bool side = hblocks && !plain && any_class;
             if (side) {
                 // CTA-granularity items on the side stream, concurrent with the
                 // warp-granularity pass (disjoint lists, reserved output slots);
@@ -501,7 +528,7 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
                 CK(cudaEventRecord(c->fork, st));
                 CK(cudaStreamWaitEvent(c->side, c->fork, 0));
                 for (int k = 0; k < 4; ++k) {
-                    if (!sched && k != 1) continue;
+                    if (!launch_class(k)) continue;
                     LevelArgs ak = a;
                     ak.heavy_list = (SelEntry *)c->cta[k].p;
                     ak.n_heavy = &c->ctr->n_cta[k];
@@ -541,7 +568,7 @@ int run_walk_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int32_t *
     const bool plain = p->schedule == CSAW_SCHED_PLAIN;
     if (!plain) TRY(ensure_nbr(g, st));
     if (BIAS != CSAW_BIAS_UNBIASED && ((!plain && g->maxdeg > WF) || g->cdf_flag)) TRY((ensure_cdf<I, BIAS>(g, st)));
-    const DevGraph dg = dev_view(g, p->schedule);
+    const DevGraph dg = dev_view(g, p->schedule, BIAS);
     WalkArgs a{};
     a.seeds = seeds;
     a.n = p->n_samples;
@@ -572,10 +599,10 @@ int run_walk_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int32_t *
                          : grid_for(k_walk_fast<I, BIAS>, FAST_THREADS, 0, g->sm_count);
         int grid = (p->n_samples + (WALK_THREADS / 32) - 1) / (WALK_THREADS / 32);
         if (grid > gmax) grid = gmax;
-        if (g->maxdeg > (plain ? WBUF : WF) && !(g->cdf && g->cdf_bias == BIAS)) {
+        if (g->maxdeg > (plain ? WBUF : WF) && !dg.cdf) {
             int64_t stride = (g->maxdeg + 63) & ~63ll;
             while (grid > 1 && (int64_t)grid * (WALK_THREADS / 32) * stride * 4 > SCRATCH_BUDGET) grid /= 2;
-            TRY(ensure(c->wscratch, sizeof(float) * stride * grid * (WALK_THREADS / 32)));
+            TRY(ensure(c->wscratch, sizeof(float) * stride * grid * (WALK_THREADS / 32), st));
             a.scratch = (float *)c->wscratch.p;
             a.scratch_stride = stride;
         }
@@ -590,7 +617,7 @@ int run_walk_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int32_t *
 template <typename I, int BIAS>
 int run_mdrw_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int32_t *seeds, const OutArgs &o,
                cudaStream_t st) {
-    const DevGraph dg = dev_view(g, p->schedule);
+    const DevGraph dg = dev_view(g, p->schedule, BIAS);
     WalkArgs a{};
     a.seeds = seeds;
     a.n = p->n_samples;
@@ -670,7 +697,7 @@ void free_job(JobCtx *c) {
     for (auto &qq : c->q)
         for (auto &b : qq) cudaFree(b.p);
     for (DevBuf *b : {&c->heavy, &c->sel, &c->hlist, &c->hscratch, &c->wscratch, &c->seeds_in, &c->out_dev, &c->cta[0],
-                      &c->cta[1], &c->cta[2], &c->cta[3], &c->retry})
+                      &c->cta[1], &c->cta[2], &c->cta[3], &c->retry, &c->stab})
         cudaFree(b->p);
     cudaFree(c->ctr);
     if (c->hctr) cudaFreeHost(c->hctr);
@@ -687,7 +714,7 @@ int64_t job_workspace(const JobCtx *c) {
     for (auto &qq : c->q)
         for (auto &b : qq) ws += (int64_t)b.n;
     for (const DevBuf *b : {&c->heavy, &c->sel, &c->hlist, &c->hscratch, &c->wscratch, &c->seeds_in, &c->out_dev,
-                            &c->cta[0], &c->cta[1], &c->cta[2], &c->cta[3], &c->retry})
+                            &c->cta[0], &c->cta[1], &c->cta[2], &c->cta[3], &c->retry, &c->stab})
         ws += (int64_t)b->n;
     return ws;
 }
@@ -760,11 +787,58 @@ int csaw_host_plain_view(csaw_graph g, const csaw_params *p, int fan[CSAW_MAX_DE
                          int64_t *maxdeg, int *device, int *idx64) {
     if (!g) return fail(CSAW_ERR_INVALID, "graph is NULL");
     TRY(check_params(g, p, fan));
-    *view = dev_view(g, CSAW_SCHED_PLAIN);
+    *view = dev_view(g, CSAW_SCHED_PLAIN, p->bias);
     *maxdeg = g->maxdeg;
     *device = g->device;
     *idx64 = g->idx64;
     return 0;
+}
+
+int csaw_host_graph_device(csaw_graph g) { return g ? g->device : -1; }
+
+int csaw_host_edge_bound(csaw_graph g, const csaw_params *p, int64_t *bound, int64_t *n_seeds) {
+    if (!g) return fail(CSAW_ERR_INVALID, "graph is NULL");
+    int fan[CSAW_MAX_DEPTH];
+    TRY(check_params(g, p, fan));
+    double b = 0;   // saturates instead of overflowing (32^64 for deep fanouts)
+    if (p->mode == CSAW_MODE_NEIGHBOR) {
+        double lvl = p->frontier_size;
+        for (int l = 0; l < p->depth; ++l) {
+            lvl *= fan[l];
+            b += lvl;
+        }
+        b *= p->n_samples;
+    } else {
+        b = (double)p->n_samples * p->depth;
+    }
+    *bound = b >= 4e18 ? (int64_t)4e18 : (int64_t)b;
+    *n_seeds = seed_count(p);
+    return 0;
+}
+
+int csaw_host_job_create(csaw_graph g, void **job, cudaStream_t *stream) {
+    if (!g || !job || !stream) return fail(CSAW_ERR_INVALID, "NULL argument");
+    JobCtx *c = nullptr;
+    TRY(new_job(&c, true));
+    *job = c;
+    *stream = c->stream;
+    return 0;
+}
+
+void csaw_host_job_destroy(void *job) { free_job((JobCtx *)job); }
+
+int64_t csaw_host_job_workspace(const void *job) { return job ? job_workspace((const JobCtx *)job) : 0; }
+
+int csaw_host_job_enqueue(csaw_graph g, void *job, const csaw_params *p, const int32_t *seeds, int32_t *src,
+                          int32_t *dst, int32_t *smp, int32_t *dep, int64_t cap) {
+    if (!g || !job || !p) return fail(CSAW_ERR_INVALID, "NULL argument");
+    JobCtx *c = (JobCtx *)job;
+    return enqueue_job(g, c, p, seeds, src, dst, smp, dep, cap, c->stream);
+}
+
+int csaw_host_job_finish(csaw_graph g, void *job, int64_t cap, int64_t *n_out) {
+    if (!g || !job || !n_out) return fail(CSAW_ERR_INVALID, "NULL argument");
+    return finish_job(g, (JobCtx *)job, cap, n_out);
 }
 
 // ===================================================================== C ABI
@@ -808,6 +882,15 @@ extern "C" int csaw_graph_create(const void *rowptr, int rowptr_is_64, const int
     auto *g = new csaw_graph_s();
     cudaGetDevice(&g->device);
     cudaDeviceGetAttribute(&g->sm_count, cudaDevAttrMultiProcessorCount, g->device);
+    {   // keep up to 2 GiB of freed stream-ordered workspace cached in the
+        // device's default pool (process-local), so regrowth maps no memory
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, g->device) == cudaSuccess) {
+            uint64_t thr = 2ull << 30;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+        cudaGetLastError();
+    }
     g->V = n_vertices;
     g->E = n_edges;
     g->maxdeg = maxdeg;
@@ -879,7 +962,7 @@ extern "C" int csaw_graph_destroy(csaw_graph g) {
     cudaFree(g->col);
     cudaFree(g->weight);
     cudaFree(g->ebias);
-    cudaFree(g->cdf);
+    for (float *c : g->cdf) cudaFree(c);
     cudaFree(g->big_verts);
     cudaFree(g->nbr_beg);
     cudaFree(g->nbr_deg);
@@ -975,9 +1058,9 @@ static int enqueue_host_job(csaw_graph_s *g, JobCtx *c, csaw_job *j, cudaStream_
     const int64_t cap = j->capacity;
     if (cap < 0) return fail(CSAW_ERR_INVALID, "capacity < 0");
     const int64_t ns = seed_count(p);
-    TRY(ensure(c->seeds_in, sizeof(int32_t) * (size_t)(ns > 0 ? ns : 1)));
+    TRY(ensure(c->seeds_in, sizeof(int32_t) * (size_t)(ns > 0 ? ns : 1), st));
     const int narr = 2 + (j->out_sample != nullptr) + (j->out_depth != nullptr);
-    TRY(ensure(c->out_dev, sizeof(int32_t) * (size_t)(cap > 0 ? cap : 1) * narr));
+    TRY(ensure(c->out_dev, sizeof(int32_t) * (size_t)(cap > 0 ? cap : 1) * narr, st));
     if (ns > 0) CK(cudaMemcpyAsync(c->seeds_in.p, j->seeds, sizeof(int32_t) * ns, cudaMemcpyHostToDevice, st));
     int32_t *d_src = (int32_t *)c->out_dev.p, *d_dst = d_src + cap;
     int32_t *d_smp = j->out_sample ? d_dst + cap : nullptr;
@@ -1192,6 +1275,32 @@ extern "C" int csaw_sched_info(csaw_graph g, int64_t *n_records, int *trained, f
     return 0;
 }
 
+// Class mask of a trained model: classes 0 and 1 always (the warp pass),
+// CTA classes only where the model picks them on its training records.
+static int pick_classes(csaw_graph_s *g, int n) {
+    g->class_mask = 0x3f;
+    if (n <= 0) return 0;
+    uint32_t *m = nullptr;
+    CK(cudaMalloc((void **)&m, sizeof(uint32_t)));
+    CK(cudaMemset(m, 0, sizeof(uint32_t)));
+    const int slots = grid_for(k_select_fast<int32_t, CSAW_BIAS_EDGE_WEIGHT>, FAST_THREADS, 0, g->sm_count) *
+                      (FAST_THREADS / 32);
+    k_sched_pick<<<g->sm_count * 4, 256>>>(g->rec, n, g->mlp_wq, g->mlp_norm, slots, WF, m);
+    uint32_t h = 0;
+    cudaError_t e = cudaMemcpy(&h, m, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    cudaFree(m);
+    CK(e);
+    g->class_mask = h | 0x3u;
+    g->launches += 1;
+    return 0;
+}
+
+extern "C" int csaw_sched_classes(csaw_graph g, uint32_t *mask) {
+    if (!g || !mask) return fail(CSAW_ERR_INVALID, "NULL argument");
+    *mask = g->trained ? g->class_mask : 0x3fu;
+    return 0;
+}
+
 // Full-batch Adam on the recorded profiles; initial weights are He-scaled
 // uniform from a 64-bit LCG keyed by `seed`.
 extern "C" int csaw_sched_train(csaw_graph g, int epochs, float lr, uint64_t seed, float *final_loss) {
@@ -1228,6 +1337,7 @@ extern "C" int csaw_sched_train(csaw_graph g, int epochs, float lr, uint64_t see
     k_mlp_to_bf16<<<(MLP_NPARAM + 255) / 256, 256>>>(g->mlp_w, g->mlp_wq);
     g->launches += 2 * epochs + 3;
     CK(cudaGetLastError());
+    TRY(pick_classes(g, (int)n));
     float loss = 0.f;
     CK(cudaMemcpy(&loss, g->mlp_loss, sizeof(float), cudaMemcpyDeviceToHost));
     loss /= (float)n;
@@ -1264,6 +1374,7 @@ extern "C" int csaw_sched_set_model(csaw_graph g, const float *params, const flo
     k_mlp_to_bf16<<<(MLP_NPARAM + 255) / 256, 256>>>(g->mlp_w, g->mlp_wq);
     CK(cudaGetLastError());
     CK(cudaDeviceSynchronize());
+    g->class_mask = 0x3f;   // no training records to prune by
     g->trained = true;
     g->recording = false;
     ++g_alloc_epoch;

@@ -82,6 +82,7 @@ struct LevelArgs {
     SelEntry *cta_list[4];    // batched: items per CTA class (128/256/512/1024)
     uint32_t *n_cta;          //   and their counts
     int cta_class;            // class of the CTA launch (0..3), for profiles
+    const uint8_t *sched_tab; // learned (trained): the level's decision table
     SelEntry *retry_list;     // batched: cached hubs the warp pass handed back
     uint32_t *n_retry;
     const SchedArgs *sched;   // learned scheduler, or null (degree rule)

@@ -340,7 +340,10 @@ k_coop_fast(DevGraph g, LevelArgs a) {
         // execution class of items that need draws: degree rule, or learned
         int cls = 1;
         if (drawn && BIASED) cls = threshold_class(d, WF, cached);
-        if (routed) {
+        if (routed && a.sched_tab) {   // trained model: one table load per item
+            if (drawn && d > 32) cls = table_class(a.sched_tab, d, a.sched->vstats[v], N, WF, cached);
+            else if (drawn) cls = 0;
+        } else if (routed) {
             float2 st = make_float2(0.f, 0.f);
             if (drawn) st = a.sched->vstats[v];
             unsigned dm = __ballot_sync(FULL, drawn);

@@ -61,6 +61,7 @@ struct SchedArgs {
     uint32_t max_rec;
     int bias_kind;
     int warp_slots;                // resident warps of the selection kernel
+    uint32_t class_mask;           // SCHED_MLP: classes the model may pick (bit c)
 };
 
 __device__ __forceinline__ int class_warps(int c) { return c <= 1 ? 1 : (4 << (c - 2)); }
@@ -116,6 +117,30 @@ __device__ __forceinline__ float mlp_infer(const __nv_bfloat16 *W, const float *
     return y;
 }
 
+// Cheapest class among `valid` from the predicted normalised log2 latency y
+// of class `lane` (lanes 0..5), or -1 when `valid` is empty.
+__device__ __forceinline__ int class_argmin(float y, const float *norm, uint32_t n_level, int warp_slots,
+                                            unsigned valid, int lane) {
+    const float u = fminf(1.f, (float)n_level / (16.f * (float)warp_slots));
+    // predicted latency in cycles (up to the common scale), weighted by warps
+    float cost = exp2f(y * norm[2 * MLP_IN + 1] + norm[2 * MLP_IN]) *
+                 (1.f + u * (float)(class_warps(lane < MLP_OUT ? lane : 0) - 1));
+    if (lane >= MLP_OUT || !((valid >> lane) & 1u)) cost = __int_as_float(0x7f800000);   // +inf
+    // argmin over lanes 0..7 (ties: lowest class)
+    int best = lane;
+#pragma unroll
+    for (int off = 4; off; off >>= 1) {
+        const float oc = __shfl_down_sync(FULL, cost, off);
+        const int ob = __shfl_down_sync(FULL, best, off);
+        if (oc < cost || (oc == cost && ob < best)) {
+            cost = oc;
+            best = ob;
+        }
+    }
+    best = __shfl_sync(FULL, best, 0);
+    return (valid >> best) & 1u ? best : -1;
+}
+
 // Class for one drawn biased item (warp-uniform inputs; all lanes call).
 __device__ __forceinline__ int choose_class(const SchedArgs *sa, const __nv_bfloat16 *W, int64_t d, int N, float2 st,
                                             uint32_t n_level, int depth, uint32_t hash, int wf, bool cached,
@@ -133,24 +158,78 @@ __device__ __forceinline__ int choose_class(const SchedArgs *sa, const __nv_bflo
     float x[MLP_IN];
     item_features(x, d, N, st, n_level, depth, sa->bias_kind, sa->warp_slots);
     const float y = mlp_infer(W, sa->norm, x, lane);
-    const float u = fminf(1.f, (float)n_level / (16.f * (float)sa->warp_slots));
-    // predicted latency in cycles (up to the common scale), weighted by warps
-    float cost = exp2f(y * sa->norm[2 * MLP_IN + 1] + sa->norm[2 * MLP_IN]) *
-                 (1.f + u * (float)(class_warps(lane < MLP_OUT ? lane : 0) - 1));
-    if (lane >= MLP_OUT || !((valid >> lane) & 1u)) cost = __int_as_float(0x7f800000);   // +inf
-    // argmin over lanes 0..5 (ties: lowest class)
-    int best = lane;
-#pragma unroll
-    for (int off = 4; off; off >>= 1) {
-        const float oc = __shfl_down_sync(FULL, cost, off);
-        const int ob = __shfl_down_sync(FULL, best, off);
-        if (oc < cost || (oc == cost && ob < best)) {
-            cost = oc;
-            best = ob;
+    const int best = class_argmin(y, sa->norm, n_level, sa->warp_slots, valid & sa->class_mask, lane);
+    return best >= 0 ? best : threshold_class(d, wf, cached);
+}
+
+// ------------------------------------------------------- decision table
+// Per level, the model is evaluated once per cell of a grid over the three
+// per-item features that vary within a level (log2 d in half steps from 5,
+// CoV in half steps, N sum p^2 in unit steps; the level's N, size, depth and
+// bias fixed), and the expansion kernel routes each item by one table load.
+// Each cell holds two picks: over classes 1..5 (the item fits a warp: d <= WF
+// or a cached prefix) and over the CTA classes 2..5 (255: none allowed).
+constexpr int TAB_D = 40, TAB_C = 8, TAB_P = 8, TAB_N = TAB_D * TAB_C * TAB_P;
+
+__device__ __forceinline__ int tab_index(int64_t d, float2 st, int N) {
+    const int bd = min(TAB_D - 1, max(0, (int)((__log2f((float)d) - 5.f) * 2.f)));
+    const int bc = min(TAB_C - 1, max(0, (int)(st.x * 2.f)));
+    const int bp = min(TAB_P - 1, max(0, (int)fminf(8.f, (float)N * st.y)));
+    return (bd * TAB_C + bc) * TAB_P + bp;
+}
+
+// Class of a drawn item with d > 32 from the level's table.
+__device__ __forceinline__ int table_class(const uint8_t *tab, int64_t d, float2 st, int N, int wf, bool cached) {
+    const bool warp_ok = cached || d <= wf;
+    const int c = tab[2 * tab_index(d, st, N) + (warp_ok ? 0 : 1)];
+    return c < N_CLASSES ? c : threshold_class(d, wf, cached);
+}
+
+// One warp per cell; n_level read on the device (the level's item count).
+static __global__ void k_sched_table(const SchedArgs *sa, const uint32_t *n_in, int N, int depth, uint8_t *tab) {
+    const int lane = threadIdx.x & 31;
+    const int cell = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (cell >= TAB_N) return;
+    const int bp = cell % TAB_P, bc = (cell / TAB_P) % TAB_C, bd = cell / (TAB_P * TAB_C);
+    const uint32_t n_level = *n_in;
+    const float ld = 5.f + ((float)bd + 0.5f) * 0.5f, lN = __log2f((float)N);
+    float x[MLP_IN];
+    x[0] = ld;
+    x[1] = lN;
+    x[2] = ld - lN;
+    x[3] = ((float)bc + 0.5f) * 0.5f;
+    x[4] = (float)bp + 0.5f;
+    x[5] = __log2f(1.f + (float)n_level / (float)sa->warp_slots);
+    x[6] = (float)depth;
+    x[7] = (float)sa->bias_kind;
+    const float y = mlp_infer(sa->wq, sa->norm, x, lane);
+    const int a = class_argmin(y, sa->norm, n_level, sa->warp_slots, sa->class_mask & 0x3eu, lane);
+    const int b = class_argmin(y, sa->norm, n_level, sa->warp_slots, sa->class_mask & 0x3cu, lane);
+    if (lane == 0) {
+        tab[2 * cell] = (uint8_t)(a < 0 ? 255 : a);
+        tab[2 * cell + 1] = (uint8_t)(b < 0 ? 255 : b);
+    }
+}
+
+// Classes the trained model picks on its own training records (both with and
+// without a prefix cache): classes it never picks are not launched.
+static __global__ void k_sched_pick(const ProfRec *rec, int n, const __nv_bfloat16 *W, const float *norm, int warp_slots,
+                                    int wf, uint32_t *mask) {
+    const int lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    for (int i = gw; i < n; i += nw) {
+        const float *x = rec[i].x;
+        const int64_t d = (int64_t)(exp2f(x[0]) + 0.5f);
+        if (d <= 32) continue;
+        const uint32_t n_level = (uint32_t)((exp2f(x[5]) - 1.f) * (float)warp_slots + 0.5f);
+        const float y = mlp_infer(W, norm, x, lane);
+        const int a = class_argmin(y, norm, n_level, warp_slots, valid_classes(d, wf, false) & 0x3eu, lane);
+        const int b = class_argmin(y, norm, n_level, warp_slots, valid_classes(d, wf, true) & 0x3eu, lane);
+        if (lane == 0) {
+            if (a >= 0) atomicOr(mask, 1u << a);
+            if (b >= 0) atomicOr(mask, 1u << b);
         }
     }
-    best = __shfl_sync(FULL, best, 0);
-    return (valid >> best) & 1u ? best : threshold_class(d, wf, cached);
 }
 
 // Appends one profile record (recording mode).

@@ -32,7 +32,8 @@ enum {
     CSAW_ERR_CUDA = 2,      /* a CUDA runtime call failed */
     CSAW_ERR_CAPACITY = 3,  /* output capacity too small; *n_out = needed */
     CSAW_ERR_NOMEM = 4,     /* device allocation failed */
-    CSAW_ERR_DEVICE = 5     /* a kernel reported an error flag */
+    CSAW_ERR_DEVICE = 5,    /* a kernel reported an error flag */
+    CSAW_PENDING = 6        /* csaw_server_wait: not finished within the timeout */
 };
 
 /* ------------------------------------------------------------- modes */
@@ -202,6 +203,11 @@ int csaw_graph_set_option(csaw_graph g, int option, int64_t value);
 int csaw_sched_info(csaw_graph g, int64_t *n_records, int *trained, float *last_loss);
 int csaw_sched_get_records(csaw_graph g, void *out, int64_t max_n, int64_t *n);
 int csaw_sched_train(csaw_graph g, int epochs, float lr, uint64_t seed, float *final_loss);
+/* Classes a trained model may pick (bit c for class c).  Training keeps the
+ * warp classes 0 and 1 and the CTA classes the model picks on its own
+ * training records; only those CTA widths are launched (plus CTA-256 for hubs
+ * above 512 edges without a cached prefix).  0x3f when untrained. */
+int csaw_sched_classes(csaw_graph g, uint32_t *mask);
 int csaw_sched_get_model(csaw_graph g, float *params, float *norm);
 int csaw_sched_set_model(csaw_graph g, const float *params, const float *norm);
 int csaw_mlp_grad_host(const float *params, const float *norm, const void *records, int n,
@@ -254,6 +260,58 @@ int csaw_stream_sample(csaw_stream_graph g, const csaw_params *p, const int32_t 
                        int32_t *out_src, int32_t *out_dst, int32_t *out_sample,
                        int32_t *out_depth, int64_t capacity, int64_t *n_out, void *stream);
 int csaw_stream_stats(csaw_stream_graph g, csaw_stream_info *out);
+
+/*
+ * Request loop (continuous batching).  The reference runs one synchronous
+ * Sampler() call per process (non-stream/main.cu:196-308, caller
+ * mpi_main.cpp:40); a server instead keeps the graph resident and serves a
+ * stream of independent requests.  A worker thread admits queued requests
+ * while a slot (a job context with its own stream) is free and the request's
+ * device bytes (seeds + outputs sized by its edge bound) fit the device
+ * budget; admitted requests run concurrently on
+ * the device, and each result is copied into the caller's host buffers (a
+ * direct asynchronous copy when they are page-locked).  Queued requests are
+ * admitted first-fit in arrival order; one waiting longer than
+ * max_wait_us (0: 2000 us) blocks later ones until it fits.  A request's
+ * output depends only on its params and seeds, never on what else runs.
+ * Latency = submit to result in host memory.  While a server exists, its
+ * graph must not be used by other calls; submit/wait/stats are thread-safe.
+ */
+typedef struct csaw_server_s *csaw_server;
+typedef struct {
+    int32_t n_slots;        /* concurrent requests on the device (1..64) */
+    int32_t max_wait_us;    /* head-of-line bound for first-fit admission */
+    int64_t device_budget;  /* bytes for in-flight request seeds and outputs */
+} csaw_server_config;
+typedef struct {
+    int64_t submitted, completed, failed;
+    int64_t queued, in_flight;
+    int64_t edges;                 /* edges returned by completed requests */
+    int64_t peak_device_bytes;     /* of the budget, at most */
+    int64_t workspace_bytes;       /* job contexts' scratch */
+    double p50_ms, p90_ms, p99_ms, max_ms, mean_ms;   /* completed since reset */
+    double p99_queue_ms;           /* submit -> admitted */
+    double p99_launch_ms;          /* admitted -> kernels enqueued (host) */
+    double p99_gpu_ms;             /* enqueued -> edge count read back */
+    double first_submit_s, last_done_s;               /* steady clock, seconds */
+} csaw_server_stats;
+int csaw_server_create(csaw_graph g, const csaw_server_config *cfg, csaw_server *out);
+/* Waits for every submitted request, then frees the server. */
+int csaw_server_destroy(csaw_server s);
+/* Copies params and seeds (host; seed count as csaw_sample: n_samples x
+ * frontier_size, or n_samples walks); outputs are host buffers of `capacity`
+ * edges each (out_sample / out_depth may be NULL) that must stay valid until
+ * the request is waited for.  Fails at once (CSAW_ERR_CAPACITY) if the
+ * request alone exceeds the device budget. */
+int csaw_server_submit(csaw_server s, const csaw_params *p, const int32_t *seeds, int32_t *out_src,
+                       int32_t *out_dst, int32_t *out_sample, int32_t *out_depth, int64_t capacity,
+                       uint64_t *ticket);
+/* Waits up to timeout_us (< 0: forever) for the request; returns its status
+ * (CSAW_PENDING if still running, the ticket stays valid), its edge count
+ * and latency.  A finished ticket is released by the call that reports it. */
+int csaw_server_wait(csaw_server s, uint64_t ticket, int64_t timeout_us, int64_t *n_out, double *latency_ms);
+/* Counters and latency percentiles; reset != 0 clears the latency record. */
+int csaw_server_get_stats(csaw_server s, int reset, csaw_server_stats *out);
 
 /*
  * Reference-compatible entry (Sampler, non-stream/main.cu:196-308): loads

@@ -135,3 +135,16 @@ def test_cache_rebuilt_for_other_bias(csaw, skewed_hubs):
         b = run_oracle(g, 0, bias, 128, 1, [32, 6], 7 + bias, seeds)
         assert_parity(a, b)
     G.close()
+
+
+def test_plain_schedule_after_cache_built(csaw, skewed_hubs):
+    """A batched job builds the cache; plain jobs on the same graph (which do
+    not see it unless asked) still equal the oracle, walks and neighbors."""
+    g = skewed_hubs
+    G = csaw.Graph(g)
+    seeds = np.concatenate([np.arange(8, dtype=np.int32), oracle.make_seeds(g.rowptr, 120, 4)]).astype(np.int32)
+    for mode, fan, sched in ((0, [32, 6], 1), (1, [1] * 20, 0), (0, [32, 6], 0), (1, [1] * 20, 1)):
+        a = run_gpu(csaw, G, mode, 2, 128, 1, fan, 5, seeds, sched)
+        b = run_oracle(g, mode, 2, 128, 1, fan, 5, seeds)
+        assert_parity(a, b)
+    G.close()
