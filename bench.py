@@ -361,6 +361,80 @@ def serving(args, n_slots=8):
     return res
 
 
+SCALE25_GRAPH = dict(scale=25, edge_factor=16, a=0.6, b=0.2, c=0.15, seed=25, symmetrize=False,
+                     weight="pareto:1.5")
+
+
+def scale25(args):
+    """Learned scheduler at scale: R-MAT (a=.6, b=.2, c=.15) scale 25, edge
+    factor 16, directed, int64 rowptr, int32 col, Pareto(1.5) weights
+    (generated on the GPU); one step = 65,536 edge-weight-biased samples
+    (F 8, N 10, D 3) and 1M edge-weight-biased walks of length 40 as one
+    batch.  The batched (degree rule) and learned forms are timed; the
+    learned one is trained on profiles recorded on warm-up steps."""
+    import torch
+    import csaw
+    from csaw import graphgen
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    g = graphgen.rmat_device(**SCALE25_GRAPH)
+    gen_s = time.perf_counter() - t0
+    torch.cuda.empty_cache()
+    G = csaw.Graph(g, rowptr64=True)
+    seeds_a = G.make_seeds(65536 * 8, 0x25A)
+    seeds_b = G.make_seeds(1 << 20, 0x25B)
+    res = {"graph": {"workload": "rmat25_ef16_a.6_b.2_c.15_pareto1.5", "n_vertices": g.n_vertices,
+                     "n_edges": g.n_edges, "max_degree": int(np.diff(g.rowptr).max()), "generate_s": gen_s},
+           "a": dict(mode=0, bias=2, n_samples=65536, frontier_size=8, neighbor_size=10, depth=3),
+           "b": dict(mode=1, bias=2, n_samples=1 << 20, depth=40)}
+    del g
+    peak, peak_kind = load_peaks()
+    outs = {}
+    for form, sch in (("batched", csaw.SCHED_BATCHED), ("learned", csaw.SCHED_LEARNED)):
+        pa = csaw.make_params(0, 2, 65536, 8, 10, 3, seed=0x25A, schedule=sch)
+        pb = csaw.make_params(1, 2, 1 << 20, 1, 1, 40, seed=0x25B, schedule=sch)
+        if "a" not in outs:
+            outs["a"] = torch.empty((3, csaw.edge_bound(pa)), dtype=torch.int32, device="cuda")
+            outs["b"] = torch.empty((3, csaw.edge_bound(pb)), dtype=torch.int32, device="cuda")
+        jobs = [csaw.BatchJob(pa, seeds_a, outs["a"].shape[1], outs["a"], with_depth=False),
+                csaw.BatchJob(pb, seeds_b, outs["b"].shape[1], outs["b"], with_depth=False)]
+        r = {}
+        if form == "learned":
+            G.sched_record(400_000)
+            for _ in range(2):
+                G.sample_batch(jobs)
+            r["train_loss"] = G.sched_train(epochs=400, lr=3e-3, seed=1)
+            r["class_mask"] = G.sched_info()["class_mask"]
+        for _ in range(args.warmup):
+            G.sample_batch(jobs)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        n = 0
+        for _ in range(args.steps):
+            res_b = G.sample_batch(jobs)
+            n += res_b[0][0].numel() + res_b[1][0].numel()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        G.profile(True)
+        G.sample_batch(jobs)
+        ks = {k: G.kernel_stats(k) for k in ("expand", "select", "heavy", "walk", "setup")}
+        G.profile(False)
+        tot_bytes = sum(v["bytes"] for v in ks.values())
+        r.update({"ms_per_step": ms, "edges_per_step": n / args.steps, "seps": n / args.steps / (ms * 1e-3),
+                  "algorithmic_bytes_per_step": tot_bytes,
+                  "achieved_gbs": tot_bytes / (ms * 1e-3) / 1e9,
+                  "roofline_frac": tot_bytes / (ms * 1e-3) / 1e9 / peak,
+                  "kernels": {k: v for k, v in ks.items() if v["launches"]}})
+        res[form] = r
+    res["peak_gbs"] = peak
+    res["peak_source"] = peak_kind
+    res["learned_speedup"] = res["batched"]["ms_per_step"] / res["learned"]["ms_per_step"]
+    G.close()
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -371,6 +445,8 @@ def main():
     ap.add_argument("--learned-gain", action="store_true",
                     help="time the degree rule vs the learned scheduler on a heavy-tailed R-MAT graph instead")
     ap.add_argument("--serve", action="store_true", help="run only the serving (request loop) workload")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving workload in the default run")
+    ap.add_argument("--scale25", action="store_true", help="run only the R-MAT scale-25 learned-scheduler workload")
     ap.add_argument("--serve-requests", type=int, default=4000, help="requests per serving stream")
     ap.add_argument("--forms", default="plain,batched,learned",
                     help="forms to time; the last one is reported as value (profiling runs use one form)")
@@ -382,6 +458,9 @@ def main():
         return
     if args.learned_gain:
         learned_gain(args)
+        return
+    if args.scale25:
+        print(json.dumps({"scale25": scale25(args)}))
         return
     if args.serve:
         import torch
@@ -564,6 +643,8 @@ def main():
                 "edges_per_step": all_edges / args.steps / world}
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(g)
+        if world == 1 and not args.no_serve:
+            line["serving"] = serving(args)
         print(json.dumps(line))
     G.close()
     if world > 1:
