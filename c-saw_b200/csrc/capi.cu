@@ -102,7 +102,7 @@ int ensure(DevBuf &b, size_t bytes, cudaStream_t st = nullptr) {
 }
 
 constexpr int64_t QUEUE_ITEM_BUDGET = 32ll << 20;   // items per ping-pong queue
-constexpr int64_t SCRATCH_BUDGET = 1ll << 30;        // bytes of high-degree scratch
+constexpr int64_t SCRATCH_BUDGET = 4ll << 30;        // bytes of high-degree scratch (CTA prefix rebuilds)
 constexpr int MDRW_MAX_F = 4096;
 
 // Per-job device state: counters, frontier queues, work lists and scratch.
@@ -187,6 +187,8 @@ DevGraph dev_view(const csaw_graph_s *g, int schedule = CSAW_SCHED_BATCHED, int 
     d.ebias = (schedule != CSAW_SCHED_PLAIN || g->ebias_flag) ? g->ebias : nullptr;
     const bool fast = schedule != CSAW_SCHED_PLAIN;
     d.cdf = ((fast || g->cdf_flag) && bias > 0 && bias < 4) ? g->cdf[bias] : nullptr;
+    d.cdf1 = d.cdf ? d.cdf + g->E : nullptr;
+    d.cdf2 = d.cdf ? d.cdf + g->E + ((g->E + 31) >> 5) : nullptr;
     d.cdf_bias = bias;
     d.nbr_beg = fast ? g->nbr_beg : nullptr;
     d.nbr_deg = fast ? g->nbr_deg : nullptr;
@@ -273,9 +275,10 @@ template <typename I, int BIAS>
 int ensure_cdf(csaw_graph_s *g, cudaStream_t st) {
     if (g->cdf[BIAS]) return 0;
     if (g->E == 0 || g->cdf_off) return 0;
-    float *cdf = nullptr;
+    float *cdf = nullptr;   // prefix [E], then its search index levels [n1] and [n2]
+    const int64_t n1 = (g->E + 31) >> 5, n2 = (g->E + 1023) >> 10;
     ++g_alloc_epoch;
-    CK(cudaMalloc((void **)&cdf, sizeof(float) * (size_t)g->E));
+    CK(cudaMalloc((void **)&cdf, sizeof(float) * (size_t)(g->E + n1 + n2)));
     const DevGraph dg = dev_view(g);
     {
         LaunchScope ls(g, KK_INIT, st);
@@ -290,10 +293,14 @@ int ensure_cdf(csaw_graph_s *g, cudaStream_t st) {
         k_cdf_build_big<I, BIAS><<<blocks, 1024, 0, st>>>(dg, cdf, g->big_verts, (int)g->n_big, scratch, stride);
         CK(cudaFreeAsync(scratch, st));
     }
+    {
+        LaunchScope ls(g, KK_INIT, st);
+        k_cdf_index<<<g->sm_count * 4, 256, 0, st>>>(cdf, g->E, cdf + g->E, n1, cdf + g->E + n1, n2);
+    }
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));
     g->cdf[BIAS] = cdf;
-    g->dev_bytes += 4 * g->E;
+    g->dev_bytes += 4 * (g->E + n1 + n2);
     ++g_alloc_epoch;
     return 0;
 }
@@ -589,11 +596,19 @@ int run_walk_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int32_t *
     if (BIAS == CSAW_BIAS_UNBIASED) {
         int grid = (p->n_samples + WALK_THREADS - 1) / WALK_THREADS;
         int gmax = plain ? grid_for(k_walk_thread<I>, WALK_THREADS, 0, g->sm_count)
-                         : grid_for(k_walk_thread_fast<I>, WALK_THREADS, 0, g->sm_count);
+                         : grid_for(k_walk_thread_fast<I, CSAW_BIAS_UNBIASED>, WALK_THREADS, 0, g->sm_count);
         if (grid > gmax) grid = gmax;
         LaunchScope ls(g, KK_WALK, st);
         if (plain) k_walk_thread<I><<<grid, WALK_THREADS, 0, st>>>(dg, a);
-        else k_walk_thread_fast<I><<<grid, WALK_THREADS, 0, st>>>(dg, a);
+        else k_walk_thread_fast<I, CSAW_BIAS_UNBIASED><<<grid, WALK_THREADS, 0, st>>>(dg, a);
+    } else if (!plain && dg.cdf && (int64_t)p->n_samples >= 16ll * grid_for(k_walk_fast<I, BIAS>, FAST_THREADS, 0,
+                                                                               g->sm_count) * (FAST_THREADS / 32)) {
+        // many biased walks over a cached prefix: one thread per walk
+        int grid = (p->n_samples + WALK_THREADS - 1) / WALK_THREADS;
+        const int gmax = grid_for(k_walk_thread_fast<I, BIAS>, WALK_THREADS, 0, g->sm_count);
+        if (grid > gmax) grid = gmax;
+        LaunchScope ls(g, KK_WALK, st);
+        k_walk_thread_fast<I, BIAS><<<grid, WALK_THREADS, 0, st>>>(dg, a);
     } else {
         int gmax = plain ? grid_for(k_walk_warp<I, BIAS>, WALK_THREADS, 0, g->sm_count)
                          : grid_for(k_walk_fast<I, BIAS>, FAST_THREADS, 0, g->sm_count);

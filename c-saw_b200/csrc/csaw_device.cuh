@@ -22,6 +22,8 @@ struct DevGraph {
     csaw_graph_view v;     // what the user hooks see
     const float *ebias;    // materialised neighbor degree per edge, or null
     const float *cdf;      // canonical per-vertex prefix of cdf_bias, or null
+    const float *cdf1;     // cdf[32k + 31] (search index, level 1), with cdf
+    const float *cdf2;     // cdf[1024u + 1023] (search index, level 2), with cdf
     int cdf_bias;          // bias kind the cdf was built for
     // Per-edge neighbor records (batched schedules): row begin and degree of
     // col[e], so a selected neighbor carries its own adjacency range and the
@@ -114,6 +116,37 @@ __device__ __forceinline__ int64_t warp_search_upper(const float *P, int64_t d, 
     const int64_t idx = lo + lane;
     const bool up = idx >= hi - 1 || __ldg(P + idx) > t;
     return lo + (__ffs(__ballot_sync(FULL, up)) - 1);
+}
+
+// First i in [0, d) with P[i] > t for the row of global edge offset beg of a
+// cached prefix, through its two index levels: a binary search of the
+// row's 1024-edge groups in cdf2 (E/1024 floats, L2-resident), then of the
+// group's 32-edge tiles in cdf1 and of the tile in cdf (each one 128-byte
+// line).  Every probe lies inside the row; the last candidate of each level
+// is known to exceed t (it ends the row, or ends the previous level's pick).
+__device__ __forceinline__ int64_t cdf_search(const DevGraph &g, int64_t beg, int64_t d, float t) {
+    const int64_t end = beg + d;
+    const int64_t ua = beg >> 10, ub = (end - 1) >> 10;
+    const int64_t u = ua + search_upper(g.cdf2 + ua, ub - ua + 1, t);
+    const int64_t ka = (u << 5) > (beg >> 5) ? (u << 5) : (beg >> 5);
+    const int64_t kb = (u << 5) + 31 < ((end - 1) >> 5) ? (u << 5) + 31 : ((end - 1) >> 5);
+    const int64_t k = ka + search_upper(g.cdf1 + ka, kb - ka + 1, t);
+    const int64_t ia = (k << 5) > beg ? (k << 5) : beg;
+    const int64_t ib = (k << 5) + 31 < end - 1 ? (k << 5) + 31 : end - 1;
+    return ia + search_upper(g.cdf + ia, ib - ia + 1, t) - beg;
+}
+
+// The same with one warp-uniform target, each level by warp_search_upper.
+__device__ __forceinline__ int64_t warp_cdf_search(const DevGraph &g, int64_t beg, int64_t d, float t, int lane) {
+    const int64_t end = beg + d;
+    const int64_t ua = beg >> 10, ub = (end - 1) >> 10;
+    const int64_t u = ua + warp_search_upper(g.cdf2 + ua, ub - ua + 1, t, lane);
+    const int64_t ka = (u << 5) > (beg >> 5) ? (u << 5) : (beg >> 5);
+    const int64_t kb = (u << 5) + 31 < ((end - 1) >> 5) ? (u << 5) + 31 : ((end - 1) >> 5);
+    const int64_t k = ka + warp_search_upper(g.cdf1 + ka, kb - ka + 1, t, lane);
+    const int64_t ia = (k << 5) > beg ? (k << 5) : beg;
+    const int64_t ib = (k << 5) + 31 < end - 1 ? (k << 5) + 31 : end - 1;
+    return ia + warp_search_upper(g.cdf + ia, ib - ia + 1, t, lane) - beg;
 }
 
 // ------------------------------------------------------------ warp scans

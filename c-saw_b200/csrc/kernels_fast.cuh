@@ -233,6 +233,50 @@ __device__ __forceinline__ int select_smem(const float *W, int d, int N, const D
     return select_spec(N, lane, dc, !(T > 0.f), cand_of, rebuild);
 }
 
+// Selection for 32 < d <= WF from the cached canonical prefix: the row's
+// prefix is copied to shared P (one coalesced pass, no scan); the raw biases
+// are loaded into W only if a rebuild is needed.  Same draws and result as
+// select_smem, since the cache holds exactly the prefix it would compute.
+template <typename I, int BIAS>
+__device__ __forceinline__ int select_cached(const DevGraph &g, int64_t beg, int d, int N, const DrawCtx &dc,
+                                             float *W, float *P, uint32_t *zb, int lane) {
+    const float *cp = g.cdf + beg;
+    for (int i0 = 0; i0 < d; i0 += 256) {
+        float r[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int i = i0 + u * 32 + lane;
+            r[u] = i < d ? __ldg(cp + i) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int i = i0 + u * 32 + lane;
+            if (i < d) P[i] = r[u];
+        }
+    }
+    __syncwarp();
+    float T = P[d - 1];
+    bool have_w = false;
+    auto cand_of = [&](uint32_t x, bool act) -> int {
+        return act ? (int)search_upper(P, d, its_target(x, T)) : -1;
+    };
+    auto rebuild = [&](const Spec4 &st, int j) -> bool {
+        if (!have_w) {
+            preload_bias<I, BIAS>(g, beg, d, W, lane);
+            have_w = true;
+        }
+        const int nwords = (d + 31) >> 5;
+        for (int w = lane; w < nwords; w += 32) zb[w] = 0u;
+        __syncwarp();
+        if (lane < j) atomicOr(&zb[st.sel >> 5], 1u << (st.sel & 31));
+        __syncwarp();
+        auto wfn = [&](int64_t i) { return W[i]; };
+        T = warp_canon_prefix(wfn, d, P, zb, lane);
+        return T > 0.f;
+    };
+    return select_spec(N, lane, dc, !(T > 0.f), cand_of, rebuild);
+}
+
 // Unbiased selection (no prefix): index ranks over the non-excluded range.
 __device__ __forceinline__ int select_unbiased(int64_t d, int N, const DrawCtx &dc, int *zs, int lane) {
     int nZ = 0;
@@ -471,6 +515,8 @@ k_select_fast(DevGraph g, LevelArgs a) {
         } else {
             if (en.cls == 0) {
                 sel = select_reg<I, BIAS>(g, beg, (int)d, N, dc, lane);
+            } else if (cached && d <= WF) {
+                sel = select_cached<I, BIAS>(g, beg, (int)d, N, dc, W, P, zb, lane);
             } else if (d > WF) {   // cached prefix (only cached items above WF reach here)
                 sel = select_warp<I, BIAS>(g, beg, d, N, dc, P, zb, zs, lane, WF);
                 if (sel == -2) {   // needs a rebuild that does not fit: retried by the CTA pass
@@ -491,7 +537,7 @@ k_select_fast(DevGraph g, LevelArgs a) {
         }
         if (lane == 0) {
             my_items++;
-            my_bytes += 16 + (BIASED && !(cached && d > WF) ? 4ull * d : 0ull) +
+            my_bytes += 16 + (BIASED && !(cached && d > WF) ? 4ull * d : 0ull) +   // weights, or cached prefix row
                         (unsigned long long)N * (4ull + 4ull * nout + (a.push ? 12ull + 2 * (sizeof(I) + 4) : 0ull));
         }
     }
@@ -592,7 +638,9 @@ k_walk_fast(DevGraph g, WalkArgs a) {
             } else if (cached) {
                 const float *cp = g.cdf + beg;
                 const float T = __ldg(cp + d - 1);
-                e = beg + (T > 0.f ? warp_search_upper(cp, d, its_target(x, T), lane) : 0);
+                const float tt = its_target(x, T);
+                e = beg + (!(T > 0.f) ? 0 : (d > 1024 ? warp_cdf_search(g, beg, d, tt, lane)
+                                                       : warp_search_upper(cp, d, tt, lane)));
                 bytes += 4ull * 32 * ((68 - __clzll((unsigned long long)d)) / 5);   // 32 probes per round
             } else if (d <= WF) {
                 preload_bias<I, BIAS>(g, beg, d, W, lane);
@@ -646,11 +694,15 @@ k_walk_fast(DevGraph g, WalkArgs a) {
     }
 }
 
-// Unbiased walks, one thread per walk, one round trip per step via the
-// neighbor records.
-template <typename I>
+// Walks with one thread per walk, for many walks: unbiased steps take one
+// round trip via the neighbor records; biased steps search the cached prefix
+// (the graph must hold it for BIAS) by binary search through its index, so a
+// warp keeps 32 walks in flight instead of one.  Same draws as the warp
+// kernels: step t of walk w uses word x of Philox(0, w, t).
+template <typename I, int BIAS>
 __global__ void __launch_bounds__(WALK_THREADS)
 k_walk_thread_fast(DevGraph g, WalkArgs a) {
+    constexpr bool BIASED = BIAS != CSAW_BIAS_UNBIASED;
     __shared__ int32_t s_out[(WALK_THREADS / 32) * 4 * STAGE];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     WarpStage stg;
@@ -660,7 +712,7 @@ k_walk_thread_fast(DevGraph g, WalkArgs a) {
     stg.s_dep = stg.s_smp + STAGE;
     const OutArgs oa{a.o_src, a.o_dst, a.o_smp, a.o_dep, a.o_count, a.cap};
     const int stride = gridDim.x * blockDim.x;
-    unsigned long long steps = 0;
+    unsigned long long steps = 0, probes = 0;
     for (int base = blockIdx.x * blockDim.x; base < a.n; base += stride) {
         const int w = base + threadIdx.x;
         bool alive = w < a.n;
@@ -685,7 +737,13 @@ k_walk_thread_fast(DevGraph g, WalkArgs a) {
                 uint32_t idx = 0;
                 if (d > 1) {
                     uint4 b = philox(make_uint4(0u, (uint32_t)(a.base + w), (TAG_SAMPLE << 24) | (uint32_t)t, 0u), a.k0, a.k1);
-                    idx = mulhi(b.x, (uint32_t)d);
+                    if constexpr (BIASED) {
+                        const float T = __ldg(g.cdf + beg + d - 1);
+                        if (T > 0.f) idx = (uint32_t)cdf_search(g, beg, d, its_target(b.x, T));
+                        probes += 1 + (64 - __clzll((unsigned long long)d));
+                    } else {
+                        idx = mulhi(b.x, (uint32_t)d);
+                    }
                 }
                 const int64_t e = beg + idx;
                 const int32_t u = __ldg(g.v.col + e);
@@ -706,11 +764,14 @@ k_walk_thread_fast(DevGraph g, WalkArgs a) {
         }
     }
     stg.flush(oa, lane);
-    unsigned long long tot = steps;
-    for (int off = 16; off; off >>= 1) tot += __shfl_xor_sync(FULL, tot, off);
+    unsigned long long tot = steps, pr = probes;
+    for (int off = 16; off; off >>= 1) {
+        tot += __shfl_xor_sync(FULL, tot, off);
+        pr += __shfl_xor_sync(FULL, pr, off);
+    }
     if (lane == 0) {
         unsigned long long per = 4 + sizeof(I) + 4 + 4ull * (2 + (a.o_smp != nullptr) + (a.o_dep != nullptr));
-        atomicAdd(&a.bytes[2], tot * per);
+        atomicAdd(&a.bytes[2], tot * per + 4 * pr);   // + prefix probes (biased)
         atomicAdd(&a.items[2], tot);
     }
 }

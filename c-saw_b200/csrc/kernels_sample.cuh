@@ -66,11 +66,11 @@ __device__ __forceinline__ int select_warp(const DevGraph &g, int64_t beg, int64
     auto wfn = [&](int64_t i) { return edge_bias<I, BIAS>(g, beg + i); };
     float T = 0.f;
     int nZ = 0;
-    const float *PP = P;
+    bool indexed = false;   // searching the cached prefix through its index
     if constexpr (BIASED) {
         if (g.cdf && g.cdf_bias == BIAS) {
-            PP = g.cdf + beg;
-            T = PP[d - 1];
+            indexed = true;
+            T = g.cdf[beg + d - 1];
         } else {
             T = warp_canon_prefix(wfn, d, P, nullptr, lane);
         }
@@ -79,8 +79,12 @@ __device__ __forceinline__ int select_warp(const DevGraph &g, int64_t beg, int64
     SelState st;
     auto cand_of = [&](uint32_t x, bool act) -> int {
         if (!act) return -1;
-        if constexpr (BIASED) return (int)search_upper(PP, d, its_target(x, T));
-        else return kth_not_excluded(mulhi(x, (uint32_t)(d - nZ)), zs, nZ);
+        if constexpr (BIASED) {
+            const float t = its_target(x, T);
+            return indexed ? (int)cdf_search(g, beg, d, t) : (int)search_upper(P, d, t);
+        } else {
+            return kth_not_excluded(mulhi(x, (uint32_t)(d - nZ)), zs, nZ);
+        }
     };
     bool zero = BIASED && !(T > 0.f);
     if (!zero) draw_pending(st, 0, N, lane, dc, rng, cand_of);
@@ -99,7 +103,7 @@ __device__ __forceinline__ int select_warp(const DevGraph &g, int64_t beg, int64
             if (lane < j) atomicOr(&zb[st.sel >> 5], 1u << (st.sel & 31));
             __syncwarp();
             T = warp_canon_prefix(wfn, d, P, zb, lane);
-            PP = P;
+            indexed = false;
             if (!(T > 0.f)) {
                 zero = true;
                 continue;
@@ -235,14 +239,15 @@ k_expand_heavy(DevGraph g, LevelArgs a) {
         float *gcar = tsum + (d >> 5) + 1;
         uint32_t *zb = (uint32_t *)(gcar + (d >> 10) + 1);
         auto wfn = [&](int64_t i) { return edge_bias<I, BIAS>(g, beg + i); };
-        const bool cached = g.cdf && g.cdf_bias == BIAS;
-        const float *PP = cached ? g.cdf + beg : P;
-        float T = cached ? PP[d - 1] : cta_canon_prefix(wfn, d, P, tsum, gcar, nullptr);
+        bool indexed = g.cdf && g.cdf_bias == BIAS;   // cached prefix, searched through its index
+        float T = indexed ? g.cdf[beg + d - 1] : cta_canon_prefix(wfn, d, P, tsum, gcar, nullptr);
         const DrawCtx dc{a.k0, a.k1, p, (uint32_t)s, (uint32_t)a.depth};
         SlotRng rng;
         SelState st;
         auto cand_of = [&](uint32_t x, bool act) -> int {
-            return act ? (int)search_upper(PP, d, its_target(x, T)) : -1;
+            if (!act) return -1;
+            const float t = its_target(x, T);
+            return indexed ? (int)cdf_search(g, beg, d, t) : (int)search_upper(P, d, t);
         };
         bool zero = !(T > 0.f);
         if (warp == 0 && !zero) draw_pending(st, 0, N, lane, dc, rng, cand_of);
@@ -265,7 +270,7 @@ k_expand_heavy(DevGraph g, LevelArgs a) {
             if (warp == 0 && lane < j) atomicOr(&zb[st.sel >> 5], 1u << (st.sel & 31));
             __syncthreads();
             T = cta_canon_prefix(wfn, d, P, tsum, gcar, zb);
-            PP = P;
+            indexed = false;
             if (warp == 0) {
                 if (!(T > 0.f)) zero = true;
                 else draw_pending(st, j, N, lane, dc, rng, cand_of);
@@ -425,11 +430,10 @@ k_walk_warp(DevGraph g, WalkArgs a) {
             int64_t idx = 0;
             bytes += 2 * sizeof(I) + 4 + obytes;
             if (d > 1) {
-                const float *PP;
+                const float *PP = nullptr;
                 float T;
                 if (cached) {
-                    PP = g.cdf + beg;
-                    T = PP[d - 1];
+                    T = g.cdf[beg + d - 1];
                     bytes += 4ull * (64 - __clzll((unsigned long long)d));
                 } else {
                     float *buf = P;
@@ -450,7 +454,10 @@ k_walk_warp(DevGraph g, WalkArgs a) {
                 if (T > 0.f) {
                     uint4 b = philox(make_uint4(0u, (uint32_t)(a.base + w), (TAG_SAMPLE << 24) | (uint32_t)t, 0u),
                                      a.k0, a.k1);
-                    idx = search_upper(PP, d, its_target(b.x, T));
+                    const float tt = its_target(b.x, T);
+                    if (!cached) idx = search_upper(PP, d, tt);
+                    else if (d > 1024) idx = warp_cdf_search(g, beg, d, tt, lane);
+                    else idx = warp_search_upper(g.cdf + beg, d, tt, lane);
                 }
             }
             int32_t dst = Update(&g.v, __ldg(g.v.col + beg + idx), v);
@@ -567,6 +574,19 @@ __global__ void k_cdf_build_big(DevGraph g, float *cdf, const int32_t *verts, in
         float *gcar = tsum + (d >> 5) + 1;
         auto wfn = [&](int64_t i) { return edge_bias<I, BIAS>(g, beg + i); };
         cta_canon_prefix(wfn, d, cdf + beg, tsum, gcar, nullptr);
+    }
+}
+
+// Search index of a built prefix cache: c1[k] = cdf[32k + 31] and
+// c2[u] = cdf[1024u + 1023] where those edges exist (others are never read).
+static __global__ void k_cdf_index(const float *cdf, int64_t E, float *c1, int64_t n1, float *c2, int64_t n2) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n1; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = (k << 5) + 31;
+        c1[k] = i < E ? cdf[i] : 0.f;
+        if (k < n2) {
+            const int64_t j = (k << 10) + 1023;
+            c2[k] = j < E ? cdf[j] : 0.f;
+        }
     }
 }
 

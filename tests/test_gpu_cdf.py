@@ -103,7 +103,7 @@ def test_hub_walk_parity(csaw, skewed_hubs, cache, schedule, bias):
 
 
 def test_cache_residency_policy(csaw, skewed_hubs):
-    """The batched schedule builds the cache (4E bytes) on first biased use of a
+    """The batched schedule builds the cache (4.13E bytes) on first biased use of a
     graph with hubs; the plain schedule does not unless asked; the opt-out
     flag keeps it off; an unbiased job never builds it."""
     g = skewed_hubs
@@ -118,9 +118,10 @@ def test_cache_residency_policy(csaw, skewed_hubs):
         G.close()
         return after - before
 
-    assert grows(None, 1, 2) - grows(False, 1, 2) == 4 * E   # batched also adds neighbor records
+    cache = 4 * (E + (E + 31) // 32 + (E + 1023) // 1024)   # prefix and its two search-index levels
+    assert grows(None, 1, 2) - grows(False, 1, 2) == cache   # batched also adds neighbor records
     assert grows(None, 0, 2) == 0
-    assert grows(True, 0, 2) == 4 * E
+    assert grows(True, 0, 2) == cache
     assert grows(None, 1, 0) == grows(False, 1, 0)
 
 
@@ -148,3 +149,18 @@ def test_plain_schedule_after_cache_built(csaw, skewed_hubs):
         b = run_oracle(g, mode, 2, 128, 1, fan, 5, seeds)
         assert_parity(a, b)
     G.close()
+
+
+@pytest.mark.parametrize("bias", [1, 2])
+def test_many_biased_walks_thread_per_walk(csaw, rmat12_pareto, powerlaw_small, bias):
+    """Enough biased walks on a cached prefix take the one-thread-per-walk
+    kernel; its edges equal the oracle's (hub graph, and a small-degree graph
+    with the cache forced on)."""
+    for g, cache, n, length in ((rmat12_pareto, None, 120_000, 8), (powerlaw_small, True, 100_000, 20)):
+        G = csaw.Graph(g, cdf_cache=cache)
+        seeds = oracle.make_seeds(g.rowptr, n, 21)
+        a = run_gpu(csaw, G, 1, bias, n, 1, [1] * length, 0xABC, seeds, 1)
+        b = run_oracle(g, 1, bias, n, 1, [1] * length, 0xABC, seeds)
+        assert len(a[0]) > n
+        assert_parity(a, b)
+        G.close()
