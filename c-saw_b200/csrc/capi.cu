@@ -51,7 +51,7 @@ int fail(int code, const std::string &msg) {
         if (rc_) return rc_;   \
     } while (0)
 
-enum { KK_EXPAND = 0, KK_HEAVY = 1, KK_WALK = 2, KK_MDRW = 3, KK_INIT = 4, KK_SELECT = 5, KK_COUNT = 8 };
+enum { KK_EXPAND = 0, KK_HEAVY = 1, KK_WALK = 2, KK_MDRW = 3, KK_INIT = 4, KK_SELECT = 5, KK_HUB = 6, KK_COUNT = 8 };
 
 struct Counters {
     unsigned long long out_count;
@@ -62,6 +62,7 @@ struct Counters {
     uint32_t n_sel;
     uint32_t n_cta[4];
     uint32_t n_retry;
+    uint32_t n_hub;
     int err;
 };
 
@@ -109,7 +110,7 @@ constexpr int MDRW_MAX_F = 4096;
 // Job 0 serves csaw_sample; csaw_sample_batch runs job i on context i, each
 // on its own stream, so independent jobs overlap on the device.
 struct JobCtx {
-    DevBuf q[2][5], heavy, sel, hlist, hscratch, wscratch, seeds_in, out_dev, cta[4], retry, stab;
+    DevBuf q[2][5], heavy, sel, hlist, hscratch, wscratch, seeds_in, out_dev, cta[4], retry, stab, hubsel;
     Counters *ctr = nullptr, *hctr = nullptr;
     cudaStream_t stream = nullptr;   // owned (batch jobs); job 0 uses the caller's
     cudaEvent_t done = nullptr;
@@ -414,13 +415,19 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
         }
     }
     const SchedArgs *sched = nullptr;
-    const int sgrid = plain ? 0 : grid_for(k_select_fast<I, BIAS>, FAST_THREADS, 0, g->sm_count);
+    const int hgrid = plain ? 0 : grid_for(k_select_hub<I, BIAS>, FAST_THREADS, 0, g->sm_count);
     if (BIASED && ((!plain && g->maxdeg > WF) || g->cdf_flag)) TRY((ensure_cdf<I, BIAS>(g, st)));
     const bool cached = BIASED && g->cdf[BIAS] && (!plain || g->cdf_flag);
+    const int sgrid = plain ? 0
+                      : (cached ? grid_for(k_select_fast<I, BIAS, true>, FAST_THREADS, 0, g->sm_count)
+                                : grid_for(k_select_fast<I, BIAS, false>, FAST_THREADS, 0, g->sm_count));
     if (!plain) {
         TRY(ensure_nbr(g, st));
         TRY(ensure(c->sel, sizeof(SelEntry) * qcap, st));
-        if (cached && g->maxdeg > WF) TRY(ensure(c->retry, sizeof(SelEntry) * qcap, st));
+        if (cached && g->maxdeg > WF) {
+            TRY(ensure(c->retry, sizeof(SelEntry) * qcap, st));
+            TRY(ensure(c->hubsel, sizeof(SelEntry) * qcap, st));
+        }
         if (p->schedule == CSAW_SCHED_LEARNED && BIASED) TRY((ensure_vstats<I, BIAS>(g, st)));
         TRY(sched_for(g, p->schedule, BIAS, sgrid * (FAST_THREADS / 32), st, &sched));
         for (int k = 0; k < 4; ++k)
@@ -477,7 +484,7 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
         for (int l = 0; l < D; ++l) {
             const int cur = l & 1, nxt = cur ^ 1;
             CK(cudaMemsetAsync(&c->ctr->nq[nxt], 0, sizeof(uint32_t), st));
-            CK(cudaMemsetAsync(&c->ctr->n_heavy, 0, 7 * sizeof(uint32_t), st));  // n_heavy, n_sel, n_cta[4], n_retry
+            CK(cudaMemsetAsync(&c->ctr->n_heavy, 0, 8 * sizeof(uint32_t), st));  // n_heavy .. n_hub
             LevelArgs a;
             a.in_v = (const int32_t *)c->q[cur][0].p;
             a.in_s = (const int32_t *)c->q[cur][1].p;
@@ -500,6 +507,8 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
             a.n_cta = c->ctr->n_cta;
             a.sched = sched;
             a.sched_tab = tabled ? (const uint8_t *)c->stab.p : nullptr;
+            a.hub_list = (SelEntry *)c->hubsel.p;
+            a.n_hub = &c->ctr->n_hub;
             a.retry_list = (SelEntry *)c->retry.p;
             a.n_retry = &c->ctr->n_retry;
             a.heavy_scratch = (float *)c->hscratch.p;
@@ -547,7 +556,12 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
             }
             if (!plain) {
                 LaunchScope ls(g, KK_SELECT, st);
-                k_select_fast<I, BIAS><<<sgrid, FAST_THREADS, 0, st>>>(dg, a);
+                if (cached) k_select_fast<I, BIAS, true><<<sgrid, FAST_THREADS, 0, st>>>(dg, a);
+                else k_select_fast<I, BIAS, false><<<sgrid, FAST_THREADS, 0, st>>>(dg, a);
+            }
+            if (!plain && cached && g->maxdeg > WF) {
+                LaunchScope ls(g, KK_HUB, st);
+                k_select_hub<I, BIAS><<<hgrid, FAST_THREADS, 0, st>>>(dg, a);
             }
             if (hblocks && plain) {
                 LaunchScope ls(g, KK_HEAVY, st);
@@ -712,7 +726,7 @@ void free_job(JobCtx *c) {
     for (auto &qq : c->q)
         for (auto &b : qq) cudaFree(b.p);
     for (DevBuf *b : {&c->heavy, &c->sel, &c->hlist, &c->hscratch, &c->wscratch, &c->seeds_in, &c->out_dev, &c->cta[0],
-                      &c->cta[1], &c->cta[2], &c->cta[3], &c->retry, &c->stab})
+                      &c->cta[1], &c->cta[2], &c->cta[3], &c->retry, &c->stab, &c->hubsel})
         cudaFree(b->p);
     cudaFree(c->ctr);
     if (c->hctr) cudaFreeHost(c->hctr);
@@ -729,7 +743,7 @@ int64_t job_workspace(const JobCtx *c) {
     for (auto &qq : c->q)
         for (auto &b : qq) ws += (int64_t)b.n;
     for (const DevBuf *b : {&c->heavy, &c->sel, &c->hlist, &c->hscratch, &c->wscratch, &c->seeds_in, &c->out_dev,
-                            &c->cta[0], &c->cta[1], &c->cta[2], &c->cta[3], &c->retry, &c->stab})
+                            &c->cta[0], &c->cta[1], &c->cta[2], &c->cta[3], &c->retry, &c->stab, &c->hubsel})
         ws += (int64_t)b->n;
     return ws;
 }
@@ -1298,7 +1312,7 @@ static int pick_classes(csaw_graph_s *g, int n) {
     uint32_t *m = nullptr;
     CK(cudaMalloc((void **)&m, sizeof(uint32_t)));
     CK(cudaMemset(m, 0, sizeof(uint32_t)));
-    const int slots = grid_for(k_select_fast<int32_t, CSAW_BIAS_EDGE_WEIGHT>, FAST_THREADS, 0, g->sm_count) *
+    const int slots = grid_for(k_select_fast<int32_t, CSAW_BIAS_EDGE_WEIGHT, false>, FAST_THREADS, 0, g->sm_count) *
                       (FAST_THREADS / 32);
     k_sched_pick<<<g->sm_count * 4, 256>>>(g->rec, n, g->mlp_wq, g->mlp_norm, slots, WF, m);
     uint32_t h = 0;

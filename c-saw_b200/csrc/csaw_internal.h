@@ -83,6 +83,8 @@ struct LevelArgs {
     uint32_t *n_cta;          //   and their counts
     int cta_class;            // class of the CTA launch (0..3), for profiles
     const uint8_t *sched_tab; // learned (trained): the level's decision table
+    SelEntry *hub_list;       // batched: items above WF searching a cached prefix
+    uint32_t *n_hub;
     SelEntry *retry_list;     // batched: cached hubs the warp pass handed back
     uint32_t *n_retry;
     const SchedArgs *sched;   // learned scheduler, or null (degree rule)

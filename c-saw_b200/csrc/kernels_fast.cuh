@@ -234,12 +234,12 @@ __device__ __forceinline__ int select_smem(const float *W, int d, int N, const D
 }
 
 // Selection for 32 < d <= WF from the cached canonical prefix: the row's
-// prefix is copied to shared P (one coalesced pass, no scan); the raw biases
-// are loaded into W only if a rebuild is needed.  Same draws and result as
-// select_smem, since the cache holds exactly the prefix it would compute.
+// prefix is copied to shared P (one coalesced pass, no scan); a rebuild reads
+// the raw biases from global memory.  Same draws and result as select_smem,
+// since the cache holds exactly the prefix it would compute.
 template <typename I, int BIAS>
 __device__ __forceinline__ int select_cached(const DevGraph &g, int64_t beg, int d, int N, const DrawCtx &dc,
-                                             float *W, float *P, uint32_t *zb, int lane) {
+                                             float *P, uint32_t *zb, int lane) {
     const float *cp = g.cdf + beg;
     for (int i0 = 0; i0 < d; i0 += 256) {
         float r[8];
@@ -256,21 +256,16 @@ __device__ __forceinline__ int select_cached(const DevGraph &g, int64_t beg, int
     }
     __syncwarp();
     float T = P[d - 1];
-    bool have_w = false;
     auto cand_of = [&](uint32_t x, bool act) -> int {
         return act ? (int)search_upper(P, d, its_target(x, T)) : -1;
     };
     auto rebuild = [&](const Spec4 &st, int j) -> bool {
-        if (!have_w) {
-            preload_bias<I, BIAS>(g, beg, d, W, lane);
-            have_w = true;
-        }
         const int nwords = (d + 31) >> 5;
         for (int w = lane; w < nwords; w += 32) zb[w] = 0u;
         __syncwarp();
         if (lane < j) atomicOr(&zb[st.sel >> 5], 1u << (st.sel & 31));
         __syncwarp();
-        auto wfn = [&](int64_t i) { return W[i]; };
+        auto wfn = [&](int64_t i) { return edge_bias<I, BIAS>(g, beg + i); };
         T = warp_canon_prefix(wfn, d, P, zb, lane);
         return T > 0.f;
     };
@@ -406,6 +401,8 @@ k_coop_fast(DevGraph g, LevelArgs a) {
             }
         }
         const bool heavy = drawn && cls >= 2;
+        // warp-class items above WF search the cached prefix: their own list
+        const bool hub = drawn && !heavy && cached && d > WF;
         const int incl = warp_incl_scan(k, lane);
         const int excl = incl - k;
         const int K = __shfl_sync(FULL, incl, 31);
@@ -420,13 +417,22 @@ k_coop_fast(DevGraph g, LevelArgs a) {
             qb = __shfl_sync(FULL, qb, 0);
         }
         // hand off items that need draws, with their reserved slots
-        const unsigned sm = __ballot_sync(FULL, drawn && !heavy);
+        const unsigned sm = __ballot_sync(FULL, drawn && !heavy && !hub);
         if (sm) {
             uint32_t pos = 0;
             if (lane == 0) pos = atomicAdd(a.n_sel, (uint32_t)__popc(sm));
             pos = __shfl_sync(FULL, pos, 0);
-            if (drawn && !heavy)
+            if (drawn && !heavy && !hub)
                 a.sel_list[pos + __popc(sm & ((1u << lane) - 1u))] =
+                    SelEntry{it, qb + (uint32_t)excl, ob + excl, v, s, p, (int32_t)d, (long long)beg, cls, 0};
+        }
+        const unsigned hbm = __ballot_sync(FULL, hub);
+        if (hbm) {
+            uint32_t pos = 0;
+            if (lane == 0) pos = atomicAdd(a.n_hub, (uint32_t)__popc(hbm));
+            pos = __shfl_sync(FULL, pos, 0);
+            if (hub)
+                a.hub_list[pos + __popc(hbm & ((1u << lane) - 1u))] =
                     SelEntry{it, qb + (uint32_t)excl, ob + excl, v, s, p, (int32_t)d, (long long)beg, cls, 0};
         }
 #pragma unroll
@@ -476,28 +482,30 @@ k_coop_fast(DevGraph g, LevelArgs a) {
     }
 }
 
-// Level expansion, part 2: one warp per listed item (N < d, and d <= WF when
-// biased without a CDF cache); writes into the slots reserved by part 1.
-template <typename I, int BIAS>
-__global__ void __launch_bounds__(FAST_THREADS, 4)
+// Level expansion, part 2: one warp per listed item (N < d <= WF when
+// biased); writes into the slots reserved by part 1.  CACHED: the graph holds
+// the prefix cache for BIAS, so no shared copy of the raw biases is kept
+// (half the shared memory, more resident warps).
+template <typename I, int BIAS, bool CACHED>
+__global__ void __launch_bounds__(FAST_THREADS, CACHED ? 6 : 4)
 k_select_fast(DevGraph g, LevelArgs a) {
     constexpr bool BIASED = BIAS != CSAW_BIAS_UNBIASED;
     constexpr int NW = FAST_THREADS / 32;
-    __shared__ float s_W[BIASED ? NW * WF : 1];
+    __shared__ float s_W[BIASED && !CACHED ? NW * WF : 1];
     __shared__ float s_P[BIASED ? NW * WF : 1];
     __shared__ uint32_t s_z[BIASED ? NW * (WF / 32) : 1];
     __shared__ int s_zs[NW * 32];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    float *W = s_W + (BIASED ? wib * WF : 0);
+    float *W = s_W + (BIASED && !CACHED ? wib * WF : 0);
     float *P = s_P + (BIASED ? wib * WF : 0);
     uint32_t *zb = s_z + (BIASED ? wib * (WF / 32) : 0);
     int *zs = s_zs + wib * 32;
     const uint32_t n = *a.n_sel;
     const uint32_t n_level = *a.n_in;
     const int N = a.N;
-    const bool cached = BIASED && g.cdf && g.cdf_bias == BIAS;
+    constexpr bool cached = BIASED && CACHED;
     const int nout = 2 + (a.o_smp != nullptr) + (a.o_dep != nullptr);
     unsigned long long my_bytes = 0, my_items = 0;
     for (uint32_t i = gw; i < n; i += nw) {
@@ -515,13 +523,15 @@ k_select_fast(DevGraph g, LevelArgs a) {
         } else {
             if (en.cls == 0) {
                 sel = select_reg<I, BIAS>(g, beg, (int)d, N, dc, lane);
-            } else if (cached && d <= WF) {
-                sel = select_cached<I, BIAS>(g, beg, (int)d, N, dc, W, P, zb, lane);
-            } else if (d > WF) {   // cached prefix (only cached items above WF reach here)
-                sel = select_warp<I, BIAS>(g, beg, d, N, dc, P, zb, zs, lane, WF);
-                if (sel == -2) {   // needs a rebuild that does not fit: retried by the CTA pass
-                    if (lane == 0) a.retry_list[atomicAdd(a.n_retry, 1u)] = en;
-                    continue;
+            } else if constexpr (CACHED) {
+                if (d <= WF) {
+                    sel = select_cached<I, BIAS>(g, beg, (int)d, N, dc, P, zb, lane);
+                } else {   // hubs are listed for k_select_hub; kept for completeness
+                    sel = select_warp<I, BIAS>(g, beg, d, N, dc, P, zb, zs, lane, WF);
+                    if (sel == -2) {   // needs a rebuild that does not fit: retried by the CTA pass
+                        if (lane == 0) a.retry_list[atomicAdd(a.n_retry, 1u)] = en;
+                        continue;
+                    }
                 }
             } else {
                 preload_bias<I, BIAS>(g, beg, (int)d, W, lane);
@@ -544,6 +554,55 @@ k_select_fast(DevGraph g, LevelArgs a) {
     if (lane == 0 && my_items) {
         atomicAdd(&a.bytes[5], my_bytes);
         atomicAdd(&a.items[5], my_items);
+    }
+}
+
+// Level expansion, part 2 for hub items (d > WF) over a cached prefix: one
+// warp per item, each draw a search of the prefix through its index
+// (cdf_search) taken one attempt at a time, since a search costs dependent
+// loads; no shared memory.  An item whose draws need a rebuild of its prefix
+// goes to the retry list (the CTA pass rebuilds it in global scratch).
+template <typename I, int BIAS>
+__global__ void __launch_bounds__(FAST_THREADS, 6)
+k_select_hub(DevGraph g, LevelArgs a) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t n = *a.n_hub;
+    const uint32_t n_level = *a.n_in;
+    const int N = a.N;
+    const int nout = 2 + (a.o_smp != nullptr) + (a.o_dep != nullptr);
+    unsigned long long my_bytes = 0, my_items = 0;
+    for (uint32_t i = gw; i < n; i += nw) {
+        const SelEntry en = a.hub_list[i];
+        const DrawCtx dc{a.k0, a.k1, en.p, (uint32_t)en.s, (uint32_t)a.depth};
+        const bool rec = a.sched && a.sched->mode == SCHED_RECORD;
+        long long t0 = 0;
+        if (rec) t0 = clock64();
+        const int sel = select_warp<I, BIAS>(g, en.beg, en.d, N, dc, nullptr, nullptr, nullptr, lane, 0);
+        if (sel == -2) {
+            if (lane == 0) a.retry_list[atomicAdd(a.n_retry, 1u)] = en;
+            continue;
+        }
+        if (lane < N)
+            emit_edge<I>(g, a, en.beg + sel, en.v, en.s, en.p * (uint32_t)N + (uint32_t)lane, (int64_t)en.ob + lane,
+                         en.q + (uint32_t)lane);
+        if (rec) {
+            __syncwarp();
+            if (lane == 0)
+                record_profile(a.sched, en.d, N, a.sched->vstats[en.v], n_level, a.depth, en.cls, clock64() - t0);
+        }
+        if (lane == 0) {
+            my_items++;
+            // per draw: one 4-byte prefix probe per halving of the row (the
+            // index levels split the same search), then the edge's records
+            my_bytes += 16 + (unsigned long long)N * (4ull * (64 - __clzll((unsigned long long)en.d)) + 4ull +
+                                                      4ull * nout + (a.push ? 12ull + 2 * (sizeof(I) + 4) : 0ull));
+        }
+    }
+    if (lane == 0 && my_items) {
+        atomicAdd(&a.bytes[6], my_bytes);
+        atomicAdd(&a.items[6], my_items);
     }
 }
 
