@@ -207,6 +207,8 @@ def learned_gain(args):
                 for _ in range(3):
                     G.sample_batch(job)
                 r["train_loss"] = G.sched_train(epochs=400, lr=3e-3, seed=1)
+                for _ in range(6):   # timed trial of the model against the degree rule
+                    G.sample_batch(job)
                 r["class_mask"] = G.sched_info()["class_mask"]
             for _ in range(args.warmup):
                 G.sample_batch(job)
@@ -377,22 +379,26 @@ def scale25(args):
     from csaw import graphgen
     torch.cuda.set_device(0)
     t0 = time.perf_counter()
-    g = graphgen.rmat_device(**SCALE25_GRAPH)
+    sc = args.s25_scale
+    g = graphgen.rmat_device(**dict(SCALE25_GRAPH, scale=sc))
     gen_s = time.perf_counter() - t0
     torch.cuda.empty_cache()
     G = csaw.Graph(g, rowptr64=True)
-    seeds_a = G.make_seeds(65536 * 8, 0x25A)
-    seeds_b = G.make_seeds(1 << 20, 0x25B)
-    res = {"graph": {"workload": "rmat25_ef16_a.6_b.2_c.15_pareto1.5", "n_vertices": g.n_vertices,
+    ns, nw = 65536 >> (25 - sc), (1 << 20) >> (25 - sc)
+    seeds_a = G.make_seeds(ns * 8, 0x25A)
+    seeds_b = G.make_seeds(nw, 0x25B)
+    res = {"graph": {"workload": f"rmat{sc}_ef16_a.6_b.2_c.15_pareto1.5", "n_vertices": g.n_vertices,
                      "n_edges": g.n_edges, "max_degree": int(np.diff(g.rowptr).max()), "generate_s": gen_s},
-           "a": dict(mode=0, bias=2, n_samples=65536, frontier_size=8, neighbor_size=10, depth=3),
-           "b": dict(mode=1, bias=2, n_samples=1 << 20, depth=40)}
+           "a": dict(mode=0, bias=2, n_samples=ns, frontier_size=8, neighbor_size=10, depth=3),
+           "b": dict(mode=1, bias=2, n_samples=nw, depth=40)}
     del g
     peak, peak_kind = load_peaks()
     outs = {}
-    for form, sch in (("batched", csaw.SCHED_BATCHED), ("learned", csaw.SCHED_LEARNED)):
-        pa = csaw.make_params(0, 2, 65536, 8, 10, 3, seed=0x25A, schedule=sch)
-        pb = csaw.make_params(1, 2, 1 << 20, 1, 1, 40, seed=0x25B, schedule=sch)
+    forms = [f for f in (("batched", csaw.SCHED_BATCHED), ("learned", csaw.SCHED_LEARNED))
+             if f[0] in args.s25_forms.split(",")]
+    for form, sch in forms:
+        pa = csaw.make_params(0, 2, ns, 8, 10, 3, seed=0x25A, schedule=sch)
+        pb = csaw.make_params(1, 2, nw, 1, 1, 40, seed=0x25B, schedule=sch)
         if "a" not in outs:
             outs["a"] = torch.empty((3, csaw.edge_bound(pa)), dtype=torch.int32, device="cuda")
             outs["b"] = torch.empty((3, csaw.edge_bound(pb)), dtype=torch.int32, device="cuda")
@@ -404,6 +410,8 @@ def scale25(args):
             for _ in range(2):
                 G.sample_batch(jobs)
             r["train_loss"] = G.sched_train(epochs=400, lr=3e-3, seed=1)
+            for _ in range(6):   # timed trial of the model against the degree rule
+                G.sample_batch(jobs)
             r["class_mask"] = G.sched_info()["class_mask"]
         for _ in range(args.warmup):
             G.sample_batch(jobs)
@@ -430,7 +438,8 @@ def scale25(args):
         res[form] = r
     res["peak_gbs"] = peak
     res["peak_source"] = peak_kind
-    res["learned_speedup"] = res["batched"]["ms_per_step"] / res["learned"]["ms_per_step"]
+    if "batched" in res and "learned" in res:
+        res["learned_speedup"] = res["batched"]["ms_per_step"] / res["learned"]["ms_per_step"]
     G.close()
     return res
 
@@ -447,6 +456,9 @@ def main():
     ap.add_argument("--serve", action="store_true", help="run only the serving (request loop) workload")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving workload in the default run")
     ap.add_argument("--scale25", action="store_true", help="run only the R-MAT scale-25 learned-scheduler workload")
+    ap.add_argument("--s25-scale", type=int, default=25,
+                    help="R-MAT scale for --scale25 (samples and walks scale with 2^scale; smaller for profiling)")
+    ap.add_argument("--s25-forms", default="batched,learned", help="forms timed by --scale25")
     ap.add_argument("--serve-requests", type=int, default=4000, help="requests per serving stream")
     ap.add_argument("--forms", default="plain,batched,learned",
                     help="forms to time; the last one is reported as value (profiling runs use one form)")
@@ -554,8 +566,11 @@ def main():
             step("learned")
         t0 = time.perf_counter()
         loss = G.sched_train(epochs=400, lr=3e-3, seed=rank)
-        sched = {"records": G.sched_info()["records"], "train_loss": loss,
-                 "train_s": time.perf_counter() - t0}
+        train_s = time.perf_counter() - t0
+        for _ in range(6):   # timed trial of the model against the degree rule
+            step("learned")
+        sched = {"records": G.sched_info()["records"], "train_loss": loss, "train_s": train_s,
+                 "class_mask": G.sched_info()["class_mask"]}
     # per-kernel events for the roofline come from a profiled pass of the same
     # steps; the reported value is the unprofiled pass (graph replay allowed)
     _, prof_ms, kstats, _, _ = timed(main_form, profile=True)

@@ -116,6 +116,8 @@ struct JobCtx {
     cudaEvent_t done = nullptr;
     cudaStream_t side = nullptr;     // CTA-granularity pass, concurrent with the warp pass
     cudaEvent_t fork = nullptr, join = nullptr;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;   // timed learned-schedule trial runs
+    int trial_arm = -1;                       // arm this job ran under, or -1
 };
 
 }  // namespace
@@ -167,6 +169,13 @@ struct csaw_graph_s {
     int64_t max_rec = 0;
     bool recording = false, trained = false;
     float last_loss = -1.f;
+    // After training, learned jobs alternate between the model's routing
+    // (arm 1) and the degree rule (arm 0), timed on the device, until each
+    // arm has TRIAL_RUNS runs; the model is kept only if its mean is lower.
+    bool trial = false, mlp_lost = false;
+    int trial_arm = 1;
+    int trial_n[2] = {};
+    double trial_ms[2] = {};
     SchedArgs *d_sched = nullptr;     // device copy read by the kernels
     SchedArgs sched_host{};           // what d_sched holds
     bool sched_valid = false;
@@ -328,8 +337,10 @@ int sched_for(csaw_graph_s *g, int schedule, int bias, int warp_slots, cudaStrea
     *out = nullptr;
     if (schedule != CSAW_SCHED_LEARNED || bias == CSAW_BIAS_UNBIASED) return 0;
     SchedArgs h{};
-    // a trained model that picks no CTA class routes exactly as the degree rule
-    const bool routes = g->trained && (g->class_mask & 0x3cu);
+    // a trained model that picks no CTA class routes exactly as the degree
+    // rule; one that lost its timed trial is not used
+    bool routes = g->trained && (g->class_mask & 0x3cu) && !g->mlp_lost;
+    if (routes && g->trial) routes = g->trial_arm == 1;
     h.mode = g->recording ? SCHED_RECORD : (routes ? SCHED_MLP : SCHED_THRESHOLD);
     h.wq = g->mlp_wq;
     h.norm = g->mlp_norm;
@@ -735,6 +746,8 @@ void free_job(JobCtx *c) {
     if (c->side) cudaStreamDestroy(c->side);
     if (c->fork) cudaEventDestroy(c->fork);
     if (c->join) cudaEventDestroy(c->join);
+    if (c->t0) cudaEventDestroy(c->t0);
+    if (c->t1) cudaEventDestroy(c->t1);
     delete c;
 }
 
@@ -769,17 +782,62 @@ int enqueue_job(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int32_t 
     if (p->n_samples > 0 && !seeds) return fail(CSAW_ERR_INVALID, "seeds is NULL");
     CK(cudaMemsetAsync(c->ctr, 0, sizeof(Counters), st));
     OutArgs o{src, dst, smp, dep, &c->ctr->out_count, cap};
+    c->trial_arm = -1;
+    const bool timed = g->trial && p->schedule == CSAW_SCHED_LEARNED && p->mode == CSAW_MODE_NEIGHBOR &&
+                       p->bias != CSAW_BIAS_UNBIASED && p->n_samples > 0 && p->depth > 0;
+    if (timed) {
+        if (!c->t0) CK(cudaEventCreate(&c->t0));
+        if (!c->t1) CK(cudaEventCreate(&c->t1));
+        CK(cudaEventRecord(c->t0, st));
+    }
     if (p->n_samples > 0 && p->depth > 0) {
         int rc = g->idx64 ? dispatch_bias<int64_t>(g, c, p, fan, seeds, o, st)
                           : dispatch_bias<int32_t>(g, c, p, fan, seeds, o, st);
         if (rc) return rc;
     }
+    if (timed) {
+        CK(cudaEventRecord(c->t1, st));
+        c->trial_arm = g->trial_arm;
+    }
     CK(cudaMemcpyAsync(c->hctr, c->ctr, sizeof(Counters), cudaMemcpyDeviceToHost, st));
     return 0;
 }
 
+constexpr int TRIAL_RUNS = 3;
+
+// Starts the timed trial of a freshly trained or loaded model (only when it
+// would route some items to CTA classes; otherwise it equals the degree rule).
+void start_trial(csaw_graph_s *g) {
+    g->mlp_lost = false;
+    g->trial = g->trained && (g->class_mask & 0x3cu);
+    g->trial_arm = 1;
+    g->trial_n[0] = g->trial_n[1] = 0;
+    g->trial_ms[0] = g->trial_ms[1] = 0.0;
+}
+
+// Folds a finished trial run in; picks the next arm or ends the trial.
+void trial_account(csaw_graph_s *g, JobCtx *c) {
+    if (c->trial_arm < 0) return;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, c->t0, c->t1) == cudaSuccess && g->trial) {
+        g->trial_ms[c->trial_arm] += ms;
+        g->trial_n[c->trial_arm] += 1;
+    }
+    cudaGetLastError();
+    c->trial_arm = -1;
+    if (!g->trial) return;
+    if (g->trial_n[0] >= TRIAL_RUNS && g->trial_n[1] >= TRIAL_RUNS) {
+        g->mlp_lost = g->trial_ms[1] / g->trial_n[1] >= g->trial_ms[0] / g->trial_n[0];
+        g->trial = false;
+        ++g_alloc_epoch;   // cached graphs hold the trial's routing
+    } else {
+        g->trial_arm = g->trial_n[1] <= g->trial_n[0] ? 1 : 0;
+    }
+}
+
 // After the job's stream has been synchronised: edge count, errors, stats.
 int finish_job(csaw_graph_s *g, JobCtx *c, int64_t cap, int64_t *n_out) {
+    trial_account(g, c);
     const Counters &k = *c->hctr;
     g->last.last_edges += (int64_t)k.out_count;
     for (int i = 0; i < KK_COUNT; ++i) {
@@ -1172,7 +1230,7 @@ extern "C" int csaw_sample_batch(csaw_graph g, csaw_job *jobs, int n_jobs, void 
     reset_last(g);
     std::vector<JobCtx *> ctx((size_t)n_jobs);
     std::vector<std::array<int32_t *, 4>> dev_out((size_t)n_jobs);
-    bool graphable = g->use_graphs && !g->prof;
+    bool graphable = g->use_graphs && !g->prof && !g->trial;   // trial runs are timed one by one
     for (int i = 0; i < n_jobs && graphable; ++i) graphable = !jobs[i].host_buffers;
     if (g->graph_epoch != g_alloc_epoch) {   // workspace moved: cached graphs are stale
         for (auto &kv : g->graphs) cudaGraphExecDestroy(kv.second);
@@ -1326,7 +1384,7 @@ static int pick_classes(csaw_graph_s *g, int n) {
 
 extern "C" int csaw_sched_classes(csaw_graph g, uint32_t *mask) {
     if (!g || !mask) return fail(CSAW_ERR_INVALID, "NULL argument");
-    *mask = g->trained ? g->class_mask : 0x3fu;
+    *mask = !g->trained ? 0x3fu : (g->mlp_lost ? 0x3u : g->class_mask);
     return 0;
 }
 
@@ -1372,6 +1430,7 @@ extern "C" int csaw_sched_train(csaw_graph g, int epochs, float lr, uint64_t see
     loss /= (float)n;
     g->last_loss = loss;
     g->trained = true;
+    start_trial(g);
     g->recording = false;
     ++g_alloc_epoch;
     if (final_loss) *final_loss = loss;
@@ -1405,6 +1464,7 @@ extern "C" int csaw_sched_set_model(csaw_graph g, const float *params, const flo
     CK(cudaDeviceSynchronize());
     g->class_mask = 0x3f;   // no training records to prune by
     g->trained = true;
+    start_trial(g);
     g->recording = false;
     ++g_alloc_epoch;
     return 0;

@@ -106,6 +106,7 @@ __device__ __forceinline__ void preload_bias(const DevGraph &g, int64_t beg, int
 // shuffle and one ballot instead of a serial search.
 struct Spec4 {
     int j = 0, a = 1;   // warp uniform: current slot, draws it used in this window
+    int have = 4;       // warp uniform: candidates computed ahead per lane (4, or 1 when lazy)
     int base = 0;       // lane: draw index of c0 (a multiple of 4)
     int sel = -1;
     int c0 = -1, c1 = -1, c2 = -1, c3 = -1;
@@ -114,11 +115,25 @@ struct Spec4 {
 
 // Windows of lanes [from, N): lane `from` starts at draw from_base, later
 // lanes at draw 0, all on the current prefix.  Warp-uniform.
+// lazy: compute only the first candidate of each window; later ones are
+// computed on demand for the rejected slot (for costly searches where a
+// rejection is rare, e.g. d >= 4N).
 template <typename CandFn>
 __device__ __forceinline__ void spec_fill(Spec4 &st, int from, int N, int lane, const DrawCtx &dc, SlotRng &rng,
-                                          CandFn cand_of, int from_base) {
+                                          CandFn cand_of, int from_base, bool lazy) {
     const bool act = lane >= from && lane < N;
     const int base = lane == from ? from_base : 0;
+    if (lazy) {
+        const uint32_t x0 = act ? rng.word(dc, lane, base) : 0u;
+        const int n0 = cand_of(x0, act);
+        if (act) {
+            st.base = base;
+            st.c0 = n0;
+        }
+        st.have = 1;
+        st.a = 1;
+        return;
+    }
     uint32_t x0 = 0, x1 = 0, x2 = 0, x3 = 0;
     if (act) {
         x0 = rng.word(dc, lane, base);
@@ -134,6 +149,7 @@ __device__ __forceinline__ void spec_fill(Spec4 &st, int from, int N, int lane, 
         st.c2 = n2;
         st.c3 = n3;
     }
+    st.have = 4;
     st.a = 1;
 }
 
@@ -144,10 +160,18 @@ __device__ __forceinline__ void fill_smallest(Spec4 &st, int j, int lane) {
 }
 
 // 0: all N slots accepted; 1: slot st.j needs a phase rebuild.
-__device__ __forceinline__ int resolve4(Spec4 &st, int N, int lane) {
+template <typename CandFn>
+__device__ __forceinline__ int resolve4(Spec4 &st, int N, int lane, const DrawCtx &dc, SlotRng &rng, CandFn cand_of) {
     while (st.j < N) {
         const int j = st.j, a = st.a;
-        const int c = __shfl_sync(FULL, st.pick(a - 1), j);
+        int cj;
+        if (a - 1 < st.have) {
+            cj = st.pick(a - 1);
+        } else {   // lazy window: the rejected slot's next draw, on its lane
+            const bool me = lane == j;
+            cj = cand_of(me ? rng.word(dc, lane, st.base + a - 1) : 0u, me);
+        }
+        const int c = __shfl_sync(FULL, cj, j);
         if (!__ballot_sync(FULL, lane < j && st.sel == c)) {
             if (lane == j) st.sel = c;
             st.j = j + 1;
@@ -171,23 +195,23 @@ __device__ __forceinline__ int resolve4(Spec4 &st, int N, int lane) {
 // prefix and returns false when no positive mass is left.
 template <typename CandFn, typename RebuildFn>
 __device__ __forceinline__ int select_spec(int N, int lane, const DrawCtx &dc, bool zero, CandFn cand_of,
-                                           RebuildFn rebuild) {
+                                           RebuildFn rebuild, bool lazy = false) {
     SlotRng rng;
     Spec4 st;
-    if (!zero) spec_fill(st, 0, N, lane, dc, rng, cand_of, 0);
+    if (!zero) spec_fill(st, 0, N, lane, dc, rng, cand_of, 0, lazy);
     for (;;) {
         if (zero) {
             for (int jj = st.j; jj < N; ++jj) fill_smallest(st, jj, lane);
             break;
         }
-        if (resolve4(st, N, lane) == 0) break;
+        if (resolve4(st, N, lane, dc, rng, cand_of) == 0) break;
         const int j = st.j;
         const int next = __shfl_sync(FULL, st.base, j) + REJECT_ATTEMPTS;
         if (!rebuild(st, j)) {
             zero = true;
             continue;
         }
-        spec_fill(st, j, N, lane, dc, rng, cand_of, next);
+        spec_fill(st, j, N, lane, dc, rng, cand_of, next, lazy);
     }
     return st.sel;
 }
@@ -230,7 +254,7 @@ __device__ __forceinline__ int select_smem(const float *W, int d, int N, const D
         T = warp_canon_prefix(wfn, d, P, zb, lane);
         return T > 0.f;
     };
-    return select_spec(N, lane, dc, !(T > 0.f), cand_of, rebuild);
+    return select_spec(N, lane, dc, !(T > 0.f), cand_of, rebuild, d >= 4 * N);
 }
 
 // Selection for 32 < d <= WF from the cached canonical prefix: the row's
@@ -269,7 +293,7 @@ __device__ __forceinline__ int select_cached(const DevGraph &g, int64_t beg, int
         T = warp_canon_prefix(wfn, d, P, zb, lane);
         return T > 0.f;
     };
-    return select_spec(N, lane, dc, !(T > 0.f), cand_of, rebuild);
+    return select_spec(N, lane, dc, !(T > 0.f), cand_of, rebuild, d >= 4 * N);
 }
 
 // Unbiased selection (no prefix): index ranks over the non-excluded range.

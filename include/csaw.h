@@ -206,7 +206,12 @@ int csaw_sched_train(csaw_graph g, int epochs, float lr, uint64_t seed, float *f
 /* Classes a trained model may pick (bit c for class c).  Training keeps the
  * warp classes 0 and 1 and the CTA classes the model picks on its own
  * training records; only those CTA widths are launched (plus CTA-256 for hubs
- * above 512 edges without a cached prefix).  0x3f when untrained. */
+ * above 512 edges without a cached prefix).  0x3f when untrained.  A trained
+ * (or loaded) model that routes items to CTA classes is then on trial: the
+ * next learned biased neighbor jobs alternate between its routing and the
+ * degree rule, timed on the device, three runs each; if its mean time is not
+ * lower it is not used and the mask reads 0x3 (the degree rule).  Output is
+ * the same under either arm. */
 int csaw_sched_classes(csaw_graph g, uint32_t *mask);
 int csaw_sched_get_model(csaw_graph g, float *params, float *norm);
 int csaw_sched_set_model(csaw_graph g, const float *params, const float *norm);

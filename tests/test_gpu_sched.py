@@ -91,4 +91,9 @@ def test_learned_schedule_keeps_output_and_trains(csaw, rmat12_pareto, bias):
     assert loss < 0.5 * zero_loss
     ref_loss, _ = np_loss_grad(w, nrm.astype(np.float64), rec)
     assert abs(ref_loss - loss) < 1e-3 * max(1.0, loss)
-    run()                                  # trained: learned granularity, same edges
+    mask = G.sched_info()["class_mask"]
+    assert mask & 0x3 == 0x3                   # the warp classes are always kept
+    for _ in range(8):
+        run()                              # trained (and timed against the degree rule): same edges
+    # after the trial the model is kept, or dropped for the degree rule
+    assert G.sched_info()["class_mask"] in (mask, 0x3)
