@@ -98,6 +98,16 @@ __device__ __forceinline__ int64_t search_upper(const float *P, int64_t d, float
     return lo;
 }
 
+// search_upper for rows held in shared memory (d < 2^31): 32-bit indices.
+__device__ __forceinline__ int search_upper32(const float *P, int d, float t) {
+    int lo = 0, hi = d - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (P[mid] > t) hi = mid; else lo = mid + 1;
+    }
+    return lo;
+}
+
 // The same index for one warp-uniform target, found by the whole warp with a
 // 32-way search: each round probes the last element of 32 equal chunks of the
 // remaining range and keeps the first chunk whose probe exceeds t, so a
@@ -321,15 +331,23 @@ template <typename CandFn>
 __device__ __forceinline__ int resolve_slots(SelState &st, int N, int lane, const DrawCtx &dc,
                                              SlotRng &rng, CandFn cand_of) {
     while (st.j < N) {
-        const int j = st.j;
-        int c = __shfl_sync(FULL, st.cand, j);
-        unsigned coll = __ballot_sync(FULL, lane < j && st.sel == c);
-        if (!coll) {
-            if (lane == j) st.sel = c;
-            st.j = j + 1;
+        // Accept in one step the run of slots j, j+1, ... whose current
+        // candidates repeat no lower slot's value (lanes below j hold their
+        // selections); the sequential order would accept each in turn.
+        const int j0 = st.j;
+        const int v = lane < j0 ? st.sel : (lane < N ? st.cand : -2 - lane);
+        const unsigned same = __match_any_sync(FULL, v);
+        const bool dup = lane >= j0 && lane < N && (same & ((1u << lane) - 1u)) != 0u;
+        const unsigned db = __ballot_sync(FULL, dup);
+        const int j = db ? __ffs(db) - 1 : N;
+        if (lane >= j0 && lane < j) st.sel = v;
+        if (j == N) {
+            st.j = N;
             st.a = 1;
-            continue;
+            return 0;
         }
+        if (j > j0) st.a = 1;   // slot j rejects its first draw of this phase
+        st.j = j;
         if (__shfl_sync(FULL, st.A, j) == MAX_SLOT_DRAWS) {
             int i = 0;
             while (__ballot_sync(FULL, lane < j && st.sel == i)) ++i;

@@ -171,21 +171,34 @@ __device__ __forceinline__ int resolve4(Spec4 &st, int N, int lane, const DrawCt
             const bool me = lane == j;
             cj = cand_of(me ? rng.word(dc, lane, st.base + a - 1) : 0u, me);
         }
-        const int c = __shfl_sync(FULL, cj, j);
-        if (!__ballot_sync(FULL, lane < j && st.sel == c)) {
-            if (lane == j) st.sel = c;
-            st.j = j + 1;
+        // Accept in one step the run of slots j, j+1, ... whose current
+        // candidates repeat no lower slot's value: lanes below j hold their
+        // selections, lane j its draw a, lanes above their first draw (the
+        // sequential order would accept each of them in turn).  f is the first
+        // slot whose candidate repeats a lower one.
+        const int v = lane < j ? st.sel : (lane == j ? cj : (lane < N ? st.c0 : -2 - lane));
+        const unsigned same = __match_any_sync(FULL, v);
+        const bool dup = lane >= j && lane < N && (same & ((1u << lane) - 1u)) != 0u;
+        const unsigned db = __ballot_sync(FULL, dup);
+        const int f = db ? __ffs(db) - 1 : N;
+        if (lane >= j && lane < f) st.sel = v;
+        if (f == N) {
+            st.j = N;
+            st.a = 1;
+            return 0;
+        }
+        // slot f's current draw (draw a of slot j, or the first of a later slot) is rejected
+        const int af = f == j ? a : 1;
+        st.j = f;
+        if (__shfl_sync(FULL, st.base, f) + af == MAX_SLOT_DRAWS) {
+            fill_smallest(st, f, lane);
+            st.j = f + 1;
             st.a = 1;
             continue;
         }
-        if (__shfl_sync(FULL, st.base, j) + a == MAX_SLOT_DRAWS) {
-            fill_smallest(st, j, lane);
-            st.j = j + 1;
-            st.a = 1;
-            continue;
-        }
-        if (a == REJECT_ATTEMPTS) return 1;
-        st.a = a + 1;
+        st.a = af;
+        if (af == REJECT_ATTEMPTS) return 1;
+        st.a = af + 1;
     }
     return 0;
 }
@@ -243,7 +256,7 @@ __device__ __forceinline__ int select_smem(const float *W, int d, int N, const D
     auto wfn = [&](int64_t i) { return W[i]; };
     float T = warp_canon_prefix(wfn, d, P, nullptr, lane);
     auto cand_of = [&](uint32_t x, bool act) -> int {
-        return act ? (int)search_upper(P, d, its_target(x, T)) : -1;
+        return act ? search_upper32(P, d, its_target(x, T)) : -1;
     };
     auto rebuild = [&](const Spec4 &st, int j) -> bool {
         const int nwords = (d + 31) >> 5;
@@ -281,7 +294,7 @@ __device__ __forceinline__ int select_cached(const DevGraph &g, int64_t beg, int
     __syncwarp();
     float T = P[d - 1];
     auto cand_of = [&](uint32_t x, bool act) -> int {
-        return act ? (int)search_upper(P, d, its_target(x, T)) : -1;
+        return act ? search_upper32(P, d, its_target(x, T)) : -1;
     };
     auto rebuild = [&](const Spec4 &st, int j) -> bool {
         const int nwords = (d + 31) >> 5;
@@ -511,7 +524,7 @@ k_coop_fast(DevGraph g, LevelArgs a) {
 // the prefix cache for BIAS, so no shared copy of the raw biases is kept
 // (half the shared memory, more resident warps).
 template <typename I, int BIAS, bool CACHED>
-__global__ void __launch_bounds__(FAST_THREADS, CACHED ? 6 : 4)
+__global__ void __launch_bounds__(FAST_THREADS, 4)
 k_select_fast(DevGraph g, LevelArgs a) {
     constexpr bool BIASED = BIAS != CSAW_BIAS_UNBIASED;
     constexpr int NW = FAST_THREADS / 32;
@@ -587,7 +600,7 @@ k_select_fast(DevGraph g, LevelArgs a) {
 // loads; no shared memory.  An item whose draws need a rebuild of its prefix
 // goes to the retry list (the CTA pass rebuilds it in global scratch).
 template <typename I, int BIAS>
-__global__ void __launch_bounds__(FAST_THREADS, 6)
+__global__ void __launch_bounds__(FAST_THREADS, 4)
 k_select_hub(DevGraph g, LevelArgs a) {
     const int lane = threadIdx.x & 31;
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
