@@ -427,7 +427,7 @@ def scale25(args):
         ms = e0.elapsed_time(e1) / args.steps
         G.profile(True)
         G.sample_batch(jobs)
-        ks = {k: G.kernel_stats(k) for k in ("expand", "select", "hub", "heavy", "walk", "setup")}
+        ks = {k: G.kernel_stats(k) for k in ("expand", "select", "hub", "pair", "heavy", "walk", "setup")}
         G.profile(False)
         tot_bytes = sum(v["bytes"] for v in ks.values())
         r.update({"ms_per_step": ms, "edges_per_step": n / args.steps, "seps": n / args.steps / (ms * 1e-3),
@@ -546,7 +546,7 @@ def main():
         clk = clocks.stop() if clocks else None
         launches = G.stats()["kernel_launches"] - launches0
         ms = sum(x.elapsed_time(y) for x, y in evs)
-        ks = {k: G.kernel_stats(k) for k in ("expand", "select", "hub", "heavy", "walk", "setup")}
+        ks = {k: G.kernel_stats(k) for k in ("expand", "select", "hub", "pair", "heavy", "walk", "setup")}
         G.profile(False)
         return edges, ms, ks, launches, clk
 
@@ -623,7 +623,7 @@ def main():
 
     peak, peak_kind = load_peaks()
     kernel_names = {"expand": "k_coop_fast" if main_form != "plain" else "k_expand_warp",
-                    "select": "k_select_fast", "hub": "k_select_hub", "heavy": "k_expand_heavy",
+                    "select": "k_select_fast", "hub": "k_select_hub", "pair": "k_select_pair", "heavy": "k_expand_heavy",
                     "walk": "k_walk_fast" if main_form != "plain" else "k_walk_warp"}
     timed_kinds = [k for k in kernel_names if kstats.get(k, {}).get("launches")]
     dom = max(timed_kinds, key=lambda k: kstats[k]["ms"])

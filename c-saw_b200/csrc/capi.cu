@@ -51,7 +51,8 @@ int fail(int code, const std::string &msg) {
         if (rc_) return rc_;   \
     } while (0)
 
-enum { KK_EXPAND = 0, KK_HEAVY = 1, KK_WALK = 2, KK_MDRW = 3, KK_INIT = 4, KK_SELECT = 5, KK_HUB = 6, KK_COUNT = 8 };
+enum { KK_EXPAND = 0, KK_HEAVY = 1, KK_WALK = 2, KK_MDRW = 3, KK_INIT = 4, KK_SELECT = 5, KK_HUB = 6, KK_PAIR = 7,
+       KK_COUNT = 8 };
 
 struct Counters {
     unsigned long long out_count;
@@ -63,6 +64,8 @@ struct Counters {
     uint32_t n_cta[4];
     uint32_t n_retry;
     uint32_t n_hub;
+    uint32_t n_pair;
+    uint32_t n_refill;
     int err;
 };
 
@@ -110,7 +113,7 @@ constexpr int MDRW_MAX_F = 4096;
 // Job 0 serves csaw_sample; csaw_sample_batch runs job i on context i, each
 // on its own stream, so independent jobs overlap on the device.
 struct JobCtx {
-    DevBuf q[2][5], heavy, sel, hlist, hscratch, wscratch, seeds_in, out_dev, cta[4], retry, stab, hubsel;
+    DevBuf q[2][5], heavy, sel, hlist, hscratch, wscratch, seeds_in, out_dev, cta[4], retry, stab, hubsel, pairsel;
     Counters *ctr = nullptr, *hctr = nullptr;
     cudaStream_t stream = nullptr;   // owned (batch jobs); job 0 uses the caller's
     cudaEvent_t done = nullptr;
@@ -427,6 +430,7 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
     }
     const SchedArgs *sched = nullptr;
     const int hgrid = plain ? 0 : grid_for(k_select_hub<I, BIAS>, FAST_THREADS, 0, g->sm_count);
+    const int pgrid = plain ? 0 : grid_for(k_select_pair<I, BIAS>, FAST_THREADS, 0, g->sm_count);
     if (BIASED && ((!plain && g->maxdeg > WF) || g->cdf_flag)) TRY((ensure_cdf<I, BIAS>(g, st)));
     const bool cached = BIASED && g->cdf[BIAS] && (!plain || g->cdf_flag);
     const int sgrid = plain ? 0
@@ -438,6 +442,7 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
         if (cached && g->maxdeg > WF) {
             TRY(ensure(c->retry, sizeof(SelEntry) * qcap, st));
             TRY(ensure(c->hubsel, sizeof(SelEntry) * qcap, st));
+            TRY(ensure(c->pairsel, sizeof(SelEntry) * qcap, st));
         }
         if (p->schedule == CSAW_SCHED_LEARNED && BIASED) TRY((ensure_vstats<I, BIAS>(g, st)));
         TRY(sched_for(g, p->schedule, BIAS, sgrid * (FAST_THREADS / 32), st, &sched));
@@ -495,7 +500,7 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
         for (int l = 0; l < D; ++l) {
             const int cur = l & 1, nxt = cur ^ 1;
             CK(cudaMemsetAsync(&c->ctr->nq[nxt], 0, sizeof(uint32_t), st));
-            CK(cudaMemsetAsync(&c->ctr->n_heavy, 0, 8 * sizeof(uint32_t), st));  // n_heavy .. n_hub
+            CK(cudaMemsetAsync(&c->ctr->n_heavy, 0, 10 * sizeof(uint32_t), st));  // n_heavy .. n_refill
             LevelArgs a;
             a.in_v = (const int32_t *)c->q[cur][0].p;
             a.in_s = (const int32_t *)c->q[cur][1].p;
@@ -520,6 +525,11 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
             a.sched_tab = tabled ? (const uint8_t *)c->stab.p : nullptr;
             a.hub_list = (SelEntry *)c->hubsel.p;
             a.n_hub = &c->ctr->n_hub;
+            const bool paired = cached && g->maxdeg > WF && fan[l] <= 16;
+            a.pair_list = paired ? (SelEntry *)c->pairsel.p : nullptr;
+            a.n_pair = &c->ctr->n_pair;
+            a.refill_list = (SelEntry *)c->sel.p;   // free once k_select_fast has run
+            a.n_refill = &c->ctr->n_refill;
             a.retry_list = (SelEntry *)c->retry.p;
             a.n_retry = &c->ctr->n_retry;
             a.heavy_scratch = (float *)c->hscratch.p;
@@ -573,6 +583,17 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
             if (!plain && cached && g->maxdeg > WF) {
                 LaunchScope ls(g, KK_HUB, st);
                 k_select_hub<I, BIAS><<<hgrid, FAST_THREADS, 0, st>>>(dg, a);
+            }
+            if (a.pair_list) {
+                {
+                    LaunchScope ls(g, KK_PAIR, st);
+                    k_select_pair<I, BIAS><<<pgrid, FAST_THREADS, 0, st>>>(dg, a);
+                }
+                LevelArgs ar = a;   // paired items that need a rebuild, redone by whole warps
+                ar.sel_list = a.refill_list;
+                ar.n_sel = a.n_refill;
+                LaunchScope ls(g, KK_SELECT, st);
+                k_select_fast<I, BIAS, true><<<sgrid, FAST_THREADS, 0, st>>>(dg, ar);
             }
             if (hblocks && plain) {
                 LaunchScope ls(g, KK_HEAVY, st);
@@ -737,7 +758,7 @@ void free_job(JobCtx *c) {
     for (auto &qq : c->q)
         for (auto &b : qq) cudaFree(b.p);
     for (DevBuf *b : {&c->heavy, &c->sel, &c->hlist, &c->hscratch, &c->wscratch, &c->seeds_in, &c->out_dev, &c->cta[0],
-                      &c->cta[1], &c->cta[2], &c->cta[3], &c->retry, &c->stab, &c->hubsel})
+                      &c->cta[1], &c->cta[2], &c->cta[3], &c->retry, &c->stab, &c->hubsel, &c->pairsel})
         cudaFree(b->p);
     cudaFree(c->ctr);
     if (c->hctr) cudaFreeHost(c->hctr);
@@ -756,7 +777,7 @@ int64_t job_workspace(const JobCtx *c) {
     for (auto &qq : c->q)
         for (auto &b : qq) ws += (int64_t)b.n;
     for (const DevBuf *b : {&c->heavy, &c->sel, &c->hlist, &c->hscratch, &c->wscratch, &c->seeds_in, &c->out_dev,
-                            &c->cta[0], &c->cta[1], &c->cta[2], &c->cta[3], &c->retry, &c->stab, &c->hubsel})
+                            &c->cta[0], &c->cta[1], &c->cta[2], &c->cta[3], &c->retry, &c->stab, &c->hubsel, &c->pairsel})
         ws += (int64_t)b->n;
     return ws;
 }

@@ -438,8 +438,10 @@ k_coop_fast(DevGraph g, LevelArgs a) {
             }
         }
         const bool heavy = drawn && cls >= 2;
-        // warp-class items above WF search the cached prefix: their own list
-        const bool hub = drawn && !heavy && cached && d > WF;
+        // cached items with few slots and a rare rebuild run two per warp;
+        // other warp-class items above WF search the cached prefix in their own list
+        const bool pair = drawn && !heavy && cached && N <= 16 && d >= 4 * N && a.pair_list;
+        const bool hub = drawn && !heavy && cached && d > WF && !pair;
         const int incl = warp_incl_scan(k, lane);
         const int excl = incl - k;
         const int K = __shfl_sync(FULL, incl, 31);
@@ -454,13 +456,22 @@ k_coop_fast(DevGraph g, LevelArgs a) {
             qb = __shfl_sync(FULL, qb, 0);
         }
         // hand off items that need draws, with their reserved slots
-        const unsigned sm = __ballot_sync(FULL, drawn && !heavy && !hub);
+        const unsigned sm = __ballot_sync(FULL, drawn && !heavy && !hub && !pair);
         if (sm) {
             uint32_t pos = 0;
             if (lane == 0) pos = atomicAdd(a.n_sel, (uint32_t)__popc(sm));
             pos = __shfl_sync(FULL, pos, 0);
-            if (drawn && !heavy && !hub)
+            if (drawn && !heavy && !hub && !pair)
                 a.sel_list[pos + __popc(sm & ((1u << lane) - 1u))] =
+                    SelEntry{it, qb + (uint32_t)excl, ob + excl, v, s, p, (int32_t)d, (long long)beg, cls, 0};
+        }
+        const unsigned pbm = __ballot_sync(FULL, pair);
+        if (pbm) {
+            uint32_t pos = 0;
+            if (lane == 0) pos = atomicAdd(a.n_pair, (uint32_t)__popc(pbm));
+            pos = __shfl_sync(FULL, pos, 0);
+            if (pair)
+                a.pair_list[pos + __popc(pbm & ((1u << lane) - 1u))] =
                     SelEntry{it, qb + (uint32_t)excl, ob + excl, v, s, p, (int32_t)d, (long long)beg, cls, 0};
         }
         const unsigned hbm = __ballot_sync(FULL, hub);
@@ -591,6 +602,152 @@ k_select_fast(DevGraph g, LevelArgs a) {
     if (lane == 0 && my_items) {
         atomicAdd(&a.bytes[5], my_bytes);
         atomicAdd(&a.items[5], my_items);
+    }
+}
+
+// Half-warp primitives: a warp runs two independent items, lanes 0-15 and
+// 16-31, each with its own mask (the halves may diverge).
+struct Half {
+    unsigned mask;
+    int base, sl;   // first lane of the half, lane within the half
+    __device__ explicit Half(int lane) : mask(0xFFFFu << (lane & 16)), base(lane & 16), sl(lane & 15) {}
+    __device__ int shfl(int v, int src) const { return __shfl_sync(mask, v, base + src); }
+    __device__ unsigned ballot(bool p) const { return (__ballot_sync(mask, p) >> base) & 0xFFFFu; }
+    __device__ unsigned match(int v) const { return (__match_any_sync(mask, v) >> base) & 0xFFFFu; }
+};
+
+// Draws of one item (N <= 16 slots) in a half-warp, slot j on lane j, the
+// same draws and acceptance order as resolve_slots; cand_of(x) is a per-lane
+// search.  Returns false when a slot exhausts its draws of the first phase
+// (the item then needs a rebuild of its prefix: the caller retries it whole
+// on the CTA path).  T <= 0: the slots take indices 0..N-1.
+template <typename CandFn>
+__device__ __forceinline__ bool half_select(const Half &h, int N, const DrawCtx &dc, float T, CandFn cand_of,
+                                            int &sel) {
+    const int sl = h.sl;
+    sel = sl;
+    if (!(T > 0.f)) return true;
+    SlotRng rng;
+    int cand = -1, A = 0;
+    if (sl < N) {
+        cand = cand_of(rng.word(dc, sl, 0));
+        A = 1;
+    }
+    int j = 0, a = 1;
+    while (j < N) {
+        const int v = sl < j ? sel : (sl < N ? cand : -2 - sl);
+        const unsigned same = h.match(v);
+        const bool dup = sl >= j && sl < N && (same & ((1u << sl) - 1u)) != 0u;
+        const unsigned db = h.ballot(dup);
+        const int f = db ? __ffs(db) - 1 : N;
+        if (sl >= j && sl < f) sel = v;
+        if (f == N) break;
+        if (f > j) a = 1;
+        j = f;
+        if (h.shfl(A, j) == MAX_SLOT_DRAWS) {   // termination guard: smallest unselected index
+            int i = 0;
+            while (h.ballot(sl < j && sel == i)) ++i;
+            if (sl == j) sel = i;
+            ++j;
+            a = 1;
+            continue;
+        }
+        if (a == REJECT_ATTEMPTS) return false;
+        if (sl == j) {
+            cand = cand_of(rng.word(dc, sl, A));
+            ++A;
+        }
+        ++a;
+    }
+    return true;
+}
+
+// Level expansion, part 2 for items over a cached prefix with N <= 16 and
+// d >= 4N (a rebuild is rare): two items per warp, one per half-warp, lanes
+// N..15 of a half idle instead of N..31 of a warp.  Rows up to WF edges are
+// staged in shared memory and searched there; larger rows are searched in
+// global memory through the prefix index.  Items that need a rebuild are
+// redone from scratch: rows up to WF by k_select_fast on the refill list
+// (written over the consumed warp list), larger ones by the CTA pass.
+template <typename I, int BIAS>
+__global__ void __launch_bounds__(FAST_THREADS, 4)
+k_select_pair(DevGraph g, LevelArgs a) {
+    constexpr int NH = FAST_THREADS / 16;
+    __shared__ float s_P[NH * WF];
+    const int lane = threadIdx.x & 31;
+    const Half h(lane);
+    float *P = s_P + (threadIdx.x >> 4) * WF;
+    const uint32_t gh = (blockIdx.x * blockDim.x + threadIdx.x) >> 4;
+    const uint32_t nh = (gridDim.x * blockDim.x) >> 4;
+    const uint32_t n = *a.n_pair;
+    const uint32_t n_level = *a.n_in;
+    const int N = a.N;
+    const int nout = 2 + (a.o_smp != nullptr) + (a.o_dep != nullptr);
+    unsigned long long my_bytes = 0, my_items = 0;
+    for (uint32_t i = gh; i < n; i += nh) {
+        const SelEntry en = a.pair_list[i];
+        const int64_t beg = en.beg, d = en.d;
+        const DrawCtx dc{a.k0, a.k1, en.p, (uint32_t)en.s, (uint32_t)a.depth};
+        const bool rec = a.sched && a.sched->mode == SCHED_RECORD;
+        long long t0 = 0;
+        if (rec) t0 = clock64();
+        int sel;
+        bool ok;
+        if (d <= WF) {
+            const float *cp = g.cdf + beg;
+            const int dd = (int)d;
+            for (int i0 = 0; i0 < dd; i0 += 128) {
+                float r[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int k = i0 + u * 16 + h.sl;
+                    r[u] = k < dd ? __ldg(cp + k) : 0.f;
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int k = i0 + u * 16 + h.sl;
+                    if (k < dd) P[k] = r[u];
+                }
+            }
+            __syncwarp(h.mask);
+            const float T = P[dd - 1];
+            ok = half_select(h, N, dc, T, [&](uint32_t x) { return search_upper32(P, dd, its_target(x, T)); }, sel);
+            __syncwarp(h.mask);
+        } else {
+            const float T = __ldg(g.cdf + beg + d - 1);
+            ok = half_select(h, N, dc, T, [&](uint32_t x) { return (int)cdf_search(g, beg, d, its_target(x, T)); },
+                             sel);
+        }
+        if (!ok) {   // rebuild needed: a whole warp redoes the item (in shared memory up to WF)
+            if (h.sl == 0) {
+                if (d <= WF) a.refill_list[atomicAdd(a.n_refill, 1u)] = en;
+                else a.retry_list[atomicAdd(a.n_retry, 1u)] = en;
+            }
+            continue;
+        }
+        if (h.sl < N)
+            emit_edge<I>(g, a, beg + sel, en.v, en.s, en.p * (uint32_t)N + (uint32_t)h.sl, (int64_t)en.ob + h.sl,
+                         en.q + (uint32_t)h.sl);
+        if (rec) {
+            __syncwarp(h.mask);
+            if (h.sl == 0)
+                record_profile(a.sched, d, N, a.sched->vstats[en.v], n_level, a.depth, en.cls, clock64() - t0);
+        }
+        if (h.sl == 0) {
+            my_items++;
+            const unsigned long long row = d <= WF ? 4ull * d : (unsigned long long)N * 4ull * (64 - __clzll(d));
+            my_bytes += 16 + row + (unsigned long long)N * (4ull + 4ull * nout + (a.push ? 12ull + 2 * (sizeof(I) + 4)
+                                                                                          : 0ull));
+        }
+    }
+#pragma unroll
+    for (int off = 16; off; off >>= 1) {
+        my_bytes += __shfl_xor_sync(FULL, my_bytes, off);
+        my_items += __shfl_xor_sync(FULL, my_items, off);
+    }
+    if (lane == 0 && my_items) {
+        atomicAdd(&a.bytes[7], my_bytes);
+        atomicAdd(&a.items[7], my_items);
     }
 }
 

@@ -122,7 +122,8 @@ int csaw_graph_stats(csaw_graph g, csaw_stats *out);
  * bytes and work items since profiling was (re)enabled.
  * Kinds: 0 level expansion (batched: take-all pass), 1 high-degree (CTA)
  * expansion, 2 walk, 3 MDRW, 4 queue/seed/residency setup, 5 batched
- * warp-granularity selection pass, 6 batched hub selection (cached prefix).
+ * warp-granularity selection pass, 6 batched hub selection (cached prefix),
+ * 7 batched two-items-per-warp selection (cached prefix, N <= 16).
  */
 int csaw_graph_profile(csaw_graph g, int enable);
 int csaw_graph_kernel_stats(csaw_graph g, int kind, double *ms, int64_t *launches,
