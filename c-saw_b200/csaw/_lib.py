@@ -14,6 +14,7 @@ MODE_NEIGHBOR, MODE_WALK, MODE_MDRW = 0, 1, 2
 BIAS_UNBIASED, BIAS_DEGREE, BIAS_EDGE_WEIGHT, BIAS_HOOK = 0, 1, 2, 3
 SCHED_PLAIN, SCHED_BATCHED, SCHED_LEARNED = 0, 1, 2
 GRAPH_DEGREE_BIAS, GRAPH_CDF_CACHE, GRAPH_NO_CDF_CACHE = 1, 2, 4
+PARAM_DEDUP = 1
 MAX_DEPTH = 64
 KERNEL_KINDS = {"expand": 0, "heavy": 1, "walk": 2, "mdrw": 3, "setup": 4, "select": 5, "hub": 6, "pair": 7}
 
@@ -50,6 +51,8 @@ class Params(ctypes.Structure):
         ("fanout", ctypes.c_int32 * MAX_DEPTH),
         ("seed", ctypes.c_uint64),
         ("sample_base", ctypes.c_int64),
+        ("flags", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 

@@ -22,7 +22,7 @@ MODE_NAMES = {"neighbor": MODE_NEIGHBOR, "walk": MODE_WALK, "mdrw": MODE_MDRW}
 
 
 def make_params(mode, bias, n_samples, frontier_size=1, neighbor_size=1, depth=1, fanout=None, seed=0,
-                schedule=SCHED_PLAIN, sample_base=0):
+                schedule=SCHED_PLAIN, sample_base=0, dedup=False):
     p = _lib.Params()
     p.mode = MODE_NAMES.get(mode, mode)
     p.bias = BIAS_NAMES.get(bias, bias)
@@ -35,6 +35,7 @@ def make_params(mode, bias, n_samples, frontier_size=1, neighbor_size=1, depth=1
         p.fanout[i] = n
     p.seed = seed
     p.sample_base = sample_base
+    p.flags = _lib.PARAM_DEDUP if dedup else 0
     return p
 
 

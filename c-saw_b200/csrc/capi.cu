@@ -113,7 +113,7 @@ constexpr int MDRW_MAX_F = 4096;
 // Job 0 serves csaw_sample; csaw_sample_batch runs job i on context i, each
 // on its own stream, so independent jobs overlap on the device.
 struct JobCtx {
-    DevBuf q[2][5], heavy, sel, hlist, hscratch, wscratch, seeds_in, out_dev, cta[4], retry, stab, hubsel, pairsel;
+    DevBuf q[2][5], heavy, sel, hlist, hscratch, wscratch, seeds_in, out_dev, cta[4], retry, stab, hubsel, pairsel, dedup;
     Counters *ctr = nullptr, *hctr = nullptr;
     cudaStream_t stream = nullptr;   // owned (batch jobs); job 0 uses the caller's
     cudaEvent_t done = nullptr;
@@ -391,6 +391,9 @@ int check_params(const csaw_graph_s *g, const csaw_params *p, int fan[CSAW_MAX_D
         return fail(CSAW_ERR_INVALID, "MDRW picks frontier vertices: use a vertex bias");
     if (p->mode == CSAW_MODE_MDRW && p->frontier_size > MDRW_MAX_F)
         return fail(CSAW_ERR_INVALID, "MDRW frontier_size above 4096");
+    if (p->flags & ~(int32_t)CSAW_PARAM_DEDUP) return fail(CSAW_ERR_INVALID, "unknown params flags");
+    if ((p->flags & CSAW_PARAM_DEDUP) && p->mode != CSAW_MODE_NEIGHBOR)
+        return fail(CSAW_ERR_INVALID, "dedup applies to neighbor sampling only");
     if (p->mode == CSAW_MODE_NEIGHBOR) {
         for (int l = 0; l < p->depth; ++l) {
             fan[l] = p->fanout[l] ? p->fanout[l] : p->neighbor_size;
@@ -421,6 +424,37 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
     if (B < 1) B = 1;
     const int64_t qcap = (int64_t)(B * per_sample) + 32;
     const bool plain = p->schedule == CSAW_SCHED_PLAIN;
+    // per-sample dedup: a (sample, vertex) table for every item one chunk can
+    // queue (all levels that push), at most half full
+    const bool dedup = (p->flags & CSAW_PARAM_DEDUP) != 0 && D > 1;
+    uint64_t dmask = 0;
+    if (dedup) {
+        double items = F, l2 = F;
+        for (int l = 0; l + 1 < D; ++l) {
+            l2 *= fan[l];
+            items += l2;
+        }
+        const double want = 2.0 * items * (double)B;
+        uint64_t slots = 1024;
+        while ((double)slots < want) slots <<= 1;
+        dmask = slots - 1;
+        TRY(ensure(c->dedup, 16 * (size_t)slots, st));
+    }
+    unsigned long long *dkeys = dedup ? (unsigned long long *)c->dedup.p : nullptr;
+    unsigned long long *dvals = dedup ? dkeys + dmask + 1 : nullptr;
+    const int dgrid = g->sm_count * 8;
+    auto dedup_level = [&](int q, int level) -> int {
+        int32_t *qdeg = plain ? nullptr : (int32_t *)c->q[q][4].p;
+        LaunchScope ls(g, KK_INIT, st);
+        k_dedup_insert<<<dgrid, 256, 0, st>>>((const int32_t *)c->q[q][0].p, (const int32_t *)c->q[q][1].p,
+                                              (const uint32_t *)c->q[q][2].p, &c->ctr->nq[q], level, dkeys, dvals,
+                                              dmask, &c->ctr->err);
+        k_dedup_filter<<<dgrid, 256, 0, st>>>((int32_t *)c->q[q][0].p, (const int32_t *)c->q[q][1].p,
+                                              (const uint32_t *)c->q[q][2].p, qdeg, &c->ctr->nq[q], level, dkeys,
+                                              dvals, dmask);
+        g->launches += 1;   // the second of the pair
+        return 0;
+    };
     for (int k = 0; k < 2; ++k) {
         for (int a = 0; a < 3; ++a) TRY(ensure(c->q[k][a], sizeof(int32_t) * qcap, st));
         if (!plain) {
@@ -496,6 +530,10 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
                     dg, seeds + s0 * F, n0, F, (int)(p->sample_base + s0), (int32_t *)c->q[0][0].p, (int32_t *)c->q[0][1].p,
                     (uint32_t *)c->q[0][2].p, (I *)c->q[0][3].p, (int32_t *)c->q[0][4].p, &c->ctr->nq[0],
                     &c->ctr->err);
+        }
+        if (dedup) {
+            CK(cudaMemsetAsync(dkeys, 0xff, 16 * (size_t)(dmask + 1), st));
+            TRY(dedup_level(0, 0));
         }
         for (int l = 0; l < D; ++l) {
             const int cur = l & 1, nxt = cur ^ 1;
@@ -609,6 +647,7 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
                 k_expand_heavy<I, BIAS><<<cta_grid[1], 256, 0, st>>>(dg, ar);
             }
             if (side) CK(cudaStreamWaitEvent(st, c->join, 0));
+            if (dedup && l + 1 < D) TRY(dedup_level(nxt, l + 1));
         }
     }
     CK(cudaGetLastError());
@@ -758,7 +797,7 @@ void free_job(JobCtx *c) {
     for (auto &qq : c->q)
         for (auto &b : qq) cudaFree(b.p);
     for (DevBuf *b : {&c->heavy, &c->sel, &c->hlist, &c->hscratch, &c->wscratch, &c->seeds_in, &c->out_dev, &c->cta[0],
-                      &c->cta[1], &c->cta[2], &c->cta[3], &c->retry, &c->stab, &c->hubsel, &c->pairsel})
+                      &c->cta[1], &c->cta[2], &c->cta[3], &c->retry, &c->stab, &c->hubsel, &c->pairsel, &c->dedup})
         cudaFree(b->p);
     cudaFree(c->ctr);
     if (c->hctr) cudaFreeHost(c->hctr);
@@ -777,7 +816,7 @@ int64_t job_workspace(const JobCtx *c) {
     for (auto &qq : c->q)
         for (auto &b : qq) ws += (int64_t)b.n;
     for (const DevBuf *b : {&c->heavy, &c->sel, &c->hlist, &c->hscratch, &c->wscratch, &c->seeds_in, &c->out_dev,
-                            &c->cta[0], &c->cta[1], &c->cta[2], &c->cta[3], &c->retry, &c->stab, &c->hubsel, &c->pairsel})
+                            &c->cta[0], &c->cta[1], &c->cta[2], &c->cta[3], &c->retry, &c->stab, &c->hubsel, &c->pairsel, &c->dedup})
         ws += (int64_t)b->n;
     return ws;
 }

@@ -146,6 +146,7 @@ k_expand_warp(DevGraph g, LevelArgs a) {
     unsigned long long my_bytes = 0, my_items = 0;
     for (uint32_t it = gw; it < n; it += nw) {
         const int32_t v = a.in_v[it];
+        if (v < 0) continue;   // dropped by per-sample dedup
         const int32_t s = a.in_s[it];
         const uint32_t p = a.in_p[it];
         const int64_t beg = row_begin<I>(g, v);
@@ -574,6 +575,80 @@ __global__ void k_cdf_build_big(DevGraph g, float *cdf, const int32_t *verts, in
         float *gcar = tsum + (d >> 5) + 1;
         auto wfn = [&](int64_t i) { return edge_bias<I, BIAS>(g, beg + i); };
         cta_canon_prefix(wfn, d, cdf + beg, tsum, gcar, nullptr);
+    }
+}
+
+// ------------------------------------------------------- per-sample dedup
+// Hash set of (sample, vertex) keys with, per key, the smallest packed
+// (level << 32 | lineage) of the items that carried it.  Open addressing,
+// linear probing; the table holds at most half its slots.  A queue item is
+// kept iff its packed value is the key's minimum, i.e. the vertex is new to
+// its sample at this level and this item has the lowest lineage among the
+// level's items that carry it.
+constexpr unsigned long long DEDUP_EMPTY = ~0ull;
+
+__device__ __forceinline__ unsigned long long dedup_key(int32_t s, int32_t v) {
+    return ((unsigned long long)(uint32_t)s << 32) | (uint32_t)v;
+}
+
+__device__ __forceinline__ uint64_t dedup_slot(unsigned long long key, uint64_t mask) {
+    unsigned long long h = key * 0x9E3779B97F4A7C15ull;
+    h ^= h >> 29;
+    return h & mask;
+}
+
+// Pass 1 over a level's queue (count *n): insert every item's key and fold
+// its packed value in with atomicMin.
+static __global__ void k_dedup_insert(const int32_t *qv, const int32_t *qs, const uint32_t *qp, const uint32_t *n,
+                                      int level, unsigned long long *keys, unsigned long long *vals, uint64_t mask,
+                                      int *err) {
+    const uint32_t cnt = *n;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        const int32_t v = qv[i];
+        if (v < 0) continue;
+        const unsigned long long key = dedup_key(qs[i], v);
+        const unsigned long long val = ((unsigned long long)(uint32_t)level << 32) | qp[i];
+        uint64_t h = dedup_slot(key, mask);
+        bool done = false;
+        for (uint64_t probe = 0; probe <= mask; ++probe) {
+            const unsigned long long prev = atomicCAS(keys + h, DEDUP_EMPTY, key);
+            if (prev == DEDUP_EMPTY || prev == key) {
+                atomicMin(vals + h, val);
+                done = true;
+                break;
+            }
+            h = (h + 1) & mask;
+        }
+        if (!done) atomicOr(err, ERR_SCRATCH);
+    }
+}
+
+// Pass 2: items that are not their key's minimum become empty (vertex -1,
+// degree 0): the next level skips them; their edges were already emitted.
+static __global__ void k_dedup_filter(int32_t *qv, const int32_t *qs, const uint32_t *qp, int32_t *qdeg,
+                                      const uint32_t *n, int level, const unsigned long long *keys,
+                                      const unsigned long long *vals, uint64_t mask) {
+    const uint32_t cnt = *n;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        const int32_t v = qv[i];
+        if (v < 0) continue;
+        const unsigned long long key = dedup_key(qs[i], v);
+        const unsigned long long val = ((unsigned long long)(uint32_t)level << 32) | qp[i];
+        uint64_t h = dedup_slot(key, mask);
+        bool keep = false;
+        for (uint64_t probe = 0; probe <= mask; ++probe) {
+            const unsigned long long k = keys[h];
+            if (k == key) {
+                keep = vals[h] == val;
+                break;
+            }
+            if (k == DEDUP_EMPTY) break;
+            h = (h + 1) & mask;
+        }
+        if (!keep) {
+            qv[i] = -1;
+            if (qdeg) qdeg[i] = 0;
+        }
     }
 }
 

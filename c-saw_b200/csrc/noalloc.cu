@@ -159,6 +159,7 @@ extern "C" int csaw_sample_noalloc(csaw_graph g, const csaw_params *p, const int
     if (rc) return rc;
     if (p->mode != CSAW_MODE_NEIGHBOR)
         return csaw_host_fail(CSAW_ERR_INVALID, "csaw_sample_noalloc runs neighbor sampling only");
+    if (p->flags) return csaw_host_fail(CSAW_ERR_INVALID, "csaw_sample_noalloc does not take params flags (dedup)");
     if (p->bias != CSAW_BIAS_UNBIASED && maxdeg > WBUF)
         return csaw_host_fail(CSAW_ERR_INVALID,
                               "csaw_sample_noalloc: biased sampling needs max degree <= 1024 (no high-degree scratch)");

@@ -356,6 +356,7 @@ int check_stream_params(const csaw_params *p, int fan[CSAW_MAX_DEPTH]) {
     if (p->mode != CSAW_MODE_NEIGHBOR && p->mode != CSAW_MODE_WALK)
         return csaw_host_fail(CSAW_ERR_INVALID, "unknown mode");
     if (p->bias < CSAW_BIAS_UNBIASED || p->bias > CSAW_BIAS_HOOK) return csaw_host_fail(CSAW_ERR_INVALID, "unknown bias");
+    if (p->flags) return csaw_host_fail(CSAW_ERR_INVALID, "params flags (dedup) are not supported by the streaming graph");
     if (p->n_samples < 0 || p->frontier_size < 1 || p->depth < 0 || p->depth > CSAW_MAX_DEPTH)
         return csaw_host_fail(CSAW_ERR_INVALID, "bad n_samples / frontier_size / depth (streaming depth <= 64)");
     if (p->sample_base < 0 || p->sample_base + p->n_samples > INT32_MAX)

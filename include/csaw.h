@@ -71,7 +71,23 @@ typedef struct {
     int64_t sample_base;    /* id of the first sample (keys and output ids are
                                sample_base + i), so shards of one job run on
                                several GPUs give exactly the single-GPU output */
+    int32_t flags;          /* CSAW_PARAM_* (0: none) */
+    int32_t reserved;
 } csaw_params;
+
+/* csaw_params.flags */
+enum {
+    /* Per-sample vertex dedup (neighbor mode; the reference's Ht hash,
+     * functions.cuh:929-953, disabled there at :979-981): a vertex is
+     * expanded at most once per sample.  Seeds and the children of each
+     * level are taken in lineage order; one whose vertex was already taken
+     * (a seed, an earlier level's child, or a lower-lineage child of the same
+     * level) is not expanded.  Every selected edge is still emitted, so
+     * sampled subgraphs keep their edges but each vertex's neighborhood is
+     * drawn once (layer-sampling / induced-subgraph style).  Not available in
+     * csaw_sample_noalloc or the streaming graph. */
+    CSAW_PARAM_DEDUP = 1
+};
 
 typedef struct csaw_graph_s *csaw_graph;
 

@@ -312,6 +312,46 @@ typedef struct {
     int status;
 } job_t;
 
+/* Set of vertex ids (open addressing, linear probing, grows at 1/2 load). */
+typedef struct {
+    int32_t *slot;
+    int64_t cap, n;
+} vset_t;
+
+static int vset_insert(vset_t *h, int32_t v) {   /* 1 if newly inserted */
+    if (2 * (h->n + 1) > h->cap) {
+        int64_t oc = h->cap, nc = oc ? 2 * oc : 64;
+        int32_t *old = h->slot;
+        h->slot = (int32_t *)malloc(sizeof(int32_t) * (size_t)nc);
+        for (int64_t i = 0; i < nc; ++i) h->slot[i] = -1;
+        h->cap = nc;
+        h->n = 0;
+        for (int64_t i = 0; i < oc; ++i)
+            if (old[i] >= 0) vset_insert(h, old[i]);
+        free(old);
+    }
+    uint64_t i = ((uint64_t)(uint32_t)v * 0x9E3779B97F4A7C15ull) & (uint64_t)(h->cap - 1);
+    while (h->slot[i] >= 0) {
+        if (h->slot[i] == v) return 0;
+        i = (i + 1) & (uint64_t)(h->cap - 1);
+    }
+    h->slot[i] = v;
+    h->n++;
+    return 1;
+}
+
+/* Keeps the items of (v, p) whose vertex is new to the set, in order. */
+static int64_t dedup_items(vset_t *h, int32_t *v, uint32_t *p, int64_t n) {
+    int64_t k = 0;
+    for (int64_t i = 0; i < n; ++i)
+        if (vset_insert(h, v[i])) {
+            v[k] = v[i];
+            p[k] = p[i];
+            ++k;
+        }
+    return k;
+}
+
 static void run_neighbor(job_t *jb, int sl) {
     const oracle_params *p = jb->p;
     const int s = (int)(p->sample_base + sl);
@@ -329,6 +369,9 @@ static void run_neighbor(job_t *jb, int sl) {
         cp[n] = (uint32_t)f;
         ++n;
     }
+    const int dedup = (p->flags & ORACLE_DEDUP) != 0;
+    vset_t seen = {NULL, 0, 0};
+    if (dedup) n = dedup_items(&seen, cv, cp, n);
     int64_t sel[1024];
     for (int l = 0; l < p->depth; ++l) {
         int N = p->fanout[l];
@@ -357,9 +400,11 @@ static void run_neighbor(job_t *jb, int sl) {
             }
         }
         free(cv); free(cp);
+        if (dedup) nn = dedup_items(&seen, nv, np, nn);
         cv = nv; cp = np; n = nn; cap = ncap;
     }
     free(cv); free(cp);
+    free(seen.slot);
 }
 
 static void run_walk(job_t *jb, int sl) {

@@ -48,7 +48,15 @@ typedef struct {
     int32_t fanout[ORACLE_MAX_DEPTH]; /* N per hop (neighbor mode) */
     uint64_t seed;          /* Philox key */
     int64_t sample_base;    /* id of the first sample (keys and output ids) */
+    int32_t flags;          /* ORACLE_DEDUP: per-sample vertex dedup */
 } oracle_params;
+
+/* Per-sample vertex dedup (neighbor mode): a vertex is expanded at most once
+ * per sample.  Seeds and pushed children are taken in lineage order; one whose
+ * vertex was already taken (an earlier seed, an earlier level's child, or a
+ * lower-lineage child of the same level) is not expanded.  Every selected
+ * edge is still emitted. */
+#define ORACLE_DEDUP 1
 
 /* Philox4x32-10 (Salmon et al., SC11). */
 void oracle_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);

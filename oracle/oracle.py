@@ -29,7 +29,11 @@ class _Params(ctypes.Structure):
         ("fanout", ctypes.c_int32 * MAX_DEPTH),
         ("seed", ctypes.c_uint64),
         ("sample_base", ctypes.c_int64),
+        ("flags", ctypes.c_int32),
     ]
+
+
+DEDUP = 1
 
 
 def build():
@@ -86,7 +90,7 @@ def make_seeds(rowptr, n, seed):
 
 
 def run(rowptr, col, weight, seeds, mode, bias, n_samples, frontier_size, depth, fanout=None,
-        seed=0, n_threads=1, cap=None, sample_base=0):
+        seed=0, n_threads=1, cap=None, sample_base=0, flags=0):
     """Returns (src, dst, sample, depth) int32 arrays in oracle order."""
     rp = np.ascontiguousarray(rowptr, dtype=np.int64)
     cl = np.ascontiguousarray(col, dtype=np.int32)
@@ -96,6 +100,7 @@ def run(rowptr, col, weight, seeds, mode, bias, n_samples, frontier_size, depth,
     P.mode, P.bias, P.n_samples = mode, bias, n_samples
     P.frontier_size, P.depth, P.seed = frontier_size, depth, seed
     P.sample_base = sample_base
+    P.flags = flags
     fo = list(fanout or [])
     for i in range(min(depth, MAX_DEPTH)):
         P.fanout[i] = fo[i] if i < len(fo) else (fo[-1] if fo else 1)

@@ -137,7 +137,7 @@ def select(wfun, d, N, seed, s, l, p, biased):
     return S
 
 
-def run(csr, seeds, mode, bias, n_samples, F, depth, fanout, seed):
+def run(csr, seeds, mode, bias, n_samples, F, depth, fanout, seed, dedup=False):
     rp, col, w = csr.rowptr, csr.col, csr.weight
     out = []
 
@@ -150,6 +150,18 @@ def run(csr, seeds, mode, bias, n_samples, F, depth, fanout, seed):
     for s in range(n_samples):
         if mode == 0:
             cur = [(int(seeds[s * F + f]), f) for f in range(F)]
+            seen = set()
+
+            def fresh(items):   # per-sample dedup: first occurrence in lineage order
+                keep = []
+                for v, p in items:
+                    if v not in seen:
+                        seen.add(v)
+                        keep.append((v, p))
+                return keep
+
+            if dedup:
+                cur = fresh(cur)
             for l in range(depth):
                 N = fanout[l]
                 nxt = []
@@ -161,8 +173,9 @@ def run(csr, seeds, mode, bias, n_samples, F, depth, fanout, seed):
                     for j, idx in enumerate(sel):
                         u = int(col[beg + idx])
                         out.append((v, u, s, l))
-                        nxt.append((u, (p * N + j) & MASK))
-                cur = nxt
+                        if l + 1 < depth:
+                            nxt.append((u, (p * N + j) & MASK))
+                cur = fresh(nxt) if dedup else nxt
         elif mode == 1:
             v = int(seeds[s])
             for t in range(depth):

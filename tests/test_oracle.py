@@ -200,3 +200,29 @@ def test_golden_edge_lists():
     for name in GCASES:
         got = build_case(name)
         assert np.array_equal(got, data[name]), name
+
+
+@pytest.mark.parametrize("bias", [0, 1, 2])
+@pytest.mark.parametrize("F,fan", [(1, [6, 5, 4]), (3, [3, 3, 3, 3]), (2, [8, 8])])
+def test_dedup_matches_python_restatement(bias, F, fan):
+    """Per-sample vertex dedup: the oracle equals the Python restatement, on a
+    small dense graph where repeats are frequent (and seeds repeat too)."""
+    g = _graph_small(41 + bias)
+    nz = np.flatnonzero(np.diff(g.rowptr) > 0)
+    rng = np.random.default_rng(8)
+    n = 40
+    seeds = rng.choice(nz[:12], n * F).astype(np.int32)   # few distinct seeds: repeats within a sample
+    a = oracle.run(g.rowptr, g.col, g.weight, seeds, 0, bias, n, F, len(fan), fan, seed=77, flags=oracle.DEDUP)
+    b = pyspec.run(g, seeds, 0, bias, n, F, len(fan), fan, 77, dedup=True)
+    assert np.array_equal(sort_edges(*a), sort_edges(*b))
+    full = oracle.run(g.rowptr, g.col, g.weight, seeds, 0, bias, n, F, len(fan), fan, seed=77)
+    assert 0 < len(a[0]) <= len(full[0])
+    if F > 1:
+        assert len(a[0]) < len(full[0])             # repeated seeds are expanded once
+    # depth-0 edges only lose repeated seeds; each sample expands a vertex at most once per level set
+    for s in range(n):
+        m = (a[2] == s)
+        src_levels = {}
+        for u, l in zip(a[0][m], a[3][m]):
+            src_levels.setdefault(int(u), set()).add(int(l))
+        assert all(len(ls) == 1 for ls in src_levels.values())
