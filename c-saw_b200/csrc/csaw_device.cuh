@@ -250,12 +250,21 @@ __device__ float cta_canon_prefix(WFn wfn, int64_t d, float *P, float *tsum, flo
         if (lane == 31) gcar[gg] = q;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (warp == 0) {
+        // serial carry across groups, in group order (C += total of group g):
+        // the warp loads 32 group totals at a time and folds them by shuffles,
+        // every lane carrying the same C; lane k keeps the carry into group g0+k
         float C = 0.f;
-        for (int64_t gg = 0; gg < ngroups; ++gg) {
-            float tot = gcar[gg];
-            gcar[gg] = C;
-            C = __fadd_rn(C, tot);
+        for (int64_t g0 = 0; g0 < ngroups; g0 += 32) {
+            const int64_t gg = g0 + lane;
+            const float tot = gg < ngroups ? gcar[gg] : 0.f;
+            const int m = ngroups - g0 < 32 ? (int)(ngroups - g0) : 32;
+            float mine = 0.f;
+            for (int k = 0; k < m; ++k) {
+                if (lane == k) mine = C;
+                C = __fadd_rn(C, __shfl_sync(FULL, tot, k));
+            }
+            if (gg < ngroups) gcar[gg] = mine;
         }
     }
     __syncthreads();
@@ -270,17 +279,30 @@ __device__ float cta_canon_prefix(WFn wfn, int64_t d, float *P, float *tsum, flo
         if (lane == 31) tsum[t] = p;
     }
     __syncthreads();
-    if (warp == 0) {
+    {
+        // exclusive running max of the tile maxima.  max is exact, so the
+        // warps scan contiguous ranges in parallel: range maxima first, then
+        // each range from the max of the ranges before it.
+        __shared__ float s_rmax[32];
+        const int64_t per = (ntiles + nw - 1) / nw;
+        const int64_t t0 = (int64_t)warp * per, t1 = t0 + per < ntiles ? t0 + per : ntiles;
+        float rmax = 0.f;
+        for (int64_t t = t0 + lane; t < t1; t += 32) rmax = fmaxf(rmax, tsum[t]);
+#pragma unroll
+        for (int off = 16; off; off >>= 1) rmax = fmaxf(rmax, __shfl_xor_sync(FULL, rmax, off));
+        if (lane == 0) s_rmax[warp] = rmax;
+        __syncthreads();
         float carry = 0.f;
-        for (int64_t base = 0; base < ntiles; base += 32) {
-            int64_t t = base + lane;
-            float m = t < ntiles ? tsum[t] : 0.f;
-            float ms = warp_max_scan(m, lane);
+        for (int w = 0; w < warp; ++w) carry = fmaxf(carry, s_rmax[w]);
+        for (int64_t base = t0; base < t1; base += 32) {
+            const int64_t t = base + lane;
+            const float m = t < t1 ? tsum[t] : 0.f;
+            const float ms = warp_max_scan(m, lane);
             float ex = __shfl_up_sync(FULL, ms, 1);
             if (lane == 0) ex = 0.f;
             ex = fmaxf(ex, carry);
             __syncwarp();
-            if (t < ntiles) tsum[t] = ex;
+            if (t < t1) tsum[t] = ex;
             carry = fmaxf(carry, __shfl_sync(FULL, ms, 31));
         }
     }
