@@ -445,6 +445,70 @@ def scale25(args):
     return res
 
 
+STREAM_GRAPH = dict(scale=26, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=29, symmetrize=False, weight="uniform")
+
+
+def streaming(args):
+    """Streaming (out-of-budget) workload at 1/8 of the scale-29 configuration:
+    R-MAT scale 26, edge factor 16, directed, U(0,1] weights (generated on the
+    GPU), adjacency in page-locked host memory with the device partition
+    budget capped at 4 GiB (under half of the 8.5 GB adjacency) and 2^17-vertex
+    partitions (512, as many as the scale-29 configuration has); one step = 131,072 edge-weight-biased walks of length 20 and
+    32,768 edge-weight-biased samples F1 N10 D2.  The same jobs on the
+    in-memory graph give the reference time and check the edge counts."""
+    import torch
+    import csaw
+    from csaw import graphgen
+    torch.cuda.set_device(0)
+    g = graphgen.rmat_device(**STREAM_GRAPH)
+    torch.cuda.empty_cache()
+    budget = 4 << 30
+    res = {"graph": {"workload": "rmat26_ef16_uniform", "n_vertices": g.n_vertices, "n_edges": g.n_edges,
+                     "host_adjacency_bytes": int(g.col.nbytes + g.weight.nbytes + g.rowptr.nbytes)},
+           "partition_bits": 17, "device_budget": budget,
+           "walks": dict(n=1 << 17, length=20), "samples": dict(n=1 << 15, F=1, N=10, D=2)}
+    pw = csaw.make_params(1, 2, 1 << 17, 1, 1, 20, seed=0x29A)
+    ps = csaw.make_params(0, 2, 1 << 15, 1, 10, 2, seed=0x29B)
+    # the in-memory reference also runs the batched schedule (cache, records)
+    pwb = csaw.make_params(1, 2, 1 << 17, 1, 1, 20, seed=0x29A, schedule=csaw.SCHED_BATCHED)
+    psb = csaw.make_params(0, 2, 1 << 15, 1, 10, 2, seed=0x29B, schedule=csaw.SCHED_BATCHED)
+    S = csaw.StreamGraph(g, partition_bits=17, slot_budget_bytes=budget, rowptr64=True)
+    G = csaw.Graph(g, rowptr64=True)
+    sw = G.make_seeds(1 << 17, 0x29C)
+    ss = G.make_seeds(1 << 15, 0x29D)
+    outs = {k: torch.empty((4, csaw.edge_bound(p)), dtype=torch.int32, device="cuda") for k, p in (("w", pw), ("s", ps))}
+
+    def step(obj, batched=False):
+        a = obj.sample(pwb if batched else pw, sw, out=outs["w"])
+        b = obj.sample(psb if batched else ps, ss, out=outs["s"])
+        return a[0].numel() + b[0].numel()
+
+    for name, obj, bt in (("stream", S, False), ("in_memory", G, False), ("in_memory_batched", G, True)):
+        for _ in range(args.warmup):
+            step(obj, bt)
+        torch.cuda.synchronize()
+        i0 = S.info() if name == "stream" else None
+        t0 = time.perf_counter()
+        e = sum(step(obj, bt) for _ in range(args.steps))
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / args.steps
+        r = {"ms_per_step": dt * 1e3, "edges_per_step": e / args.steps, "seps": e / args.steps / dt}
+        if name == "stream":
+            i1 = S.info()
+            r["h2d_bytes_per_step"] = (i1["bytes_h2d"] - i0["bytes_h2d"]) / args.steps
+            r["partition_loads_per_step"] = (i1["partition_loads"] - i0["partition_loads"]) / args.steps
+            r["partitions"] = i1["n_partitions"]
+            r["slots"] = i1["n_slots"]
+            r["h2d_gbs"] = r["h2d_bytes_per_step"] / dt / 1e9
+        res[name] = r
+    assert res["stream"]["edges_per_step"] == res["in_memory"]["edges_per_step"] == \
+        res["in_memory_batched"]["edges_per_step"]
+    res["stream_vs_in_memory"] = res["stream"]["seps"] / res["in_memory"]["seps"]
+    S.close()
+    G.close()
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -457,6 +521,7 @@ def main():
     ap.add_argument("--serve", action="store_true", help="run only the serving (request loop) workload")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving workload in the default run")
     ap.add_argument("--scale25", action="store_true", help="run only the R-MAT scale-25 learned-scheduler workload")
+    ap.add_argument("--stream", action="store_true", help="run only the streaming (out-of-budget) workload")
     ap.add_argument("--s25-scale", type=int, default=25,
                     help="R-MAT scale for --scale25 (samples and walks scale with 2^scale; smaller for profiling)")
     ap.add_argument("--s25-forms", default="batched,learned", help="forms timed by --scale25")
@@ -471,6 +536,9 @@ def main():
         return
     if args.learned_gain:
         learned_gain(args)
+        return
+    if args.stream:
+        print(json.dumps({"streaming": streaming(args)}))
         return
     if args.scale25:
         print(json.dumps({"scale25": scale25(args)}))

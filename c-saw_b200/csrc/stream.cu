@@ -139,6 +139,7 @@ struct csaw_stream_graph_s {
     int32_t *slot_col = nullptr;
     float *slot_w = nullptr;          // null when the graph has no weights
     std::vector<int> slot_part;
+    std::vector<char> slot_has_w;     // the slot holds its partition's weights too
     std::vector<cudaEvent_t> slot_ready, slot_free;
     cudaStream_t copy = nullptr;
     Buf q[3][3], counts, offsets, cursor, heavy, hscratch, ctr;
@@ -166,6 +167,17 @@ int make_resident(csaw_stream_graph_s *g, int part, bool need_w, const std::vect
                   int keep, bool use, cudaStream_t compute, int *slot_out) {
     for (int s = 0; s < g->nslots; ++s)
         if (g->slot_part[s] == part) {
+            if (need_w && g->slot_w && !g->slot_has_w[s]) {   // resident without its weights: add them
+                const int64_t e0 = g->pbeg[part], ne = g->pbeg[part + 1] - e0;
+                SCK(cudaStreamWaitEvent(g->copy, g->slot_free[s], 0));
+                if (ne > 0) {
+                    SCK(cudaMemcpyAsync(g->slot_w + (size_t)s * g->max_pedges, g->h_w + e0, sizeof(float) * ne,
+                                        cudaMemcpyHostToDevice, g->copy));
+                    g->bytes_h2d += 4 * ne;
+                }
+                SCK(cudaEventRecord(g->slot_ready[s], g->copy));
+                g->slot_has_w[s] = 1;
+            }
             if (use) {   // a use (not a prefetch): wait for the copy
                 g->hits++;
                 SCK(cudaStreamWaitEvent(compute, g->slot_ready[s], 0));
@@ -207,6 +219,7 @@ int make_resident(csaw_stream_graph_s *g, int part, bool need_w, const std::vect
     }
     SCK(cudaEventRecord(g->slot_ready[victim], g->copy));
     g->slot_part[victim] = part;
+    g->slot_has_w[victim] = need_w && g->slot_w ? 1 : 0;
     g->loads++;
     if (use) SCK(cudaStreamWaitEvent(compute, g->slot_ready[victim], 0));
     *slot_out = victim;
@@ -432,6 +445,7 @@ extern "C" int csaw_stream_graph_create(const void *rowptr, int rowptr_is_64, co
         cudaMalloc((void **)&g->slot_w, sizeof(float) * (size_t)std::max<int64_t>(g->max_pedges, 1) * ns) != cudaSuccess)
         return bail("slot allocation failed", CSAW_ERR_NOMEM);
     g->slot_part.assign((size_t)ns, -1);
+    g->slot_has_w.assign((size_t)ns, 0);
     g->slot_ready.resize((size_t)ns);
     g->slot_free.resize((size_t)ns);
     for (int64_t k = 0; k < ns; ++k) {

@@ -71,3 +71,18 @@ def test_stream_rejects_mdrw_and_tiny_budget(csaw, powerlaw_small):
     p = csaw.make_params(2, 1, 10, 4, 1, 5, None, seed=1)
     with pytest.raises(csaw.CsawError):
         sg.sample(p, torch.zeros(40, dtype=torch.int32, device="cuda"))
+
+
+def test_stream_weights_added_to_resident_partitions(csaw, powerlaw_small):
+    """A degree-biased job leaves partitions resident without their weights;
+    an edge-weight job on the same streaming graph must still see them."""
+    import torch
+    g = powerlaw_small
+    sg = csaw.StreamGraph(g, partition_bits=11, slot_budget_bytes=64 << 20)
+    seeds = oracle.make_seeds(g.rowptr, 300, 7)
+    sd = torch.from_numpy(seeds).cuda()
+    for bias in (1, 2, 1, 2):
+        p = csaw.make_params(0, bias, 300, 1, 10, 2, [10, 5], seed=3)
+        a = [x.cpu().numpy() for x in sg.sample(p, sd)]
+        b = oracle.run(g.rowptr, g.col, g.weight, seeds, 0, bias, 300, 1, 2, [10, 5], seed=3, n_threads=8)
+        _same(a, b)
