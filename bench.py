@@ -345,6 +345,9 @@ def serving(args, n_slots=8):
     for k in range(3):   # n_slots largest requests at once: every slot grows its scratch once
         run_stream(csaw, S, serve_requests(csaw, g, n_slots, rng, kind=k, n_seeds=8192), 1e6, rng, pool)
     run_stream(csaw, S, serve_requests(csaw, g, 400, rng), SERVE_RATE, rng, pool)
+    # and the 1024-seed 2-hop shape, so its page-locked output buffers exist
+    # before timing (allocating them takes the driver lock for milliseconds)
+    run_stream(csaw, S, serve_requests(csaw, g, 200, rng, kind=0, n_seeds=1024), SERVE_RATE, rng, pool)
     S.stats(reset=True)
     for name, rate, reqs in (
             ("mixed", SERVE_RATE, serve_requests(csaw, g, args.serve_requests, rng)),
