@@ -419,6 +419,8 @@ def scale25(args):
             r["class_mask"] = G.sched_info()["class_mask"]
         for _ in range(args.warmup):
             G.sample_batch(jobs)
+        if form == "batched":
+            r["autotune"] = G.autotune(jobs)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -628,6 +630,11 @@ def main():
     other = {}
     if "plain" in forms and main_form != "plain":
         plain_edges, plain_ms, plain_k, _, _ = timed("plain", profile=True)
+    tune = None
+    if "batched" in forms:   # the launch-shape autotuner, on the batched form's own batch
+        for _ in range(args.warmup):
+            step("batched")
+        tune = G.autotune(batch_jobs["batched"])
     if "batched" in forms and main_form != "batched":
         other["batched"] = timed("batched")[1]
     sched = None
@@ -725,7 +732,7 @@ def main():
                           "speedup_vs_plain": plain_t / t_max if plain_t else None,
                           **{f: all_edges / (ms_f / 1e3) for f, ms_f in other.items()},
                           **({"learned_vs_batched": (other["batched"] / ms)} if "batched" in other else {}),
-                          "scheduler": sched,
+                          "scheduler": sched, "autotune": tune,
                           "plain_kernels": {k: v for k, v in plain_k.items() if v["launches"]}},
                 "edges_per_step": all_edges / args.steps / world}
         if not args.no_cpu_baseline:

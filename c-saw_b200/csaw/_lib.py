@@ -26,10 +26,12 @@ EXPORTS = [
     "csaw_graph_set_option", "csaw_stream_graph_create", "csaw_stream_graph_destroy", "csaw_stream_sample",
     "csaw_stream_stats", "csaw_sched_info", "csaw_sched_get_records", "csaw_sched_train", "csaw_sched_classes", "csaw_sched_get_model", "csaw_sched_set_model",
     "csaw_mlp_grad_host", "csaw_server_create", "csaw_server_destroy", "csaw_server_submit", "csaw_server_wait",
-    "csaw_server_get_stats",
+    "csaw_server_get_stats", "csaw_graph_autotune",
 ]
 OPT_CUDA_GRAPHS = 1
 OPT_SCHED_RECORD = 2
+OPT_GRID_PCT = 3
+OPT_PAIR = 4
 MLP_NPARAM, MLP_NORM = 1542, 18
 
 
@@ -65,6 +67,11 @@ class ServerStats(ctypes.Structure):
                                                "peak_device_bytes", "workspace_bytes")] + \
                [(f, ctypes.c_double) for f in ("p50_ms", "p90_ms", "p99_ms", "max_ms", "mean_ms", "p99_queue_ms",
                                                 "p99_launch_ms", "p99_gpu_ms", "first_submit_s", "last_done_s")]
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("grid_pct", ctypes.c_int32), ("pair", ctypes.c_int32), ("best_ms", ctypes.c_double),
+                ("default_ms", ctypes.c_double), ("candidates", ctypes.c_int32)]
 
 
 class Job(ctypes.Structure):
@@ -133,6 +140,7 @@ def lib():
     L.csaw_sched_get_model.argtypes = [p, p, p]
     L.csaw_sched_set_model.argtypes = [p, p, p]
     L.csaw_mlp_grad_host.argtypes = [p, p, p, i32, p, PF]
+    L.csaw_graph_autotune.argtypes = [p, ctypes.POINTER(Job), i32, p, ctypes.POINTER(TuneResult)]
     L.csaw_server_create.argtypes = [p, ctypes.POINTER(ServerConfig), ctypes.POINTER(p)]
     L.csaw_server_destroy.argtypes = [p]
     L.csaw_server_submit.argtypes = [p, ctypes.POINTER(Params), p, p, p, p, p, i64, ctypes.POINTER(ctypes.c_uint64)]

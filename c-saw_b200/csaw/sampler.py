@@ -195,6 +195,17 @@ class Graph:
         return (out[0, :k], out[1, :k], out[2, :k] if with_sample else None,
                 out[2 + with_sample, :k] if with_depth else None)
 
+    def autotune(self, jobs, stream=None):
+        """Times the batch under each launch shape (csaw_graph_autotune) and
+        keeps the fastest; returns the chosen shape and times."""
+        arr = (_lib.Job * len(jobs))()
+        for j, bj in zip(arr, jobs):
+            bj.fill(j)
+        r = _lib.TuneResult()
+        st = stream if stream is not None else _torch().cuda.current_stream().cuda_stream
+        check(lib().csaw_graph_autotune(self.h, arr, len(jobs), ctypes.c_void_p(st), ctypes.byref(r)))
+        return {f: getattr(r, f) for f, _ in _lib.TuneResult._fields_}
+
     def sample_batch(self, jobs, stream=None):
         """Run several BatchJobs together (csaw_sample_batch); returns their edge lists."""
         arr = (_lib.Job * len(jobs))()

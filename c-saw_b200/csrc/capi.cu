@@ -137,6 +137,8 @@ struct csaw_graph_s {
     float *cdf[4] = {};           // per bias kind: canonical per-vertex prefix, or null
     bool cdf_flag = false;        // CSAW_GRAPH_CDF_CACHE: visible to the plain schedule too
     bool cdf_off = false;         // CSAW_GRAPH_NO_CDF_CACHE
+    int grid_pct = 100;           // CSAW_OPT_GRID_PCT
+    bool pair = true;             // CSAW_OPT_PAIR
     uint32_t class_mask = 0x3f;   // classes the trained model picks (bit c)
     int32_t *big_verts = nullptr; // vertices above CDF_BIG (the cache builds them one CTA each)
     int64_t n_big = 0;
@@ -463,13 +465,16 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
         }
     }
     const SchedArgs *sched = nullptr;
-    const int hgrid = plain ? 0 : grid_for(k_select_hub<I, BIAS>, FAST_THREADS, 0, g->sm_count);
-    const int pgrid = plain ? 0 : grid_for(k_select_pair<I, BIAS>, FAST_THREADS, 0, g->sm_count);
+    const int hgrid = plain ? 0 : std::max(1, grid_for(k_select_hub<I, BIAS>, FAST_THREADS, 0, g->sm_count) *
+                                                     g->grid_pct / 100);
+    const int pgrid = plain ? 0 : std::max(1, grid_for(k_select_pair<I, BIAS>, FAST_THREADS, 0, g->sm_count) *
+                                                     g->grid_pct / 100);
     if (BIASED && ((!plain && g->maxdeg > WF) || g->cdf_flag)) TRY((ensure_cdf<I, BIAS>(g, st)));
     const bool cached = BIASED && g->cdf[BIAS] && (!plain || g->cdf_flag);
+    auto shaped = [&](int gsz) { return std::max(1, (int)((int64_t)gsz * g->grid_pct / 100)); };
     const int sgrid = plain ? 0
-                      : (cached ? grid_for(k_select_fast<I, BIAS, true>, FAST_THREADS, 0, g->sm_count)
-                                : grid_for(k_select_fast<I, BIAS, false>, FAST_THREADS, 0, g->sm_count));
+                      : shaped(cached ? grid_for(k_select_fast<I, BIAS, true>, FAST_THREADS, 0, g->sm_count)
+                                      : grid_for(k_select_fast<I, BIAS, false>, FAST_THREADS, 0, g->sm_count));
     if (!plain) {
         TRY(ensure_nbr(g, st));
         TRY(ensure(c->sel, sizeof(SelEntry) * qcap, st));
@@ -515,7 +520,7 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
     const DevGraph dg = dev_view(g, p->schedule, BIAS);
     const uint64_t seed = p->seed;
     const int grid = plain ? grid_for(k_expand_warp<I, BIAS>, EXPAND_THREADS, 0, g->sm_count)
-                           : grid_for(k_coop_fast<I, BIAS>, FAST_THREADS, 0, g->sm_count);
+                           : shaped(grid_for(k_coop_fast<I, BIAS>, FAST_THREADS, 0, g->sm_count));
     for (int64_t s0 = 0; s0 < S; s0 += B) {
         const int64_t nb = (S - s0 < B) ? S - s0 : B;
         const uint32_t n0 = (uint32_t)(nb * F);
@@ -563,7 +568,7 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
             a.sched_tab = tabled ? (const uint8_t *)c->stab.p : nullptr;
             a.hub_list = (SelEntry *)c->hubsel.p;
             a.n_hub = &c->ctr->n_hub;
-            const bool paired = cached && g->maxdeg > WF && fan[l] <= 16;
+            const bool paired = cached && g->maxdeg > WF && fan[l] <= 16 && g->pair;
             a.pair_list = paired ? (SelEntry *)c->pairsel.p : nullptr;
             a.n_pair = &c->ctr->n_pair;
             a.refill_list = (SelEntry *)c->sel.p;   // free once k_select_fast has run
@@ -1407,9 +1412,73 @@ extern "C" int csaw_graph_set_option(csaw_graph g, int option, int64_t value) {
             g->recording = value > 0;
             ++g_alloc_epoch;   // launch sets differ by mode: drop cached graphs
             return 0;
+        case CSAW_OPT_GRID_PCT:
+            if (value < 25 || value > 400) return fail(CSAW_ERR_INVALID, "grid percent must be in [25, 400]");
+            g->grid_pct = (int)value;
+            ++g_alloc_epoch;   // launch shapes are baked into cached graphs
+            return 0;
+        case CSAW_OPT_PAIR:
+            g->pair = value != 0;
+            ++g_alloc_epoch;
+            return 0;
         default:
             return fail(CSAW_ERR_INVALID, "unknown option");
     }
+}
+
+extern "C" int csaw_graph_autotune(csaw_graph g, csaw_job *jobs, int n_jobs, void *stream, csaw_tune_result *out) {
+    if (!g || !out) return fail(CSAW_ERR_INVALID, "NULL argument");
+    CK(cudaSetDevice(g->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    const int pcts[3] = {100, 50, 200};
+    const int old_pct = g->grid_pct;
+    const bool old_pair = g->pair, old_graphs = g->use_graphs;
+    g->use_graphs = false;   // each candidate timed launch by launch
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    double best = 1e300, dflt = 0.0;
+    int best_pct = old_pct, n = 0;
+    bool best_pair = old_pair;
+    int rc = 0;
+    for (int pair = 1; pair >= 0 && !rc; --pair)
+        for (int k = 0; k < 3 && !rc; ++k) {
+            g->grid_pct = pcts[k];
+            g->pair = pair != 0;
+            rc = csaw_sample_batch(g, jobs, n_jobs, stream);   // untimed: workspace, caches
+            if (rc) break;
+            cudaEventRecord(e0, st);
+            rc = csaw_sample_batch(g, jobs, n_jobs, stream);
+            cudaEventRecord(e1, st);
+            if (rc) break;
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ++n;
+            if (pair == 1 && pcts[k] == 100) dflt = ms;
+            if (ms < best) {
+                best = ms;
+                best_pct = pcts[k];
+                best_pair = pair != 0;
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    g->use_graphs = old_graphs;
+    if (rc) {
+        g->grid_pct = old_pct;
+        g->pair = old_pair;
+        return rc;
+    }
+    g->grid_pct = best_pct;
+    g->pair = best_pair;
+    ++g_alloc_epoch;
+    out->grid_pct = best_pct;
+    out->pair = best_pair ? 1 : 0;
+    out->best_ms = best;
+    out->default_ms = dflt;
+    out->candidates = n;
+    return 0;
 }
 
 extern "C" int csaw_sched_info(csaw_graph g, int64_t *n_records, int *trained, float *last_loss) {

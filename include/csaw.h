@@ -200,9 +200,31 @@ enum {
     /* n > 0: the next CSAW_SCHED_LEARNED runs record up to n execution
      * profiles (features, granularity, cycles) with a random valid
      * granularity per item; 0: stop recording. */
-    CSAW_OPT_SCHED_RECORD = 2
+    CSAW_OPT_SCHED_RECORD = 2,
+    /* Launch shape of the batched kernels (never changes the output):
+     * persistent grid size in percent of the occupancy-filled grid
+     * (25..400, default 100) ... */
+    CSAW_OPT_GRID_PCT = 3,
+    /* ... and whether cached items with N <= 16 run two per warp (1, the
+     * default) or one per warp (0). */
+    CSAW_OPT_PAIR = 4
 };
 int csaw_graph_set_option(csaw_graph g, int option, int64_t value);
+
+/*
+ * Autotuner of the launch shape for a recurring batch (north-star "tile
+ * sizes from an autotuner"; the reference fixes n_blocks x n_threads by
+ * hand, main.cu:219-224): times the batch under each candidate
+ * (grid 50/100/200 % x pairing on/off), device-timed, after one untimed run
+ * each, and keeps the fastest in the graph's options.  The jobs' outputs are
+ * overwritten by the runs (identical under every candidate).
+ */
+typedef struct {
+    int32_t grid_pct, pair;         /* chosen shape */
+    double best_ms, default_ms;     /* its time, and the default shape's */
+    int32_t candidates;
+} csaw_tune_result;
+int csaw_graph_autotune(csaw_graph g, csaw_job *jobs, int n_jobs, void *stream, csaw_tune_result *out);
 
 /*
  * Learned execution-granularity scheduler (CSAW_SCHED_LEARNED).  Replaces

@@ -1,0 +1,64 @@
+"""Launch shapes and the autotuner: the batched kernels' grid size and the
+two-items-per-warp pairing never change the output; the autotuner keeps the
+fastest shape of the candidates it timed."""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import sort_edges
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def csaw():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("gpu test without a CUDA device")
+    import csaw as c
+    c.lib()
+    return c
+
+
+def jobs_for(csaw, g):
+    import torch
+    sa = torch.from_numpy(oracle.make_seeds(g.rowptr, 300 * 2, 12)).cuda()
+    sb = torch.from_numpy(oracle.make_seeds(g.rowptr, 500, 13)).cuda()
+    pa = csaw.make_params(0, 2, 300, 2, 10, 3, [10, 5, 3], seed=31, schedule=csaw.SCHED_BATCHED)
+    pb = csaw.make_params(1, 2, 500, 1, 1, 25, seed=32, schedule=csaw.SCHED_BATCHED)
+    return [csaw.BatchJob(pa, sa), csaw.BatchJob(pb, sb)]
+
+
+def edges(res):
+    return [sort_edges(*[x.cpu().numpy() for x in r]) for r in res]
+
+
+@pytest.mark.parametrize("which", ["rmat12_pareto", "powerlaw_small"])
+def test_launch_shapes_keep_output(csaw, which, request):
+    from csaw import _lib
+    g = request.getfixturevalue(which)
+    G = csaw.Graph(g)
+    jobs = jobs_for(csaw, g)
+    ref = edges(G.sample_batch(jobs))
+    for pct, pair in ((25, 1), (400, 1), (100, 0), (50, 0), (200, 1)):
+        G.set_option(_lib.OPT_GRID_PCT, pct)
+        G.set_option(_lib.OPT_PAIR, pair)
+        for _ in range(2):   # the second run of a shape replays a CUDA graph
+            got = edges(G.sample_batch(jobs))
+            assert all(np.array_equal(a, b) for a, b in zip(got, ref))
+    with pytest.raises(csaw.CsawError):
+        G.set_option(_lib.OPT_GRID_PCT, 10)
+    G.close()
+
+
+def test_autotune_keeps_fastest_and_output(csaw, rmat12_pareto):
+    G = csaw.Graph(rmat12_pareto)
+    jobs = jobs_for(csaw, rmat12_pareto)
+    ref = edges(G.sample_batch(jobs))
+    r = G.autotune(jobs)
+    assert r["candidates"] == 6
+    assert r["grid_pct"] in (50, 100, 200) and r["pair"] in (0, 1)
+    assert 0 < r["best_ms"] <= r["default_ms"]
+    got = edges(G.sample_batch(jobs))
+    assert all(np.array_equal(a, b) for a, b in zip(got, ref))
+    G.close()
