@@ -321,6 +321,14 @@ class PinnedPool:
     def put(self, cls, buf):
         self.free[cls].append(buf)
 
+    def prefill(self, cap, n):
+        """n buffers of cap's class, allocated before timing."""
+        import torch
+        cls = max(1 << 12, 1 << int(np.ceil(np.log2(max(cap, 1)))))
+        lst = self.free.setdefault(cls, [])
+        while len(lst) < n:
+            lst.append(torch.empty((2, cls), dtype=torch.int32).pin_memory())
+
 
 def serving(args, n_slots=8):
     """Serving workload: R-MAT scale 22, edge factor 16, U(0,1] weights (4.19M
@@ -348,6 +356,7 @@ def serving(args, n_slots=8):
     # and the 1024-seed 2-hop shape, so its page-locked output buffers exist
     # before timing (allocating them takes the driver lock for milliseconds)
     run_stream(csaw, S, serve_requests(csaw, g, 200, rng, kind=0, n_seeds=1024), SERVE_RATE, rng, pool)
+    pool.prefill(1024 * (25 + 250), 64)   # a burst of late waits must not allocate mid-stream
     S.stats(reset=True)
     for name, rate, reqs in (
             ("mixed", SERVE_RATE, serve_requests(csaw, g, args.serve_requests, rng)),
