@@ -62,9 +62,9 @@ def _torch():
 class Graph:
     """A CSR resident on the current CUDA device (csaw_graph_create).
 
-    cdf_cache: None builds the per-vertex bias prefix cache when a batched or
-    learned biased job meets a vertex above 512 edges; True builds it for every
-    schedule (the plain one included); False never builds it.
+    cdf_cache: None builds the per-vertex bias prefix cache on the first
+    batched or learned biased job; True builds it for every schedule (the
+    plain one included); False never builds it.
     """
 
     def __init__(self, csr, rowptr64=None, degree_bias=False, cdf_cache=None):

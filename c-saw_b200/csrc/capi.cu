@@ -283,9 +283,9 @@ int ensure_nbr(csaw_graph_s *g, cudaStream_t st) {
 constexpr int64_t CDF_BIG = 4096;   // vertices above are built by one CTA each
 
 // Per-vertex CDF cache: the canonical prefix of every vertex's biases for bias
-// kind BIAS (4E bytes), built on first biased use by a batched schedule on a
-// graph with vertices above the per-warp shared capacity, or when the graph
-// was created with CSAW_GRAPH_CDF_CACHE; never with CSAW_GRAPH_NO_CDF_CACHE.
+// kind BIAS (4E bytes, plus its search index), built on first biased use by a
+// batched schedule, or by any schedule when the graph was created with
+// CSAW_GRAPH_CDF_CACHE; never with CSAW_GRAPH_NO_CDF_CACHE.
 template <typename I, int BIAS>
 int ensure_cdf(csaw_graph_s *g, cudaStream_t st) {
     if (g->cdf[BIAS]) return 0;
@@ -469,7 +469,7 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
                                                      g->grid_pct / 100);
     const int pgrid = plain ? 0 : std::max(1, grid_for(k_select_pair<I, BIAS>, FAST_THREADS, 0, g->sm_count) *
                                                      g->grid_pct / 100);
-    if (BIASED && ((!plain && g->maxdeg > WF) || g->cdf_flag)) TRY((ensure_cdf<I, BIAS>(g, st)));
+    if (BIASED && (!plain || g->cdf_flag)) TRY((ensure_cdf<I, BIAS>(g, st)));
     const bool cached = BIASED && g->cdf[BIAS] && (!plain || g->cdf_flag);
     auto shaped = [&](int gsz) { return std::max(1, (int)((int64_t)gsz * g->grid_pct / 100)); };
     const int sgrid = plain ? 0
@@ -664,7 +664,7 @@ int run_walk_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int32_t *
                cudaStream_t st) {
     const bool plain = p->schedule == CSAW_SCHED_PLAIN;
     if (!plain) TRY(ensure_nbr(g, st));
-    if (BIAS != CSAW_BIAS_UNBIASED && ((!plain && g->maxdeg > WF) || g->cdf_flag)) TRY((ensure_cdf<I, BIAS>(g, st)));
+    if (BIAS != CSAW_BIAS_UNBIASED && (!plain || g->cdf_flag)) TRY((ensure_cdf<I, BIAS>(g, st)));
     const DevGraph dg = dev_view(g, p->schedule, BIAS);
     WalkArgs a{};
     a.seeds = seeds;
