@@ -252,3 +252,32 @@ def test_repeated_batches_replay_identically(csaw, powerlaw_small, graphs):
             assert_parity(a, b)
     ref = oracle_run(powerlaw_small, 0, 1, 100, 4, 3, [20, 20, 20], 5, sa.cpu().numpy())
     assert_parity(outs[-1][0], ref)
+
+
+@pytest.mark.parametrize("sched", SCHEDULES)
+def test_pinned_and_pageable_host_outputs(csaw, rmat12_pareto, sched):
+    """Host-buffer jobs give the same edges into page-locked and pageable
+    output arrays, for neighbor sampling and walks, alone and in a batch, and
+    a too-small capacity fails."""
+    import torch
+    g = rmat12_pareto
+    G = csaw.Graph(g)
+    seeds = oracle.make_seeds(g.rowptr, 400, 4)
+    for mode, fan, depth in ((0, [10, 5, 3], 3), (1, None, 30)):
+        p = csaw.make_params(mode, 2, 400 if mode else 100, 1 if mode else 4, (fan or [1])[0], depth, fan, 11,
+                             schedule=sched)
+        cap = csaw.edge_bound(p)
+        pinned = torch.empty((4, cap), dtype=torch.int32).pin_memory().numpy()
+        a = G.sample_host(p, seeds, out=pinned)
+        b = G.sample_host(p, seeds)
+        assert len(a[0]) > 0
+        assert_parity(a, b)
+        jobs = [csaw.BatchJob(p, seeds, cap, torch.empty((4, cap), dtype=torch.int32).pin_memory().numpy(),
+                              host=True), csaw.BatchJob(p, seeds, cap, host=True)]
+        r = G.sample_batch(jobs)
+        assert_parity(r[0], b)
+        assert_parity(r[1], b)
+    p = csaw.make_params(0, 2, 100, 4, 10, 2, [10, 5], 11, schedule=sched)
+    small = torch.empty((4, 16), dtype=torch.int32).pin_memory().numpy()
+    with pytest.raises(csaw.CsawError):
+        G.sample_host(p, seeds, capacity=16, out=small)
