@@ -48,7 +48,7 @@ FLUSH_BYTES = 256 << 20
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum, mean over
 # the three level launches of one step) from one full ncu capture of the
 # batched form of this workload; the capture is summarised under profiles/.
-DRAM_TRAFFIC = {"k_select_fast": 4.15e6, "k_coop_fast": 13.8e6, "k_walk_fast": 40.3e6}
+DRAM_TRAFFIC = {"k_select_fast": 5.01e6, "k_coop_fast": 13.8e6, "k_walk_fast": 43.1e6}
 
 
 def load_peaks():
