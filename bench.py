@@ -304,6 +304,28 @@ def run_stream(csaw, S, reqs, rate, rng, pool):
     return np.array(lat), np.array(edges), wall
 
 
+def run_closed(csaw, S, reqs, window, pool):
+    """Closed loop: at most `window` requests outstanding, the next one
+    submitted as soon as the oldest returns (the loop's sustained capacity)."""
+    from collections import deque
+    out = deque()
+    t0 = time.perf_counter()
+    edges = 0
+    for k, m, p, seeds in reqs:
+        if len(out) >= window:
+            t, buf, cls = out.popleft()
+            edges += S.wait(t)[0]
+            pool.put(cls, buf)
+        cap = csaw.edge_bound(p)
+        cls, buf = pool.get(cap)
+        out.append((S.submit(p, seeds, out=buf, capacity=cap, with_sample=False, with_depth=False), buf, cls))
+    while out:
+        t, buf, cls = out.popleft()
+        edges += S.wait(t)[0]
+        pool.put(cls, buf)
+    return edges, time.perf_counter() - t0
+
+
 class PinnedPool:
     """Page-locked (2, cap) int32 buffers by power-of-two size class."""
 
@@ -361,9 +383,13 @@ def serving(args, n_slots=8):
     for name, rate, reqs in (
             ("mixed", SERVE_RATE, serve_requests(csaw, g, args.serve_requests, rng)),
             ("twohop_1024", SERVE_RATE, serve_requests(csaw, g, args.serve_requests, rng, kind=0, n_seeds=1024)),
-            # every request at once: the loop's capacity (latency is then queueing)
-            ("mixed_saturated", 1e7, serve_requests(csaw, g, args.serve_requests, rng))):
-        lat, edges, wall = run_stream(csaw, S, reqs, rate, rng, pool)
+            # closed loop, 4 requests per slot outstanding: the loop's capacity
+            ("mixed_saturated", None, serve_requests(csaw, g, args.serve_requests, rng))):
+        if rate is None:
+            e, wall = run_closed(csaw, S, reqs, 4 * n_slots, pool)
+            edges = np.array([e])
+        else:
+            lat, edges, wall = run_stream(csaw, S, reqs, rate, rng, pool)
         st = S.stats(reset=True)
         res[name] = {"requests": len(reqs), "p50_ms": st["p50_ms"], "p90_ms": st["p90_ms"], "p99_ms": st["p99_ms"],
                      "max_ms": st["max_ms"], "mean_ms": st["mean_ms"], "p99_queue_ms": st["p99_queue_ms"],
