@@ -108,3 +108,32 @@ def test_reference_file_roundtrip(tmp_path):
     h = graphgen.read_reference_format(tmp_path / "beg.bin", tmp_path / "csr.bin")
     assert np.array_equal(g.rowptr, h.rowptr) and np.array_equal(g.col, h.col)
     assert np.fromfile(tmp_path / "beg.bin", dtype=np.int64).size == g.n_vertices + 1
+
+
+def test_device_rmat_generator_is_clean_on_cpu():
+    """rmat_device (the torch generator used for the large synthetic graphs)
+    produces a sorted CSR without self-loops or duplicates, symmetric when
+    asked, with the requested weight law; run here on the CPU device."""
+    from csaw import graphgen
+    g = graphgen.rmat_device(11, 8, seed=4, device="cpu", weight="pareto:1.5")
+    rp, col = g.rowptr, g.col
+    src = np.repeat(np.arange(g.n_vertices), np.diff(rp))
+    key = src * g.n_vertices + col
+    assert (np.diff(key) > 0).all() and (src != col).all()
+    assert np.array_equal(np.sort(col.astype(np.int64) * g.n_vertices + src), key)   # symmetric
+    assert g.weight.dtype == np.float32 and g.weight.min() >= 1.0                   # Pareto, x_m = 1
+    d = graphgen.rmat_device(11, 8, seed=4, device="cpu", symmetrize=False, weight="uniform")
+    assert d.n_edges < g.n_edges and 0.0 < d.weight.min() and d.weight.max() <= 1.0
+    again = graphgen.rmat_device(11, 8, seed=4, device="cpu", weight="pareto:1.5")
+    assert np.array_equal(again.col, g.col) and np.array_equal(again.weight, g.weight)
+
+
+def test_params_flags_layout():
+    """The Python mirror of csaw_params carries the dedup flag where the C ABI
+    expects it (size and offset of the trailing fields)."""
+    import ctypes
+    from csaw import _lib, make_params
+    p = make_params(0, 1, 10, 2, 5, 2, seed=3, dedup=True)
+    assert p.flags == _lib.PARAM_DEDUP
+    assert _lib.Params.flags.offset == _lib.Params.sample_base.offset + 8
+    assert ctypes.sizeof(_lib.Params) == _lib.Params.reserved.offset + 4
