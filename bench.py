@@ -723,6 +723,24 @@ def main():
     barrier()
     e2e_ms = e0.elapsed_time(e1)
 
+    # ---- MDRW, as the reference dispatches FrontierSize > 1 (main.cu:281-288):
+    # 4000 degree-biased samples, frontier 4, 3 steps (timed separately)
+    pm = cdist.replica_params(csaw.make_params(2, 1, 4000, 4, 20, 3, seed=SEED_A ^ 0x5A, schedule=csaw.SCHED_BATCHED),
+                              rank)
+    out_m = torch.empty((3, csaw.edge_bound(pm)), dtype=torch.int32, device="cuda")
+    for _ in range(args.warmup):
+        G.sample(pm, seeds_a, out=out_m, with_depth=False)
+    m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    m0.record(stream)
+    m_edges = 0
+    for _ in range(args.steps):
+        m_edges += G.sample(pm, seeds_a, out=out_m, with_depth=False)[0].numel()
+    m1.record(stream)
+    barrier()
+    mdrw = {"samples": 4000, "frontier_size": 4, "depth": 3, "bias": "degree",
+            "ms_per_step": m0.elapsed_time(m1) / args.steps, "edges_per_step": m_edges / args.steps,
+            "seps": m_edges / (m0.elapsed_time(m1) * 1e-3)}
+
     # ---- whole-job totals: edges summed, device time max over ranks
     t_s = ms / 1e3
     if world > 1:
@@ -769,7 +787,7 @@ def main():
                           **({"learned_vs_batched": (other["batched"] / ms)} if "batched" in other else {}),
                           "scheduler": sched, "autotune": tune,
                           "plain_kernels": {k: v for k, v in plain_k.items() if v["launches"]}},
-                "edges_per_step": all_edges / args.steps / world}
+                "edges_per_step": all_edges / args.steps / world, "mdrw": mdrw}
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(g)
         if world == 1 and not args.no_serve:
