@@ -545,6 +545,9 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
             CK(cudaMemsetAsync(&c->ctr->nq[nxt], 0, sizeof(uint32_t), st));
             CK(cudaMemsetAsync(&c->ctr->n_heavy, 0, 10 * sizeof(uint32_t), st));  // n_heavy .. n_refill
             LevelArgs a;
+            a.in_dep = nullptr;   // every item of this level is at depth l
+            a.out_dep = nullptr;
+            a.D = D;
             a.in_v = (const int32_t *)c->q[cur][0].p;
             a.in_s = (const int32_t *)c->q[cur][1].p;
             a.in_p = (const uint32_t *)c->q[cur][2].p;

@@ -102,7 +102,27 @@ struct LevelArgs {
     int *err;
     uint32_t k0, k1;
     int depth, N, push;
+    // Mixed-depth input (streaming): each item's depth in in_dep, its fanout
+    // fan[depth], children pushed while depth + 1 < D with their depth in
+    // out_dep.  Null in_dep: every item is at `depth` with N and push.
+    const int32_t *in_dep;
+    int32_t *out_dep;
+    int D;
+    uint8_t fan[CSAW_MAX_DEPTH];
 };
+
+// Level of input item `it`: depth, fanout, whether its children are pushed.
+__host__ __device__ __forceinline__ void item_level(const LevelArgs &a, uint32_t it, int &l, int &N, bool &push) {
+    if (a.in_dep) {
+        l = a.in_dep[it];
+        N = a.fan[l];
+        push = l + 1 < a.D;
+    } else {
+        l = a.depth;
+        N = a.N;
+        push = a.push != 0;
+    }
+}
 
 struct WalkArgs {
     const int32_t *seeds;

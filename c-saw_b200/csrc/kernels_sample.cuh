@@ -20,7 +20,7 @@ namespace csaw {
 // children.
 template <typename I, int BIAS>
 __device__ __forceinline__ unsigned long long expansion_bytes(const DevGraph &g, int64_t d, int k,
-                                                              bool scanned, const LevelArgs &a) {
+                                                              bool scanned, const LevelArgs &a, bool push) {
     unsigned long long b = 12 + 2 * sizeof(I);
     if (scanned) {
         if (BIAS == CSAW_BIAS_EDGE_WEIGHT || (BIAS == CSAW_BIAS_DEGREE && g.ebias))
@@ -31,7 +31,7 @@ __device__ __forceinline__ unsigned long long expansion_bytes(const DevGraph &g,
         b += 4ull * k;
     }
     b += 4ull * k * (2 + (a.o_smp != nullptr) + (a.o_dep != nullptr));
-    if (a.push) b += 12ull * k;
+    if (push) b += 12ull * k;
     return b;
 }
 
@@ -142,11 +142,13 @@ k_expand_warp(DevGraph g, LevelArgs a) {
     stg.s_dep = stg.s_smp + STAGE;
     const OutArgs oa{a.o_src, a.o_dst, a.o_smp, a.o_dep, a.o_count, a.cap};
     const uint32_t n = *a.n_in;
-    const int N = a.N;
     unsigned long long my_bytes = 0, my_items = 0;
     for (uint32_t it = gw; it < n; it += nw) {
         const int32_t v = a.in_v[it];
         if (v < 0) continue;   // dropped by per-sample dedup
+        int l, N;
+        bool push;
+        item_level(a, it, l, N, push);
         const int32_t s = a.in_s[it];
         const uint32_t p = a.in_p[it];
         const int64_t beg = row_begin<I>(g, v);
@@ -169,7 +171,7 @@ k_expand_warp(DevGraph g, LevelArgs a) {
         bool scanned = false;
         if (d > N) {
             scanned = BIASED && !(g.cdf && g.cdf_bias == BIAS);
-            const DrawCtx dc{a.k0, a.k1, p, (uint32_t)s, (uint32_t)a.depth};
+            const DrawCtx dc{a.k0, a.k1, p, (uint32_t)s, (uint32_t)l};
             sel = select_warp<I, BIAS>(g, beg, d, N, dc, P, zb, zs, lane, WBUF);
             if (sel == -2) {   // cached hub that needs a rebuild: the CTA path redoes it
                 my_items--;
@@ -189,8 +191,8 @@ k_expand_warp(DevGraph g, LevelArgs a) {
                 dst = 0;
             }
         }
-        stg.push(oa, act, v, dst, s, a.depth, lane);
-        if (a.push) {
+        stg.push(oa, act, v, dst, s, l, lane);
+        if (push) {
             uint32_t q = 0;
             if (lane == 0) q = atomicAdd(a.n_out, (uint32_t)k);
             q = __shfl_sync(FULL, q, 0);
@@ -198,9 +200,10 @@ k_expand_warp(DevGraph g, LevelArgs a) {
                 a.out_v[q + lane] = dst;
                 a.out_s[q + lane] = s;
                 a.out_p[q + lane] = p * (uint32_t)N + (uint32_t)lane;
+                if (a.out_dep) a.out_dep[q + lane] = l + 1;
             }
         }
-        my_bytes += expansion_bytes<I, BIAS>(g, d, k, scanned, a);
+        my_bytes += expansion_bytes<I, BIAS>(g, d, k, scanned, a, push);
     }
     stg.flush(oa, lane);
     if (lane == 0) {
@@ -220,10 +223,12 @@ k_expand_heavy(DevGraph g, LevelArgs a) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float *P = a.heavy_scratch + (int64_t)blockIdx.x * a.heavy_stride;
     const uint32_t nh = *a.n_heavy;
-    const int N = a.N;
     unsigned long long my_bytes = 0, my_items = 0;
     for (uint32_t h = blockIdx.x; h < nh; h += gridDim.x) {
         const uint32_t it = a.heavy_list ? a.heavy_list[h].it : a.heavy[h];
+        int l, N;
+        bool push;
+        item_level(a, it, l, N, push);
         const bool rec = a.sched && a.sched->mode == SCHED_RECORD;
         long long t0 = 0;
         if (rec && threadIdx.x == 0) t0 = clock64();
@@ -242,7 +247,7 @@ k_expand_heavy(DevGraph g, LevelArgs a) {
         auto wfn = [&](int64_t i) { return edge_bias<I, BIAS>(g, beg + i); };
         bool indexed = g.cdf && g.cdf_bias == BIAS;   // cached prefix, searched through its index
         float T = indexed ? g.cdf[beg + d - 1] : cta_canon_prefix(wfn, d, P, tsum, gcar, nullptr);
-        const DrawCtx dc{a.k0, a.k1, p, (uint32_t)s, (uint32_t)a.depth};
+        const DrawCtx dc{a.k0, a.k1, p, (uint32_t)s, (uint32_t)l};
         SlotRng rng;
         SelState st;
         auto cand_of = [&](uint32_t x, bool act) -> int {
@@ -295,7 +300,7 @@ k_expand_heavy(DevGraph g, LevelArgs a) {
             } else {
                 if (lane == 0) {
                     ob = atomicAdd(a.o_count, (unsigned long long)N);
-                    if (a.push) q = atomicAdd(a.n_out, (uint32_t)N);
+                    if (push) q = atomicAdd(a.n_out, (uint32_t)N);
                 }
                 ob = __shfl_sync(FULL, ob, 0);
                 q = __shfl_sync(FULL, q, 0);
@@ -306,12 +311,13 @@ k_expand_heavy(DevGraph g, LevelArgs a) {
                     a.o_src[pos] = v;
                     a.o_dst[pos] = dst;
                     if (a.o_smp) a.o_smp[pos] = s;
-                    if (a.o_dep) a.o_dep[pos] = a.depth;
+                    if (a.o_dep) a.o_dep[pos] = l;
                 }
-                if (a.push) {
+                if (push) {
                     a.out_v[q + lane] = dst;
                     a.out_s[q + lane] = s;
                     a.out_p[q + lane] = p * (uint32_t)N + (uint32_t)lane;
+                    if (a.out_dep) a.out_dep[q + lane] = l + 1;
                     if (a.out_beg) {
                         const int64_t nb = row_begin<I>(g, dst);
                         ((I *)a.out_beg)[q + lane] = (I)nb;
@@ -321,10 +327,10 @@ k_expand_heavy(DevGraph g, LevelArgs a) {
             }
         }
         my_items++;
-        my_bytes += expansion_bytes<I, BIAS>(g, d, N, true, a);
+        my_bytes += expansion_bytes<I, BIAS>(g, d, N, true, a, push);
         __syncthreads();
         if (rec && threadIdx.x == 0)
-            record_profile(a.sched, d, N, a.sched->vstats[v], *a.n_in, a.depth, 2 + a.cta_class, clock64() - t0);
+            record_profile(a.sched, d, N, a.sched->vstats[v], *a.n_in, l, 2 + a.cta_class, clock64() - t0);
     }
     if (threadIdx.x == 0) {
         atomicAdd(&a.bytes[1], my_bytes);

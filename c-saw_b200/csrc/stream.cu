@@ -10,23 +10,33 @@
 //   - row offsets stay resident; column ids (and weights when the bias needs
 //     them) stay in page-locked host memory, split into vertex-range
 //     partitions of 2^k vertices;
-//   - a fixed number of device slots (from the byte budget) hold partitions;
-//     a level's partition order is known, so the victim is the slot whose
-//     partition is needed farthest ahead (or never);
-//   - copies run on a copy stream, each slot has a ready event (copy done)
-//     and a free event (last kernel using it done); the next partition's copy
-//     is issued before the current partition's kernels, so transfer overlaps
-//     sampling;
-//   - frontier items are binned by partition each level (histogram, scan,
-//     scatter); the level-expansion kernel runs once per resident partition
-//     on that partition's items with the column/weight pointers re-based onto
-//     the slot, so col[e] of any edge of the partition is read from HBM;
+//   - resident partitions live in one device arena of the byte budget, each
+//     in a region of its own size (first fit), so many small partitions fit
+//     beside a few large ones;
+//   - the frontier is asynchronous: every pending item carries its depth,
+//     and pending items are kept sorted by (partition, depth) (histogram,
+//     scan, scatter).  A round processes all pending items of the resident
+//     partitions, whatever their depth; only when no resident partition has
+//     pending items are new ones loaded: the not-yet-visited partitions of
+//     the current sweep with the most pending items per byte, as many as fit
+//     once partitions without pending items are evicted.  A sweep ends when
+//     every partition with pending items has been visited.  Walks that stay
+//     within resident partitions advance many steps per load;
+//   - copies run on a copy stream; each partition has a ready event (copy
+//     done) and a free event (last kernel using it done), so an eviction
+//     waits only for that partition's kernels;
+//   - the expansion kernel runs once per resident partition on all of its
+//     pending items, whatever their depths (each item carries its depth;
+//     its fanout and whether it pushes children follow from it), with the
+//     column/weight pointers re-based onto the partition's region, so col[e]
+//     of any edge of the partition is read from HBM;
 //   - walks are neighbor sampling with N = 1 (same keys, same output).
 // Because every draw is keyed by (sample, depth, lineage, slot, draw), the
-// output equals the in-memory output exactly, whatever the partition order.
+// output equals the in-memory output exactly, whatever the processing order.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -43,20 +53,41 @@ struct StreamCounters {
     unsigned long long out_count;
     unsigned long long bytes[8];
     unsigned long long items[8];
-    uint32_t n_next;      // unsorted next-level items
+    uint32_t n_next;      // unsorted new items (children)
     uint32_t n_heavy;
     int err;
-    uint32_t pad;
+    uint32_t n_pend;      // pending items, sorted by (partition, depth)
 };
 
-__global__ void k_part_hist(const int32_t *v, const uint32_t *n, int pbits, uint32_t *counts) {
+// Pending-set histogram over (partition, depth) keys; items of partitions
+// flagged in skip (processed this round) are left out.
+__global__ void k_key_hist(const int32_t *v, const int32_t *dep, const uint32_t *n, int pbits, int D,
+                           const uint8_t *skip, uint32_t *counts) {
     const uint32_t m = *n;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
-        atomicAdd(&counts[v[i] >> pbits], 1u);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        const int part = v[i] >> pbits;
+        if (skip && skip[part]) continue;
+        atomicAdd(&counts[part * D + dep[i]], 1u);
+    }
 }
 
-// Exclusive scan of npart counts into offsets[0..npart] and a cursor copy
-// (one block; npart is at most a few thousand).
+__global__ void k_key_scatter(const int32_t *v, const int32_t *s, const uint32_t *p, const int32_t *dep,
+                              const uint32_t *n, int pbits, int D, const uint8_t *skip, uint32_t *cursor, int32_t *ov,
+                              int32_t *os, uint32_t *op, int32_t *od) {
+    const uint32_t m = *n;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        const int part = v[i] >> pbits;
+        if (skip && skip[part]) continue;
+        const uint32_t pos = atomicAdd(&cursor[part * D + dep[i]], 1u);
+        ov[pos] = v[i];
+        os[pos] = s[i];
+        op[pos] = p[i];
+        od[pos] = dep[i];
+    }
+}
+
+
+// Exclusive scan of n counts into offsets[0..n] and a cursor copy (one block).
 __global__ void k_part_scan(const uint32_t *counts, int npart, uint32_t *offsets, uint32_t *cursor) {
     __shared__ uint32_t carry;
     if (threadIdx.x == 0) carry = 0;
@@ -95,17 +126,6 @@ __global__ void k_part_scan(const uint32_t *counts, int npart, uint32_t *offsets
     if (threadIdx.x == 0) offsets[npart] = carry;
 }
 
-__global__ void k_part_scatter(const int32_t *v, const int32_t *s, const uint32_t *p, const uint32_t *n, int pbits,
-                               uint32_t *cursor, int32_t *ov, int32_t *os, uint32_t *op) {
-    const uint32_t m = *n;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-        const uint32_t pos = atomicAdd(&cursor[v[i] >> pbits], 1u);
-        ov[pos] = v[i];
-        os[pos] = s[i];
-        op[pos] = p[i];
-    }
-}
-
 struct Buf {
     void *p = nullptr;
     size_t n = 0;
@@ -135,14 +155,17 @@ struct csaw_stream_graph_s {
     const int32_t *h_col = nullptr;
     const float *h_w = nullptr;
     bool reg_col = false, reg_w = false;
-    int nslots = 0;
-    int32_t *slot_col = nullptr;
-    float *slot_w = nullptr;          // null when the graph has no weights
-    std::vector<int> slot_part;
-    std::vector<char> slot_has_w;     // the slot holds its partition's weights too
-    std::vector<cudaEvent_t> slot_ready, slot_free;
+    int nslots = 0;                   // largest partitions the budget holds (reported)
+    unsigned char *arena = nullptr;   // resident partitions, one region each
+    int64_t arena_bytes = 0;
+    std::map<int64_t, int64_t> free_regions;   // offset -> bytes
+    std::vector<int64_t> res_off;     // per partition: region offset, or -1
+    std::vector<int64_t> res_bytes;
+    std::vector<char> res_w;          // region holds the partition's weights too
+    std::vector<int> resident;        // resident partitions, in load order
+    std::vector<cudaEvent_t> ready, freed;   // per partition, created on first load
     cudaStream_t copy = nullptr;
-    Buf q[3][3], counts, offsets, cursor, heavy, hscratch, ctr;
+    Buf q[3][4], counts, offsets, cursor, heavy, hscratch, ctr, skip, pcount;
     StreamCounters *hctr = nullptr;
     int64_t loads = 0, hits = 0, bytes_h2d = 0, launches = 0;
 };
@@ -158,79 +181,115 @@ namespace {
         }                                                                           \
     } while (0)
 
-// Makes partition `part` resident and returns its slot.  On a miss the victim
-// is the slot whose partition is needed farthest ahead in `order` (from
-// position `from`), or never; `keep` is never evicted.  The copy waits for the
-// victim's last kernel; for a use (not a prefetch) the compute stream -- which
-// may be the legacy default stream, handle 0 -- waits for the copy.
-int make_resident(csaw_stream_graph_s *g, int part, bool need_w, const std::vector<int> &order, size_t from,
-                  int keep, bool use, cudaStream_t compute, int *slot_out) {
-    for (int s = 0; s < g->nslots; ++s)
-        if (g->slot_part[s] == part) {
-            if (need_w && g->slot_w && !g->slot_has_w[s]) {   // resident without its weights: add them
-                const int64_t e0 = g->pbeg[part], ne = g->pbeg[part + 1] - e0;
-                SCK(cudaStreamWaitEvent(g->copy, g->slot_free[s], 0));
-                if (ne > 0) {
-                    SCK(cudaMemcpyAsync(g->slot_w + (size_t)s * g->max_pedges, g->h_w + e0, sizeof(float) * ne,
-                                        cudaMemcpyHostToDevice, g->copy));
-                    g->bytes_h2d += 4 * ne;
-                }
-                SCK(cudaEventRecord(g->slot_ready[s], g->copy));
-                g->slot_has_w[s] = 1;
-            }
-            if (use) {   // a use (not a prefetch): wait for the copy
-                g->hits++;
-                SCK(cudaStreamWaitEvent(compute, g->slot_ready[s], 0));
-            }
-            *slot_out = s;
-            return 0;
-        }
-    // victim: an empty slot, else the partition needed farthest ahead (or never)
-    int victim = -1;
-    size_t far = 0;
-    for (int s = 0; s < g->nslots; ++s) {
-        if (s == keep) continue;
-        size_t nu = SIZE_MAX;
-        if (g->slot_part[s] >= 0) {
-            nu = SIZE_MAX - 1;
-            for (size_t k = from; k < order.size(); ++k)
-                if (order[k] == g->slot_part[s]) {
-                    nu = k;
-                    break;
-                }
-        }
-        if (victim < 0 || nu > far) {
-            victim = s;
-            far = nu;
-        }
-    }
-    if (victim < 0) return csaw_host_fail(CSAW_ERR_INVALID, "no free partition slot");
-    const int64_t e0 = g->pbeg[part], ne = g->pbeg[part + 1] - e0;
-    SCK(cudaStreamWaitEvent(g->copy, g->slot_free[victim], 0));
-    if (ne > 0) {
-        SCK(cudaMemcpyAsync(g->slot_col + (size_t)victim * g->max_pedges, g->h_col + e0, sizeof(int32_t) * ne,
-                            cudaMemcpyHostToDevice, g->copy));
-        g->bytes_h2d += 4 * ne;
-        if (need_w && g->slot_w) {
-            SCK(cudaMemcpyAsync(g->slot_w + (size_t)victim * g->max_pedges, g->h_w + e0, sizeof(float) * ne,
-                                cudaMemcpyHostToDevice, g->copy));
-            g->bytes_h2d += 4 * ne;
-        }
-    }
-    SCK(cudaEventRecord(g->slot_ready[victim], g->copy));
-    g->slot_part[victim] = part;
-    g->slot_has_w[victim] = need_w && g->slot_w ? 1 : 0;
-    g->loads++;
-    if (use) SCK(cudaStreamWaitEvent(compute, g->slot_ready[victim], 0));
-    *slot_out = victim;
-    return 0;
-}
-
 #define STRY(x)              \
     do {                     \
         int rc_ = (x);       \
         if (rc_) return rc_; \
     } while (0)
+
+int64_t region_bytes(const csaw_stream_graph_s *g, int part, bool with_w) {
+    const int64_t ne = g->pbeg[part + 1] - g->pbeg[part];
+    const int64_t colb = (4 * std::max<int64_t>(ne, 1) + 255) & ~255ll;
+    return with_w ? 2 * colb : colb;
+}
+
+// First-fit region of `bytes` in the arena, or -1.
+int64_t region_alloc(csaw_stream_graph_s *g, int64_t bytes) {
+    for (auto it = g->free_regions.begin(); it != g->free_regions.end(); ++it) {
+        if (it->second < bytes) continue;
+        const int64_t off = it->first, rem = it->second - bytes;
+        g->free_regions.erase(it);
+        if (rem > 0) g->free_regions[off + bytes] = rem;
+        return off;
+    }
+    return -1;
+}
+
+void region_free(csaw_stream_graph_s *g, int64_t off, int64_t bytes) {
+    auto it = g->free_regions.emplace(off, bytes).first;
+    auto nx = std::next(it);
+    if (nx != g->free_regions.end() && it->first + it->second == nx->first) {
+        it->second += nx->second;
+        g->free_regions.erase(nx);
+    }
+    if (it != g->free_regions.begin()) {
+        auto pv = std::prev(it);
+        if (pv->first + pv->second == it->first) {
+            pv->second += it->second;
+            g->free_regions.erase(it);
+        }
+    }
+}
+
+// Drops partition `part` from the device; later copies into its region wait
+// for its last kernel.
+int evict(csaw_stream_graph_s *g, int part) {
+    SCK(cudaStreamWaitEvent(g->copy, g->freed[part], 0));
+    region_free(g, g->res_off[part], g->res_bytes[part]);
+    g->res_off[part] = -1;
+    g->resident.erase(std::find(g->resident.begin(), g->resident.end(), part));
+    return 0;
+}
+
+// Makes `part` resident (with its weights if need_w), evicting partitions
+// that are neither protected nor have pending items, oldest first; *ok is
+// false (nothing changed) when it does not fit without evicting those.
+int make_resident(csaw_stream_graph_s *g, int part, bool need_w, const std::vector<char> &protect,
+                  const std::vector<int64_t> &pend, bool *ok) {
+    *ok = false;
+    const bool with_w = need_w && g->h_w;
+    if (g->res_off[part] >= 0) {
+        if (!with_w || g->res_w[part]) {
+            g->hits++;
+            *ok = true;
+            return 0;
+        }
+        STRY(evict(g, part));   // resident without the weights this job needs: reload
+    }
+    const int64_t bytes = region_bytes(g, part, with_w);
+    int64_t off = region_alloc(g, bytes);
+    while (off < 0) {
+        int victim = -1;
+        for (int q : g->resident)   // nothing pending there, oldest first
+            if (!protect[q] && pend[q] == 0) {
+                victim = q;
+                break;
+            }
+        if (victim < 0)
+            for (int q : g->resident)   // or unusable by this job (weights missing)
+                if (!protect[q] && with_w && !g->res_w[q]) {
+                    victim = q;
+                    break;
+                }
+        if (victim < 0) return 0;
+        STRY(evict(g, victim));
+        off = region_alloc(g, bytes);
+    }
+    if (!g->ready[part]) {
+        SCK(cudaEventCreateWithFlags(&g->ready[part], cudaEventDisableTiming));
+        SCK(cudaEventCreateWithFlags(&g->freed[part], cudaEventDisableTiming));
+    }
+    const int64_t e0 = g->pbeg[part], ne = g->pbeg[part + 1] - e0;
+    if (ne > 0) {
+        SCK(cudaMemcpyAsync(g->arena + off, g->h_col + e0, sizeof(int32_t) * ne, cudaMemcpyHostToDevice, g->copy));
+        g->bytes_h2d += 4 * ne;
+        if (with_w) {
+            SCK(cudaMemcpyAsync(g->arena + off + bytes / 2, g->h_w + e0, sizeof(float) * ne, cudaMemcpyHostToDevice,
+                                g->copy));
+            g->bytes_h2d += 4 * ne;
+        }
+    }
+    SCK(cudaEventRecord(g->ready[part], g->copy));
+    g->res_off[part] = off;
+    g->res_bytes[part] = bytes;
+    g->res_w[part] = with_w ? 1 : 0;
+    g->resident.push_back(part);
+    g->loads++;
+    *ok = true;
+    return 0;
+}
+
+
 
 template <typename I, int BIAS>
 int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], const int32_t *seeds, int32_t *src,
@@ -238,20 +297,24 @@ int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], co
     constexpr bool BIASED = BIAS != CSAW_BIAS_UNBIASED;
     const bool need_w = (BIAS == CSAW_BIAS_EDGE_WEIGHT || BIAS == CSAW_BIAS_HOOK) && g->h_w;
     const int S = p->n_samples, F = p->mode == CSAW_MODE_WALK ? 1 : p->frontier_size, D = p->depth;
+    // pending items at once: at most every item of every level
     double per = F, lvl = F;
     for (int l = 0; l + 1 < D; ++l) {
         lvl *= fan[l];
-        per = std::max(per, lvl);
+        per += lvl;
     }
-    if (per > 4294967295.0) return csaw_host_fail(CSAW_ERR_INVALID, "lineage items exceed 2^32");
-    if (per * S > 2.0e9) return csaw_host_fail(CSAW_ERR_INVALID, "a frontier level exceeds 2e9 items");
+    if (lvl > 4294967295.0) return csaw_host_fail(CSAW_ERR_INVALID, "lineage items exceed 2^32");
+    if (per * S > 2.0e9) return csaw_host_fail(CSAW_ERR_INVALID, "the frontier exceeds 2e9 items");
     const int64_t qcap = (int64_t)(per * S) + 32;
+    const int nbins = g->npart * D;
     for (auto &qq : g->q)
         for (auto &b : qq) STRY(grow(b, sizeof(int32_t) * (size_t)qcap));
-    STRY(grow(g->counts, sizeof(uint32_t) * (size_t)g->npart));
-    STRY(grow(g->cursor, sizeof(uint32_t) * (size_t)g->npart));
-    STRY(grow(g->offsets, sizeof(uint32_t) * (size_t)(g->npart + 1)));
+    STRY(grow(g->counts, sizeof(uint32_t) * (size_t)nbins));
+    STRY(grow(g->cursor, sizeof(uint32_t) * (size_t)nbins));
+    STRY(grow(g->offsets, sizeof(uint32_t) * (size_t)(nbins + 1)));
     STRY(grow(g->ctr, sizeof(StreamCounters)));
+    STRY(grow(g->skip, (size_t)g->npart));
+    STRY(grow(g->pcount, sizeof(uint32_t) * (size_t)g->npart));
     int hblocks = 0;
     int64_t hstride = 0;
     if (BIASED && g->maxdeg > WBUF) {
@@ -263,66 +326,113 @@ int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], co
     }
     StreamCounters *c = (StreamCounters *)g->ctr.p;
     uint32_t *d_counts = (uint32_t *)g->counts.p;
+    uint8_t *d_skip = (uint8_t *)g->skip.p;
     SCK(cudaMemsetAsync(c, 0, sizeof(StreamCounters), st));
     auto qv = [&](int k, int a) { return (int32_t *)g->q[k][a].p; };
-    const int U = 2;           // unsorted next-level items
-    int A = 0, B = 1;          // sorted current / next
+    const int U = 2;      // unsorted new items
+    int A = 0, B = 1;     // sorted pending / scratch for the next sorted pending
     const int bgrid = g->sm_count * 4;
-    auto bin = [&](int into) -> int {
-        SCK(cudaMemsetAsync(d_counts, 0, sizeof(uint32_t) * g->npart, st));
-        k_part_hist<<<bgrid, 256, 0, st>>>(qv(U, 0), &c->n_next, g->pbits, d_counts);
-        k_part_scan<<<1, 1024, 0, st>>>(d_counts, g->npart, (uint32_t *)g->offsets.p, (uint32_t *)g->cursor.p);
-        k_part_scatter<<<bgrid, 256, 0, st>>>(qv(U, 0), qv(U, 1), (const uint32_t *)qv(U, 2), &c->n_next, g->pbits,
-                                              (uint32_t *)g->cursor.p, qv(into, 0), qv(into, 1),
-                                              (uint32_t *)qv(into, 2));
-        g->launches += 3;
+    // pending := (pending items of partitions not flagged in skip) + new items,
+    // sorted by (partition, depth); new := empty
+    auto rebin = [&](bool use_skip) -> int {
+        const uint8_t *sk = use_skip ? d_skip : nullptr;
+        SCK(cudaMemsetAsync(d_counts, 0, sizeof(uint32_t) * (size_t)nbins, st));
+        k_key_hist<<<bgrid, 256, 0, st>>>(qv(A, 0), qv(A, 3), &c->n_pend, g->pbits, D, sk, d_counts);
+        k_key_hist<<<bgrid, 256, 0, st>>>(qv(U, 0), qv(U, 3), &c->n_next, g->pbits, D, nullptr, d_counts);
+        k_part_scan<<<1, 1024, 0, st>>>(d_counts, nbins, (uint32_t *)g->offsets.p, (uint32_t *)g->cursor.p);
+        k_key_scatter<<<bgrid, 256, 0, st>>>(qv(A, 0), qv(A, 1), (const uint32_t *)qv(A, 2), qv(A, 3), &c->n_pend,
+                                             g->pbits, D, sk, (uint32_t *)g->cursor.p, qv(B, 0), qv(B, 1),
+                                             (uint32_t *)qv(B, 2), qv(B, 3));
+        k_key_scatter<<<bgrid, 256, 0, st>>>(qv(U, 0), qv(U, 1), (const uint32_t *)qv(U, 2), qv(U, 3), &c->n_next,
+                                             g->pbits, D, nullptr, (uint32_t *)g->cursor.p, qv(B, 0), qv(B, 1),
+                                             (uint32_t *)qv(B, 2), qv(B, 3));
+        SCK(cudaMemcpyAsync(&c->n_pend, (uint32_t *)g->offsets.p + nbins, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                            st));
+        SCK(cudaMemsetAsync(&c->n_next, 0, sizeof(uint32_t), st));
+        std::swap(A, B);
+        g->launches += 5;
         return 0;
     };
     const uint32_t n0 = (uint32_t)((int64_t)S * F);
     k_init_queue<<<(n0 + 255) / 256, 256, 0, st>>>(seeds, n0, F, (int)p->sample_base, g->V, qv(U, 0), qv(U, 1),
                                                    (uint32_t *)qv(U, 2), &c->n_next, &c->err);
+    SCK(cudaMemsetAsync(qv(U, 3), 0, sizeof(int32_t) * (size_t)n0, st));
     g->launches++;
-    STRY(bin(A));
+    STRY(rebin(false));
     int grid = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid, k_expand_warp<I, BIAS>, EXPAND_THREADS, 0);
     grid = (grid > 0 ? grid : 1) * g->sm_count;
-    std::vector<uint32_t> h_counts((size_t)g->npart);
-    std::vector<int64_t> h_off((size_t)g->npart + 1);
-    for (int l = 0; l < D; ++l) {
-        SCK(cudaMemcpyAsync(h_counts.data(), d_counts, sizeof(uint32_t) * g->npart, cudaMemcpyDeviceToHost, st));
+    std::vector<uint32_t> h_counts((size_t)nbins);
+    std::vector<int64_t> h_off((size_t)nbins + 1), pend((size_t)g->npart);
+    std::vector<uint8_t> h_skip((size_t)g->npart);
+    std::vector<uint32_t> h_pc((size_t)g->npart);
+    std::vector<char> visited((size_t)g->npart, 0), in_round((size_t)g->npart, 0);
+    for (;;) {
+        SCK(cudaMemcpyAsync(h_counts.data(), d_counts, sizeof(uint32_t) * (size_t)nbins, cudaMemcpyDeviceToHost, st));
         SCK(cudaStreamSynchronize(st));
         h_off[0] = 0;
-        for (int q = 0; q < g->npart; ++q) h_off[q + 1] = h_off[q] + h_counts[q];
-        // resident partitions first, then the others in id order
-        std::vector<int> order;
-        for (int s2 = 0; s2 < g->nslots; ++s2)
-            if (g->slot_part[s2] >= 0 && h_counts[g->slot_part[s2]] > 0) order.push_back(g->slot_part[s2]);
-        for (int q = 0; q < g->npart; ++q)
-            if (h_counts[q] > 0 && std::find(order.begin(), order.end(), q) == order.end()) order.push_back(q);
-        SCK(cudaMemsetAsync(&c->n_next, 0, sizeof(uint32_t), st));
-        for (size_t k = 0; k < order.size(); ++k) {
-            const int part = order[k];
-            int slot = -1;
-            STRY(make_resident(g, part, need_w, order, k, -1, true, st, &slot));
-            if (k + 1 < order.size() && g->nslots >= 2) {   // prefetch the next partition
-                int pslot = -1;
-                STRY(make_resident(g, order[k + 1], need_w, order, k + 1, slot, false, nullptr, &pslot));
+        for (int k = 0; k < nbins; ++k) h_off[k + 1] = h_off[k] + h_counts[k];
+        if (h_off[nbins] == 0) break;
+        for (int q = 0; q < g->npart; ++q) {
+            pend[q] = 0;
+            for (int l = 0; l < D; ++l) pend[q] += h_counts[(size_t)q * D + l];
+        }
+        // this round: the resident partitions with pending items (with the
+        // weights this job needs); if none, the next partitions of the sweep
+        std::vector<int> round;
+        for (int q : g->resident)
+            if (pend[q] > 0 && (!need_w || g->res_w[q])) round.push_back(q);
+        std::fill(in_round.begin(), in_round.end(), 0);
+        if (round.empty()) {
+            std::vector<int> cand;
+            for (int q = 0; q < g->npart; ++q)
+                if (pend[q] > 0 && !visited[q]) cand.push_back(q);
+            if (cand.empty()) {   // a new sweep
+                std::fill(visited.begin(), visited.end(), 0);
+                for (int q = 0; q < g->npart; ++q)
+                    if (pend[q] > 0) cand.push_back(q);
             }
+            // most pending items per byte first
+            std::stable_sort(cand.begin(), cand.end(), [&](int x, int y) {
+                return (double)pend[x] * (double)region_bytes(g, y, need_w) >
+                       (double)pend[y] * (double)region_bytes(g, x, need_w);
+            });
+            for (int q : cand) {
+                bool ok = false;
+                STRY(make_resident(g, q, need_w, in_round, pend, &ok));
+                if (!ok) break;
+                in_round[q] = 1;
+                visited[q] = 1;
+                round.push_back(q);
+            }
+            if (round.empty()) return csaw_host_fail(CSAW_ERR_INVALID, "no partition fits the device budget");
+        }
+        for (int q = 0; q < g->npart; ++q) h_pc[q] = (uint32_t)pend[q];
+        SCK(cudaMemcpyAsync(g->pcount.p, h_pc.data(), sizeof(uint32_t) * (size_t)g->npart, cudaMemcpyHostToDevice,
+                            st));
+        std::fill(h_skip.begin(), h_skip.end(), 0);
+        for (int part : round) {
+            SCK(cudaStreamWaitEvent(st, g->ready[part], 0));
+            h_skip[part] = 1;
+            unsigned char *base = g->arena + g->res_off[part];
             DevGraph dg{};
             dg.v.rowptr = g->d_rowptr;
             dg.v.rowptr_is_64 = g->idx64;
-            dg.v.col = g->slot_col + (size_t)slot * g->max_pedges - g->pbeg[part];
-            dg.v.weight = g->slot_w ? g->slot_w + (size_t)slot * g->max_pedges - g->pbeg[part] : nullptr;
+            dg.v.col = (const int32_t *)base - g->pbeg[part];
+            dg.v.weight = g->res_w[part] ? (const float *)(base + g->res_bytes[part] / 2) - g->pbeg[part] : nullptr;
             dg.v.n_vertices = g->V;
             dg.v.n_edges = g->E;
+            const size_t key0 = (size_t)part * D;
             LevelArgs a{};
-            a.in_v = qv(A, 0) + h_off[part];
-            a.in_s = qv(A, 1) + h_off[part];
-            a.in_p = (const uint32_t *)qv(A, 2) + h_off[part];
-            a.n_in = d_counts + part;
+            a.in_v = qv(A, 0) + h_off[key0];
+            a.in_s = qv(A, 1) + h_off[key0];
+            a.in_p = (const uint32_t *)qv(A, 2) + h_off[key0];
+            a.in_dep = qv(A, 3) + h_off[key0];
+            a.n_in = (const uint32_t *)g->pcount.p + part;
             a.out_v = qv(U, 0);
             a.out_s = qv(U, 1);
             a.out_p = (uint32_t *)qv(U, 2);
+            a.out_dep = qv(U, 3);
             a.n_out = &c->n_next;
             a.heavy = (uint32_t *)g->heavy.p;
             a.n_heavy = &c->n_heavy;
@@ -339,9 +449,8 @@ int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], co
             a.err = &c->err;
             a.k0 = (uint32_t)p->seed;
             a.k1 = (uint32_t)(p->seed >> 32);
-            a.depth = l;
-            a.N = fan[l];
-            a.push = l + 1 < D;
+            a.D = D;
+            for (int l = 0; l < D; ++l) a.fan[l] = (uint8_t)fan[l];
             if (hblocks) SCK(cudaMemsetAsync(&c->n_heavy, 0, sizeof(uint32_t), st));
             k_expand_warp<I, BIAS><<<grid, EXPAND_THREADS, 0, st>>>(dg, a);
             g->launches++;
@@ -349,12 +458,10 @@ int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], co
                 k_expand_heavy<I, BIAS><<<hblocks, HEAVY_THREADS, 0, st>>>(dg, a);
                 g->launches++;
             }
-            SCK(cudaEventRecord(g->slot_free[slot], st));
+            SCK(cudaEventRecord(g->freed[part], st));
         }
-        if (l + 1 < D) {
-            STRY(bin(B));
-            std::swap(A, B);
-        }
+        SCK(cudaMemcpyAsync(d_skip, h_skip.data(), (size_t)g->npart, cudaMemcpyHostToDevice, st));
+        STRY(rebin(true));
     }
     SCK(cudaGetLastError());
     SCK(cudaMemcpyAsync(g->hctr, c, sizeof(StreamCounters), cudaMemcpyDeviceToHost, st));
@@ -434,24 +541,25 @@ extern "C" int csaw_stream_graph_create(const void *rowptr, int rowptr_is_64, co
             g->reg_w = cudaHostRegister((void *)weights, sizeof(float) * n_edges, cudaHostRegisterDefault) == cudaSuccess;
         cudaGetLastError();
     }
-    const int64_t per_slot = std::max<int64_t>(g->max_pedges, 1) * (weights ? 8 : 4);
-    int64_t ns = slot_budget_bytes / per_slot;
+    const int64_t per_max = std::max<int64_t>(g->max_pedges, 1) * (weights ? 8 : 4);
+    int64_t ns = slot_budget_bytes / per_max;
     if (ns > g->npart) ns = g->npart;
     if (ns < std::min(2, g->npart)) return bail("slot budget holds fewer than 2 partitions", CSAW_ERR_INVALID);
     g->nslots = (int)ns;
-    if (cudaMalloc((void **)&g->slot_col, sizeof(int32_t) * (size_t)std::max<int64_t>(g->max_pedges, 1) * ns) != cudaSuccess)
-        return bail("slot allocation failed", CSAW_ERR_NOMEM);
-    if (weights &&
-        cudaMalloc((void **)&g->slot_w, sizeof(float) * (size_t)std::max<int64_t>(g->max_pedges, 1) * ns) != cudaSuccess)
-        return bail("slot allocation failed", CSAW_ERR_NOMEM);
-    g->slot_part.assign((size_t)ns, -1);
-    g->slot_has_w.assign((size_t)ns, 0);
-    g->slot_ready.resize((size_t)ns);
-    g->slot_free.resize((size_t)ns);
-    for (int64_t k = 0; k < ns; ++k) {
-        cudaEventCreateWithFlags(&g->slot_ready[k], cudaEventDisableTiming);
-        cudaEventCreateWithFlags(&g->slot_free[k], cudaEventDisableTiming);
-    }
+    // regions are 256-byte aligned: room for the padding of two largest ones
+    g->arena_bytes = ((slot_budget_bytes + 255) & ~255ll) + 1024;
+    int64_t all = 0;   // no larger than every partition at once
+    for (int q = 0; q < g->npart; ++q) all += (((4 * std::max<int64_t>(g->pbeg[q + 1] - g->pbeg[q], 1) + 255) & ~255ll)) *
+                                               (weights ? 2 : 1);
+    if (g->arena_bytes > all) g->arena_bytes = all;
+    if (cudaMalloc((void **)&g->arena, (size_t)g->arena_bytes) != cudaSuccess)
+        return bail("partition arena allocation failed", CSAW_ERR_NOMEM);
+    g->free_regions[0] = g->arena_bytes;
+    g->res_off.assign((size_t)g->npart, -1);
+    g->res_bytes.assign((size_t)g->npart, 0);
+    g->res_w.assign((size_t)g->npart, 0);
+    g->ready.assign((size_t)g->npart, nullptr);
+    g->freed.assign((size_t)g->npart, nullptr);
     if (cudaStreamCreateWithFlags(&g->copy, cudaStreamNonBlocking) != cudaSuccess)
         return bail("copy stream creation failed", CSAW_ERR_CUDA);
     if (cudaMallocHost((void **)&g->hctr, sizeof(StreamCounters)) != cudaSuccess)
@@ -466,13 +574,15 @@ extern "C" int csaw_stream_graph_destroy(csaw_stream_graph g) {
     if (g->copy) cudaStreamSynchronize(g->copy);
     cudaDeviceSynchronize();
     cudaFree(g->d_rowptr);
-    cudaFree(g->slot_col);
-    cudaFree(g->slot_w);
+    cudaFree(g->arena);
     for (auto &qq : g->q)
         for (auto &b : qq) cudaFree(b.p);
-    for (Buf *b : {&g->counts, &g->offsets, &g->cursor, &g->heavy, &g->hscratch, &g->ctr}) cudaFree(b->p);
-    for (auto e : g->slot_ready) cudaEventDestroy(e);
-    for (auto e : g->slot_free) cudaEventDestroy(e);
+    for (Buf *b : {&g->counts, &g->offsets, &g->cursor, &g->heavy, &g->hscratch, &g->ctr, &g->skip, &g->pcount})
+        cudaFree(b->p);
+    for (auto e : g->ready)
+        if (e) cudaEventDestroy(e);
+    for (auto e : g->freed)
+        if (e) cudaEventDestroy(e);
     if (g->copy) cudaStreamDestroy(g->copy);
     if (g->hctr) cudaFreeHost(g->hctr);
     if (g->reg_col) cudaHostUnregister((void *)g->h_col);
