@@ -712,16 +712,23 @@ def main():
         return ra[0].size + rb[0].size
 
     e2e_steps = max(3, args.steps // 2)
-    e2e_step()
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    e2e_edges = 0
-    for _ in range(e2e_steps):
-        e2e_edges += e2e_step()
-    e1.record(stream)
-    barrier()
-    e2e_ms = e0.elapsed_time(e1)
+
+    def e2e_time(parts):
+        # parts: CSAW_OPT_HOST_PARTS (0 = by output size; -1 = copy after sampling)
+        G.set_option(csaw._lib.OPT_HOST_PARTS, parts)
+        e2e_step()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        n = 0
+        for _ in range(e2e_steps):
+            n += e2e_step()
+        e1.record(stream)
+        barrier()
+        return n, e0.elapsed_time(e1)
+
+    one_edges, one_ms = e2e_time(-1)
+    e2e_edges, e2e_ms = e2e_time(0)
 
     # ---- MDRW, as the reference dispatches FrontierSize > 1 (main.cu:281-288):
     # 4000 degree-biased samples, frontier 4, 3 steps (timed separately)
@@ -746,9 +753,11 @@ def main():
     if world > 1:
         all_edges, t_max = cdist.reduce_totals(edges, t_s)
         e2e_all, e2e_t = cdist.reduce_totals(e2e_edges, e2e_ms / 1e3)
+        one_all, one_t = cdist.reduce_totals(one_edges, one_ms / 1e3)
         _, plain_t = cdist.reduce_totals(0, (plain_ms or 0.0) / 1e3)
     else:
         all_edges, t_max, e2e_all, e2e_t = float(edges), t_s, float(e2e_edges), e2e_ms / 1e3
+        one_all, one_t = float(one_edges), one_ms / 1e3
         plain_t = (plain_ms or 0.0) / 1e3
     value = all_edges / t_max
     e2e_value = e2e_all / e2e_t
@@ -778,6 +787,10 @@ def main():
                 "e2e": {"value": e2e_value, "unit": "edges/s",
                         "h2d_bytes_per_step": 4 * (seeds_a_h.size + seeds_b_h.size),
                         "d2h_bytes_per_step": int(12 * e2e_edges / e2e_steps)},
+                "e2e_detail": {"host_parts": "by output size (one sample range per job here; edges copied back after every hop)",
+                               "no_overlap_value": one_all / one_t,
+                               "note": "no_overlap_value: the same calls with every host job's edges "
+                                       "copied back after all of its sampling (CSAW_OPT_HOST_PARTS -1)"},
                 "gpu_launches": int(launches), "clocks": clk, "roofline": roofline,
                 "kernels": {k: v for k, v in kstats.items() if v["launches"]},
                 "profiled_pass_ms_per_step": prof_ms / args.steps,

@@ -32,6 +32,7 @@ OPT_CUDA_GRAPHS = 1
 OPT_SCHED_RECORD = 2
 OPT_GRID_PCT = 3
 OPT_PAIR = 4
+OPT_HOST_PARTS = 5
 MLP_NPARAM, MLP_NORM = 1542, 18
 
 

@@ -17,6 +17,7 @@
 #include <array>
 #include <map>
 #include <set>
+#include <thread>
 #include <vector>
 
 #include "csaw.h"
@@ -108,6 +109,8 @@ int ensure(DevBuf &b, size_t bytes, cudaStream_t st = nullptr) {
 constexpr int64_t QUEUE_ITEM_BUDGET = 32ll << 20;   // items per ping-pong queue
 constexpr int64_t SCRATCH_BUDGET = 4ll << 30;        // bytes of high-degree scratch (CTA prefix rebuilds)
 constexpr int MDRW_MAX_F = 4096;
+constexpr int MAX_HOST_PARTS = 8;                   // parts of a host-buffer job (copy-out pipelining)
+constexpr int MAX_POSTS = 64;                       // edge-count posts of a host-buffer job
 
 // Per-job device state: counters, frontier queues, work lists and scratch.
 // Job 0 serves csaw_sample; csaw_sample_batch runs job i on context i, each
@@ -121,6 +124,16 @@ struct JobCtx {
     cudaEvent_t fork = nullptr, join = nullptr;
     cudaEvent_t t0 = nullptr, t1 = nullptr;   // timed learned-schedule trial runs
     int trial_arm = -1;                       // arm this job ran under, or -1
+    // Host-buffer jobs run as n_parts consecutive sample ranges appended to
+    // one output.  While `posting`, the running edge count is posted to the
+    // next of the page-locked slots `posts` after every hop and every part
+    // (edges below a posted count are final), and the host copies them back
+    // on the copy stream while the job still samples.
+    int n_parts = 1;
+    bool posting = false;
+    int n_posts = 0;
+    cudaStream_t copy = nullptr;
+    unsigned long long *posts = nullptr;
 };
 
 }  // namespace
@@ -139,6 +152,7 @@ struct csaw_graph_s {
     bool cdf_off = false;         // CSAW_GRAPH_NO_CDF_CACHE
     int grid_pct = 100;           // CSAW_OPT_GRID_PCT
     bool pair = true;             // CSAW_OPT_PAIR
+    int host_parts = 0;           // CSAW_OPT_HOST_PARTS (0: by output size; -1: copy after the job)
     uint32_t class_mask = 0x3f;   // classes the trained model picks (bit c)
     int32_t *big_verts = nullptr; // vertices above CDF_BIG (the cache builds them one CTA each)
     int64_t n_big = 0;
@@ -406,6 +420,23 @@ int check_params(const csaw_graph_s *g, const csaw_params *p, int fan[CSAW_MAX_D
     return 0;
 }
 
+constexpr unsigned long long POST_PENDING = ~0ull;
+
+// Publishes the running edge count to page-locked host memory (the host
+// polls it; written after the kernels before it in stream order, so the
+// edges below it are complete).
+__global__ void k_post_count(const unsigned long long *count, unsigned long long *host_slot) {
+    *(volatile unsigned long long *)host_slot = *count;
+    __threadfence_system();
+}
+
+// Posts c's running edge count to its next slot (host-buffer jobs only).
+void post_count(csaw_graph_s *g, JobCtx *c, cudaStream_t st) {
+    if (!c->posting || c->n_posts >= MAX_POSTS) return;
+    LaunchScope ls(g, KK_INIT, st);
+    k_post_count<<<1, 1, 0, st>>>(&c->ctr->out_count, &c->posts[c->n_posts++]);
+}
+
 template <typename I, int BIAS>
 int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int fan[], const int32_t *seeds,
                    const OutArgs &o, cudaStream_t st) {
@@ -656,6 +687,7 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
             }
             if (side) CK(cudaStreamWaitEvent(st, c->join, 0));
             if (dedup && l + 1 < D) TRY(dedup_level(nxt, l + 1));
+            if (l + 1 < D) post_count(g, c, st);   // this hop's edges are final
         }
     }
     CK(cudaGetLastError());
@@ -780,6 +812,8 @@ int dispatch_bias(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int fa
 #undef CSAW_MODES
 }
 
+void free_job(JobCtx *c);
+
 int new_job(JobCtx **out, bool own_stream) {
     auto *c = new JobCtx();
     cudaError_t e = cudaMalloc((void **)&c->ctr, sizeof(Counters));
@@ -789,11 +823,11 @@ int new_job(JobCtx **out, bool own_stream) {
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&c->posts, sizeof(unsigned long long) * MAX_POSTS);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        cudaFree(c->ctr);
-        if (c->hctr) cudaFreeHost(c->hctr);
-        delete c;
+        free_job(c);
         return fail(CSAW_ERR_NOMEM, std::string("job context: ") + cudaGetErrorString(e));
     }
     *out = c;
@@ -802,6 +836,8 @@ int new_job(JobCtx **out, bool own_stream) {
 
 void free_job(JobCtx *c) {
     if (!c) return;
+    if (c->copy) cudaStreamDestroy(c->copy);
+    if (c->posts) cudaFreeHost(c->posts);
     for (auto &qq : c->q)
         for (auto &b : qq) cudaFree(b.p);
     for (DevBuf *b : {&c->heavy, &c->sel, &c->hlist, &c->hscratch, &c->wscratch, &c->seeds_in, &c->out_dev, &c->cta[0],
@@ -841,14 +877,16 @@ int get_job(csaw_graph_s *g, size_t i, JobCtx **out) {
 
 // Enqueues one job on `st` (no host synchronisation): counter reset, the
 // mode's kernels, and the asynchronous read-back of the counter block.
+// reset = false appends to the previous job's output and counters (the
+// later parts of a host-buffer job).
 int enqueue_job(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int32_t *seeds, int32_t *src,
-                int32_t *dst, int32_t *smp, int32_t *dep, int64_t cap, cudaStream_t st) {
+                int32_t *dst, int32_t *smp, int32_t *dep, int64_t cap, cudaStream_t st, bool reset = true) {
     int fan[CSAW_MAX_DEPTH];
     TRY(check_params(g, p, fan));
     if (cap < 0) return fail(CSAW_ERR_INVALID, "capacity < 0");
     if (cap > 0 && (!src || !dst)) return fail(CSAW_ERR_INVALID, "out_src/out_dst are NULL");
     if (p->n_samples > 0 && !seeds) return fail(CSAW_ERR_INVALID, "seeds is NULL");
-    CK(cudaMemsetAsync(c->ctr, 0, sizeof(Counters), st));
+    if (reset) CK(cudaMemsetAsync(c->ctr, 0, sizeof(Counters), st));
     OutArgs o{src, dst, smp, dep, &c->ctr->out_count, cap};
     c->trial_arm = -1;
     const bool timed = g->trial && p->schedule == CSAW_SCHED_LEARNED && p->mode == CSAW_MODE_NEIGHBOR &&
@@ -1206,13 +1244,39 @@ extern "C" int csaw_sample(csaw_graph g, const csaw_params *p, const int32_t *se
     return finish_job(g, c, capacity, n_out);
 }
 
-// Host-buffer job on context c: seeds staged in, outputs staged out.
-static int enqueue_host_job(csaw_graph_s *g, JobCtx *c, csaw_job *j, cudaStream_t st, int32_t **dev_out) {
+// Parts a host-buffer job runs in: with P > 1 the output copy of part k
+// overlaps the sampling of parts k+1.. (hop posts already overlap the copy
+// of a hop's edges with the later hops; parts add overlap for single-kernel
+// walks and for the last hop).  A part costs the job's fixed per-kernel
+// latency again, so by default 4 parts only when the job can emit at least
+// 4 MB of (src, dst) and each part stays throughput-bound (16384 samples;
+// walks: 256 per SM), else 1.  Never during a timed scheduler trial.
+static int host_parts(const csaw_graph_s *g, const csaw_params *p, int64_t cap) {
+    const int64_t S = p->n_samples;
+    if (g->trial || S < 2 || p->depth < 1) return 1;
+    int P = g->host_parts;
+    if (P < 0) return 1;
+    if (P == 0) {
+        int64_t bound = 0, ns = 0;
+        if (csaw_host_edge_bound((csaw_graph)g, p, &bound, &ns)) return 1;
+        const int64_t min_part = p->mode == CSAW_MODE_WALK ? 256ll * g->sm_count : 16384;
+        P = std::min(bound, cap) >= (512ll << 10) ? 4 : 1;
+        while (P > 1 && S / P < min_part) --P;
+    }
+    return (int)std::max<int64_t>(1, std::min<int64_t>(P, S));
+}
+
+// Host-buffer job, before its kernels (never inside a graph capture): the
+// device seeds and output buffers, the seeds copied in on `st`, the part
+// count and the pending markers the parts overwrite.
+static int prepare_host_job(csaw_graph_s *g, JobCtx *c, csaw_job *j, cudaStream_t st, int32_t **dev_out) {
     const csaw_params *p = j->params;
-    if (!p) return fail(CSAW_ERR_INVALID, "params is NULL");
     const int64_t cap = j->capacity;
     if (cap < 0) return fail(CSAW_ERR_INVALID, "capacity < 0");
     const int64_t ns = seed_count(p);
+    if (ns < 0) return fail(CSAW_ERR_INVALID, "n_samples < 0");
+    if (ns > 0 && !j->seeds) return fail(CSAW_ERR_INVALID, "seeds is NULL");
+    if (cap > 0 && (!j->out_src || !j->out_dst)) return fail(CSAW_ERR_INVALID, "out_src/out_dst are NULL");
     TRY(ensure(c->seeds_in, sizeof(int32_t) * (size_t)(ns > 0 ? ns : 1), st));
     const int narr = 2 + (j->out_sample != nullptr) + (j->out_depth != nullptr);
     TRY(ensure(c->out_dev, sizeof(int32_t) * (size_t)(cap > 0 ? cap : 1) * narr, st));
@@ -1224,32 +1288,88 @@ static int enqueue_host_job(csaw_graph_s *g, JobCtx *c, csaw_job *j, cudaStream_
     dev_out[1] = d_dst;
     dev_out[2] = d_smp;
     dev_out[3] = d_dep;
-    return enqueue_job(g, c, p, (const int32_t *)c->seeds_in.p, d_src, d_dst, d_smp, d_dep, cap, st);
-}
-
-// Copies a finished host-buffer job's edges back (n edges per array).
-static int copy_back(csaw_job *j, int32_t *const *dev_out, int64_t n, cudaStream_t st) {
-    const size_t nb = sizeof(int32_t) * (size_t)n;
-    if (!nb) return 0;
-    CK(cudaMemcpyAsync(j->out_src, dev_out[0], nb, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(j->out_dst, dev_out[1], nb, cudaMemcpyDeviceToHost, st));
-    if (j->out_sample) CK(cudaMemcpyAsync(j->out_sample, dev_out[2], nb, cudaMemcpyDeviceToHost, st));
-    if (j->out_depth) CK(cudaMemcpyAsync(j->out_depth, dev_out[3], nb, cudaMemcpyDeviceToHost, st));
+    c->n_parts = host_parts(g, p, cap);
+    for (int k = 0; k < MAX_POSTS; ++k) c->posts[k] = POST_PENDING;
     return 0;
 }
 
-extern "C" int csaw_sample_host(csaw_graph g, const csaw_params *p, const int32_t *seeds,
-                                int32_t *out_src, int32_t *out_dst, int32_t *out_sample,
-                                int32_t *out_depth, int64_t capacity, int64_t *n_out, void *stream) {
-    if (!g || !p || !n_out) return fail(CSAW_ERR_INVALID, "NULL argument");
-    csaw_job j{p, seeds, out_src, out_dst, out_sample, out_depth, capacity, 0, 0, 1};
-    int rc = csaw_sample_batch(g, &j, 1, stream);
-    *n_out = j.n_out;
-    return rc;
+// The prepared host-buffer job's kernels on `st` (capturable): its parts,
+// consecutive sample ranges appended to one output (sample ids, and so
+// every draw, as in one run), posting the edge count after every hop and
+// every part.
+static int enqueue_host_parts(csaw_graph_s *g, JobCtx *c, const csaw_job *j, cudaStream_t st,
+                              int32_t *const *dev_out) {
+    const csaw_params *p = j->params;
+    const int P = c->n_parts;
+    const int64_t S = p->n_samples, per_sample = p->mode == CSAW_MODE_WALK ? 1 : p->frontier_size;
+    const int32_t *seeds = (const int32_t *)c->seeds_in.p;
+    c->posting = g->host_parts >= 0;
+    c->n_posts = 0;
+    int rc = 0;
+    for (int k = 0; k < P && !rc; ++k) {
+        csaw_params q = *p;
+        const int64_t s0 = S * k / P, s1 = S * (k + 1) / P;
+        if (P > 1) {
+            q.n_samples = (int32_t)(s1 - s0);
+            q.sample_base = p->sample_base + s0;
+        }
+        rc = enqueue_job(g, c, &q, seeds + s0 * per_sample, dev_out[0], dev_out[1], dev_out[2], dev_out[3],
+                         j->capacity, st, k == 0);
+        if (!rc) post_count(g, c, st);
+    }
+    c->posting = false;
+    if (rc) return rc;
+    CK(cudaGetLastError());
+    return 0;
+}
+
+// Copies edges [lo, hi) of a host-buffer job's output back.
+static int copy_range(csaw_job *j, int32_t *const *dev_out, int64_t lo, int64_t hi, cudaStream_t st) {
+    if (hi <= lo) return 0;
+    const size_t nb = sizeof(int32_t) * (size_t)(hi - lo);
+    CK(cudaMemcpyAsync(j->out_src + lo, dev_out[0] + lo, nb, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(j->out_dst + lo, dev_out[1] + lo, nb, cudaMemcpyDeviceToHost, st));
+    if (j->out_sample) CK(cudaMemcpyAsync(j->out_sample + lo, dev_out[2] + lo, nb, cudaMemcpyDeviceToHost, st));
+    if (j->out_depth) CK(cudaMemcpyAsync(j->out_depth + lo, dev_out[3] + lo, nb, cudaMemcpyDeviceToHost, st));
+    return 0;
+}
+
+// While the batch runs: as a host-buffer job posts edge counts (in slot
+// order), copies the edges up to each (clipped to the capacity) back on the
+// job's copy stream, so the copy overlaps the sampling still running.
+// Returns once `st` (which joins all jobs) has finished or failed and the
+// posts made by then are taken.  copied[i]: edges of job i on their way.
+static void pipe_copies(csaw_job *jobs, int n_jobs, const std::vector<JobCtx *> &ctx,
+                        const std::vector<std::array<int32_t *, 4>> &dev_out, cudaStream_t st,
+                        std::vector<int64_t> &copied) {
+    std::vector<int> next((size_t)n_jobs, 0);
+    bool st_done = false;
+    for (;;) {
+        bool waiting = false;
+        for (int i = 0; i < n_jobs; ++i) {
+            JobCtx *c = ctx[i];
+            csaw_job &j = jobs[i];
+            if (!c || j.status || !j.host_buffers) continue;
+            while (next[i] < MAX_POSTS) {
+                const unsigned long long v = *(volatile unsigned long long *)&c->posts[next[i]];
+                if (v == POST_PENDING) {
+                    waiting = true;
+                    break;
+                }
+                const int64_t hi = std::min<int64_t>((int64_t)v, j.capacity);
+                if (hi > copied[i] && copy_range(&j, dev_out[i].data(), copied[i], hi, c->copy) == 0) copied[i] = hi;
+                ++next[i];
+            }
+        }
+        if (!waiting || st_done) return;
+        // all posted counts are in host memory once st has finished
+        st_done = cudaStreamQuery(st) != cudaErrorNotReady;
+        if (!st_done) std::this_thread::yield();
+    }
 }
 
 // Forks the jobs from `st` onto their context streams, enqueues them and
-// joins them back into `st`.
+// joins them back into `st`.  Host-buffer jobs are already prepared.
 static int enqueue_batch(csaw_graph_s *g, csaw_job *jobs, int n_jobs, cudaStream_t st, std::vector<JobCtx *> &ctx,
                          std::vector<std::array<int32_t *, 4>> &dev_out) {
     JobCtx *c0 = g->jobs[0];
@@ -1257,11 +1377,12 @@ static int enqueue_batch(csaw_graph_s *g, csaw_job *jobs, int n_jobs, cudaStream
     int first_rc = 0;
     for (int i = 0; i < n_jobs; ++i) {
         csaw_job &j = jobs[i];
+        if (j.status) continue;   // preparation failed
         int rc = get_job(g, (size_t)i + 1, &ctx[i]);
         if (!rc) rc = cudaStreamWaitEvent(ctx[i]->stream, c0->done, 0) == cudaSuccess ? 0 :
                       fail(CSAW_ERR_CUDA, "cudaStreamWaitEvent failed");
         if (!rc) {
-            if (j.host_buffers) rc = enqueue_host_job(g, ctx[i], &j, ctx[i]->stream, dev_out[i].data());
+            if (j.host_buffers) rc = enqueue_host_parts(g, ctx[i], &j, ctx[i]->stream, dev_out[i].data());
             else rc = enqueue_job(g, ctx[i], j.params, j.seeds, j.out_src, j.out_dst, j.out_sample, j.out_depth,
                                   j.capacity, ctx[i]->stream);
         }
@@ -1276,13 +1397,18 @@ static int enqueue_batch(csaw_graph_s *g, csaw_job *jobs, int n_jobs, cudaStream
     return first_rc;
 }
 
-static std::string batch_key(const csaw_job *jobs, int n_jobs) {
+static std::string batch_key(const csaw_graph_s *g, const csaw_job *jobs, int n_jobs) {
     std::string k;
     for (int i = 0; i < n_jobs; ++i) {
         const csaw_job &j = jobs[i];
         k.append((const char *)j.params, sizeof(csaw_params));
-        const void *ptrs[6] = {j.seeds, j.out_src, j.out_dst, j.out_sample, j.out_depth, (const void *)(intptr_t)j.capacity};
+        const void *ptrs[7] = {j.seeds, j.out_src, j.out_dst, j.out_sample, j.out_depth,
+                               (const void *)(intptr_t)j.capacity, (const void *)(intptr_t)j.host_buffers};
         k.append((const char *)ptrs, sizeof(ptrs));
+        if (j.host_buffers) {   // the parts' layout is part of the graph
+            const int P = g->host_parts < 0 ? -1 : g->jobs.size() > (size_t)i + 1 ? g->jobs[(size_t)i + 1]->n_parts : 0;
+            k.append((const char *)&P, sizeof(P));
+        }
     }
     return k;
 }
@@ -1298,8 +1424,29 @@ extern "C" int csaw_sample_batch(csaw_graph g, csaw_job *jobs, int n_jobs, void 
     reset_last(g);
     std::vector<JobCtx *> ctx((size_t)n_jobs);
     std::vector<std::array<int32_t *, 4>> dev_out((size_t)n_jobs);
+    for (int i = 0; i < n_jobs; ++i) {
+        jobs[i].n_out = 0;
+        jobs[i].status = 0;
+    }
+    int first_rc = 0;
+    std::string first_msg;
     bool graphable = g->use_graphs && !g->prof && !g->trial;   // trial runs are timed one by one
-    for (int i = 0; i < n_jobs && graphable; ++i) graphable = !jobs[i].host_buffers;
+    // host-buffer jobs: seeds in and buffers sized before anything is launched
+    // or captured (the copies in and out stay outside any graph)
+    for (int i = 0; i < n_jobs; ++i) {
+        csaw_job &j = jobs[i];
+        if (!j.host_buffers) continue;
+        int rc = get_job(g, (size_t)i + 1, &ctx[i]);
+        if (!rc) rc = prepare_host_job(g, ctx[i], &j, st, dev_out[i].data());
+        if (rc) {
+            j.status = rc;
+            graphable = false;
+            if (!first_rc) {
+                first_rc = rc;
+                first_msg = g_err;
+            }
+        }
+    }
     if (g->graph_epoch != g_alloc_epoch) {   // workspace moved: cached graphs are stale
         for (auto &kv : g->graphs) cudaGraphExecDestroy(kv.second);
         g->graphs.clear();
@@ -1307,12 +1454,7 @@ extern "C" int csaw_sample_batch(csaw_graph g, csaw_job *jobs, int n_jobs, void 
         g->warm.clear();
         g->graph_epoch = g_alloc_epoch;
     }
-    std::string key = graphable ? batch_key(jobs, n_jobs) : std::string();
-    for (int i = 0; i < n_jobs; ++i) {
-        jobs[i].n_out = 0;
-        jobs[i].status = 0;
-    }
-    int first_rc = 0;
+    std::string key = graphable ? batch_key(g, jobs, n_jobs) : std::string();
     bool launched = false;
     if (graphable) {
         auto it = g->graphs.find(key);
@@ -1352,17 +1494,26 @@ extern "C" int csaw_sample_batch(csaw_graph g, csaw_job *jobs, int n_jobs, void 
             launched = true;
         }
     }
-    if (!launched) first_rc = enqueue_batch(g, jobs, n_jobs, st, ctx, dev_out);
+    if (!launched) {
+        // a capture that was not kept left nothing queued: run eagerly
+        if (graphable)
+            for (int i = 0; i < n_jobs; ++i) jobs[i].status = 0;   // no preparation failed
+        int rc = enqueue_batch(g, jobs, n_jobs, st, ctx, dev_out);
+        if (rc && !first_rc) {
+            first_rc = rc;
+            first_msg = g_err;
+        }
+    }
+    std::vector<int64_t> copied((size_t)n_jobs, 0);
+    pipe_copies(jobs, n_jobs, ctx, dev_out, st, copied);
     cudaError_t e = cudaStreamSynchronize(st);
     drain_profile(g);
     if (e != cudaSuccess) return fail(CSAW_ERR_CUDA, std::string("stream sync: ") + cudaGetErrorString(e));
-    std::string first_msg;
-    if (first_rc) first_msg = g_err;
     for (int i = 0; i < n_jobs; ++i) {
         csaw_job &j = jobs[i];
         if (j.status) continue;
         int rc = finish_job(g, ctx[i], j.capacity, &j.n_out);
-        if (!rc && j.host_buffers) rc = copy_back(&j, dev_out[i].data(), j.n_out, ctx[i]->stream);
+        if (!rc && j.host_buffers) rc = copy_range(&j, dev_out[i].data(), copied[i], j.n_out, ctx[i]->copy);
         j.status = rc;
         if (rc && !first_rc) {
             first_rc = rc;
@@ -1370,13 +1521,23 @@ extern "C" int csaw_sample_batch(csaw_graph g, csaw_job *jobs, int n_jobs, void 
         }
     }
     for (int i = 0; i < n_jobs; ++i)
-        if (jobs[i].host_buffers && ctx[i]) CK(cudaStreamSynchronize(ctx[i]->stream));
+        if (jobs[i].host_buffers && ctx[i]) CK(cudaStreamSynchronize(ctx[i]->copy));
     if (first_rc) {
         g_err = first_msg;
     } else if (graphable && !launched) {
         g->warm.insert(key);
     }
     return first_rc;
+}
+
+extern "C" int csaw_sample_host(csaw_graph g, const csaw_params *p, const int32_t *seeds,
+                                int32_t *out_src, int32_t *out_dst, int32_t *out_sample,
+                                int32_t *out_depth, int64_t capacity, int64_t *n_out, void *stream) {
+    if (!g || !p || !n_out) return fail(CSAW_ERR_INVALID, "NULL argument");
+    csaw_job j{p, seeds, out_src, out_dst, out_sample, out_depth, capacity, 0, 0, 1};
+    int rc = csaw_sample_batch(g, &j, 1, stream);
+    *n_out = j.n_out;
+    return rc;
 }
 
 static int ensure_mlp(csaw_graph_s *g) {
@@ -1423,6 +1584,10 @@ extern "C" int csaw_graph_set_option(csaw_graph g, int option, int64_t value) {
         case CSAW_OPT_PAIR:
             g->pair = value != 0;
             ++g_alloc_epoch;
+            return 0;
+        case CSAW_OPT_HOST_PARTS:
+            if (value < -1 || value > MAX_HOST_PARTS) return fail(CSAW_ERR_INVALID, "host parts must be in [-1, 8]");
+            g->host_parts = (int)value;
             return 0;
         default:
             return fail(CSAW_ERR_INVALID, "unknown option");

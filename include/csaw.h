@@ -161,7 +161,9 @@ int csaw_sample(csaw_graph g, const csaw_params *p, const int32_t *seeds,
                 int32_t *out_src, int32_t *out_dst, int32_t *out_sample,
                 int32_t *out_depth, int64_t capacity, int64_t *n_out, void *stream);
 
-/* Same, with HOST seeds and HOST outputs (copies inside the call). */
+/* Same, with HOST seeds and HOST outputs (copies inside the call; large
+ * jobs copy edges back while they still sample, CSAW_OPT_HOST_PARTS).  On
+ * an error the host arrays hold an unspecified part of the output. */
 int csaw_sample_host(csaw_graph g, const csaw_params *p, const int32_t *seeds,
                      int32_t *out_src, int32_t *out_dst, int32_t *out_sample,
                      int32_t *out_depth, int64_t capacity, int64_t *n_out, void *stream);
@@ -207,7 +209,15 @@ enum {
     CSAW_OPT_GRID_PCT = 3,
     /* ... and whether cached items with N <= 16 run two per warp (1, the
      * default) or one per warp (0). */
-    CSAW_OPT_PAIR = 4
+    CSAW_OPT_PAIR = 4,
+    /* Host-buffer jobs (csaw_sample_host, host_buffers != 0) copy edges
+     * back while they still sample: the edges of every finished hop, and of
+     * every finished part when the job runs as P consecutive sample ranges
+     * (1..8); 0 (default): 4 ranges when the job can emit at least 512 Ki
+     * edges and each range has 16384 samples (walks: 256 per SM), else 1;
+     * -1: one range, copied back after all of its sampling.  Never changes
+     * the edge multiset. */
+    CSAW_OPT_HOST_PARTS = 5
 };
 int csaw_graph_set_option(csaw_graph g, int option, int64_t value);
 
