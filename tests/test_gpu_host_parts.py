@@ -1,8 +1,9 @@
-"""GPU tests of multi-part host-buffer jobs (CSAW_OPT_HOST_PARTS): a job run
-as P consecutive sample ranges, each range's edges copied back while the
-later ranges still sample, gives exactly the edges of the one-range run and
-of the oracle, for all three modes, ragged splits, page-locked and pageable
-outputs, alone and in a batch; a capacity below the output still fails."""
+"""GPU tests of host-buffer jobs that copy edges back while they sample
+(CSAW_OPT_HOST_PARTS): a job run as P consecutive sample ranges, its edges
+posted after every hop and range, gives exactly the edges of the one-range
+run and of the oracle, for all three modes and schedules, ragged splits,
+page-locked and pageable outputs, alone and in a batch (eager, captured,
+replayed); a capacity below the output still fails."""
 import numpy as np
 import pytest
 
@@ -42,7 +43,7 @@ def seeds_for(g, case, shift=0):
     return oracle.make_seeds(g.rowptr, n * (1 if mode == 1 else F), 7 + shift)
 
 
-@pytest.mark.parametrize("sched", [0, 1])
+@pytest.mark.parametrize("sched", [0, 1, 2])
 def test_parts_equal_one_part_and_oracle(csaw, rmat12_pareto, sched):
     import torch
     from csaw import _lib
