@@ -109,6 +109,13 @@ struct LevelArgs {
     int32_t *out_dep;
     int D;
     uint8_t fan[CSAW_MAX_DEPTH];
+    // Streaming, one launch over all pending items: per partition (vertex >>
+    // pbits) the column and weight bases re-based so that col[e] is edge e,
+    // or a null column base when the partition is not sampled this round
+    // (its items stay pending).
+    const int32_t *const *part_col;
+    const float *const *part_w;
+    int pbits;
 };
 
 // Level of input item `it`: depth, fanout, whether its children are pushed.

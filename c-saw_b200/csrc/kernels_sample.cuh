@@ -119,10 +119,12 @@ __device__ __forceinline__ int select_warp(const DevGraph &g, int64_t beg, int64
 
 // ----------------------------------------------------- level expansion
 // One warp per queue item (grid-stride, persistent grid).  Biased items whose
-// degree exceeds WBUF are deferred to k_expand_heavy.
-template <typename I, int BIAS>
+// degree exceeds WBUF are deferred to k_expand_heavy.  STREAM: each item
+// reads the adjacency of its own partition (LevelArgs::part_col/part_w) and
+// items of partitions not sampled this round are skipped.
+template <typename I, int BIAS, bool STREAM = false>
 __global__ void __launch_bounds__(EXPAND_THREADS)
-k_expand_warp(DevGraph g, LevelArgs a) {
+k_expand_warp(DevGraph g0, LevelArgs a) {
     constexpr bool BIASED = BIAS != CSAW_BIAS_UNBIASED;
     constexpr int NW = EXPAND_THREADS / 32;
     __shared__ float s_P[BIASED ? NW * WBUF : 1];
@@ -146,6 +148,13 @@ k_expand_warp(DevGraph g, LevelArgs a) {
     for (uint32_t it = gw; it < n; it += nw) {
         const int32_t v = a.in_v[it];
         if (v < 0) continue;   // dropped by per-sample dedup
+        DevGraph g = g0;
+        if (STREAM) {
+            const int part = v >> a.pbits;
+            g.v.col = a.part_col[part];
+            if (!g.v.col) continue;   // partition not resident this round
+            g.v.weight = a.part_w[part];
+        }
         int l, N;
         bool push;
         item_level(a, it, l, N, push);
@@ -216,9 +225,9 @@ k_expand_warp(DevGraph g, LevelArgs a) {
 // One CTA per deferred item: the canonical prefix is built by the whole CTA in
 // global scratch (same canonical order, so bit-identical to the warp path);
 // warp 0 runs the slot resolver; every rebuild is a CTA-wide rescan.
-template <typename I, int BIAS>
+template <typename I, int BIAS, bool STREAM = false>
 __global__ void __launch_bounds__(1024)
-k_expand_heavy(DevGraph g, LevelArgs a) {
+k_expand_heavy(DevGraph g0, LevelArgs a) {
     __shared__ int s_flag, s_j;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float *P = a.heavy_scratch + (int64_t)blockIdx.x * a.heavy_stride;
@@ -233,6 +242,12 @@ k_expand_heavy(DevGraph g, LevelArgs a) {
         long long t0 = 0;
         if (rec && threadIdx.x == 0) t0 = clock64();
         const int32_t v = a.in_v[it];
+        DevGraph g = g0;
+        if (STREAM) {   // deferred by the warp pass, so its partition is resident
+            const int part = v >> a.pbits;
+            g.v.col = a.part_col[part];
+            g.v.weight = a.part_w[part];
+        }
         const int32_t s = a.in_s[it];
         const uint32_t p = a.in_p[it];
         const int64_t beg = row_begin<I>(g, v);

@@ -25,11 +25,12 @@
 //   - copies run on a copy stream; each partition has a ready event (copy
 //     done) and a free event (last kernel using it done), so an eviction
 //     waits only for that partition's kernels;
-//   - the expansion kernel runs once per resident partition on all of its
-//     pending items, whatever their depths (each item carries its depth;
-//     its fanout and whether it pushes children follow from it), with the
-//     column/weight pointers re-based onto the partition's region, so col[e]
-//     of any edge of the partition is read from HBM;
+//   - the expansion kernel runs once per round over all pending items,
+//     whatever their depths (each item carries its depth; its fanout and
+//     whether it pushes children follow from it): each item reads the
+//     column/weight bases of its partition from a per-round table (re-based
+//     onto the partition's region, so col[e] of any edge of the partition is
+//     read from HBM), and items of partitions not in the round are skipped;
 //   - walks are neighbor sampling with N = 1 (same keys, same output).
 // Because every draw is keyed by (sample, depth, lineage, slot, draw), the
 // output equals the in-memory output exactly, whatever the processing order.
@@ -165,7 +166,7 @@ struct csaw_stream_graph_s {
     std::vector<int> resident;        // resident partitions, in load order
     std::vector<cudaEvent_t> ready, freed;   // per partition, created on first load
     cudaStream_t copy = nullptr;
-    Buf q[3][4], counts, offsets, cursor, heavy, hscratch, ctr, skip, pcount;
+    Buf q[3][4], counts, offsets, cursor, heavy, hscratch, ctr, skip, ptab;
     StreamCounters *hctr = nullptr;
     int64_t loads = 0, hits = 0, bytes_h2d = 0, launches = 0;
 };
@@ -314,7 +315,7 @@ int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], co
     STRY(grow(g->offsets, sizeof(uint32_t) * (size_t)(nbins + 1)));
     STRY(grow(g->ctr, sizeof(StreamCounters)));
     STRY(grow(g->skip, (size_t)g->npart));
-    STRY(grow(g->pcount, sizeof(uint32_t) * (size_t)g->npart));
+    STRY(grow(g->ptab, sizeof(void *) * 2 * (size_t)g->npart));
     int hblocks = 0;
     int64_t hstride = 0;
     if (BIASED && g->maxdeg > WBUF) {
@@ -360,12 +361,12 @@ int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], co
     g->launches++;
     STRY(rebin(false));
     int grid = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid, k_expand_warp<I, BIAS>, EXPAND_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid, k_expand_warp<I, BIAS, true>, EXPAND_THREADS, 0);
     grid = (grid > 0 ? grid : 1) * g->sm_count;
     std::vector<uint32_t> h_counts((size_t)nbins);
     std::vector<int64_t> h_off((size_t)nbins + 1), pend((size_t)g->npart);
     std::vector<uint8_t> h_skip((size_t)g->npart);
-    std::vector<uint32_t> h_pc((size_t)g->npart);
+    std::vector<const void *> h_tab(2 * (size_t)g->npart);
     std::vector<char> visited((size_t)g->npart, 0), in_round((size_t)g->npart, 0);
     for (;;) {
         SCK(cudaMemcpyAsync(h_counts.data(), d_counts, sizeof(uint32_t) * (size_t)nbins, cudaMemcpyDeviceToHost, st));
@@ -407,28 +408,33 @@ int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], co
             }
             if (round.empty()) return csaw_host_fail(CSAW_ERR_INVALID, "no partition fits the device budget");
         }
-        for (int q = 0; q < g->npart; ++q) h_pc[q] = (uint32_t)pend[q];
-        SCK(cudaMemcpyAsync(g->pcount.p, h_pc.data(), sizeof(uint32_t) * (size_t)g->npart, cudaMemcpyHostToDevice,
-                            st));
+        // one launch over all pending items: the round's partitions in the
+        // table, every other partition's items skipped (they stay pending)
         std::fill(h_skip.begin(), h_skip.end(), 0);
+        std::fill(h_tab.begin(), h_tab.end(), nullptr);
         for (int part : round) {
             SCK(cudaStreamWaitEvent(st, g->ready[part], 0));
             h_skip[part] = 1;
             unsigned char *base = g->arena + g->res_off[part];
+            h_tab[part] = (const int32_t *)base - g->pbeg[part];
+            if (g->res_w[part]) h_tab[g->npart + part] = (const float *)(base + g->res_bytes[part] / 2) - g->pbeg[part];
+        }
+        SCK(cudaMemcpyAsync(g->ptab.p, h_tab.data(), sizeof(void *) * h_tab.size(), cudaMemcpyHostToDevice, st));
+        {
             DevGraph dg{};
             dg.v.rowptr = g->d_rowptr;
             dg.v.rowptr_is_64 = g->idx64;
-            dg.v.col = (const int32_t *)base - g->pbeg[part];
-            dg.v.weight = g->res_w[part] ? (const float *)(base + g->res_bytes[part] / 2) - g->pbeg[part] : nullptr;
             dg.v.n_vertices = g->V;
             dg.v.n_edges = g->E;
-            const size_t key0 = (size_t)part * D;
             LevelArgs a{};
-            a.in_v = qv(A, 0) + h_off[key0];
-            a.in_s = qv(A, 1) + h_off[key0];
-            a.in_p = (const uint32_t *)qv(A, 2) + h_off[key0];
-            a.in_dep = qv(A, 3) + h_off[key0];
-            a.n_in = (const uint32_t *)g->pcount.p + part;
+            a.in_v = qv(A, 0);
+            a.in_s = qv(A, 1);
+            a.in_p = (const uint32_t *)qv(A, 2);
+            a.in_dep = qv(A, 3);
+            a.n_in = &c->n_pend;
+            a.part_col = (const int32_t *const *)g->ptab.p;
+            a.part_w = (const float *const *)((const void *const *)g->ptab.p + g->npart);
+            a.pbits = g->pbits;
             a.out_v = qv(U, 0);
             a.out_s = qv(U, 1);
             a.out_p = (uint32_t *)qv(U, 2);
@@ -452,14 +458,14 @@ int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], co
             a.D = D;
             for (int l = 0; l < D; ++l) a.fan[l] = (uint8_t)fan[l];
             if (hblocks) SCK(cudaMemsetAsync(&c->n_heavy, 0, sizeof(uint32_t), st));
-            k_expand_warp<I, BIAS><<<grid, EXPAND_THREADS, 0, st>>>(dg, a);
+            k_expand_warp<I, BIAS, true><<<grid, EXPAND_THREADS, 0, st>>>(dg, a);
             g->launches++;
             if (hblocks) {
-                k_expand_heavy<I, BIAS><<<hblocks, HEAVY_THREADS, 0, st>>>(dg, a);
+                k_expand_heavy<I, BIAS, true><<<hblocks, HEAVY_THREADS, 0, st>>>(dg, a);
                 g->launches++;
             }
-            SCK(cudaEventRecord(g->freed[part], st));
         }
+        for (int part : round) SCK(cudaEventRecord(g->freed[part], st));
         SCK(cudaMemcpyAsync(d_skip, h_skip.data(), (size_t)g->npart, cudaMemcpyHostToDevice, st));
         STRY(rebin(true));
     }
@@ -577,7 +583,7 @@ extern "C" int csaw_stream_graph_destroy(csaw_stream_graph g) {
     cudaFree(g->arena);
     for (auto &qq : g->q)
         for (auto &b : qq) cudaFree(b.p);
-    for (Buf *b : {&g->counts, &g->offsets, &g->cursor, &g->heavy, &g->hscratch, &g->ctr, &g->skip, &g->pcount})
+    for (Buf *b : {&g->counts, &g->offsets, &g->cursor, &g->heavy, &g->hscratch, &g->ctr, &g->skip, &g->ptab})
         cudaFree(b->p);
     for (auto e : g->ready)
         if (e) cudaEventDestroy(e);
