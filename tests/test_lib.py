@@ -137,3 +137,15 @@ def test_params_flags_layout():
     assert p.flags == _lib.PARAM_DEDUP
     assert _lib.Params.flags.offset == _lib.Params.sample_base.offset + 8
     assert ctypes.sizeof(_lib.Params) == _lib.Params.reserved.offset + 4
+
+
+def test_python_constants_match_header():
+    """Every CSAW_* enum value of include/csaw.h has the same value in the
+    Python binding (status codes, modes, biases, schedules, flags, options)."""
+    from csaw import _lib
+    txt = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "csaw.h")).read(), flags=re.S)
+    consts = re.findall(r"\bCSAW_(\w+)\s*=\s*(-?\d+)", txt)
+    assert len(consts) >= 20
+    for name, value in consts:
+        assert hasattr(_lib, name), name
+        assert getattr(_lib, name) == int(value), name
