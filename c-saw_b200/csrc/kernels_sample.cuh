@@ -146,7 +146,7 @@ k_expand_warp(DevGraph g0, LevelArgs a) {
     const uint32_t n = *a.n_in;
     unsigned long long my_bytes = 0, my_items = 0;
     for (uint32_t it = gw; it < n; it += nw) {
-        const int32_t v = a.in_v[it];
+        int32_t v = a.in_v[it];
         if (v < 0) continue;   // dropped by per-sample dedup
         DevGraph g = g0;
         if (STREAM) {
@@ -160,59 +160,83 @@ k_expand_warp(DevGraph g0, LevelArgs a) {
         item_level(a, it, l, N, push);
         const int32_t s = a.in_s[it];
         const uint32_t p = a.in_p[it];
-        const int64_t beg = row_begin<I>(g, v);
-        const int64_t d = row_begin<I>(g, v + 1) - beg;
-        if (d <= 0) {
-            my_items++;
-            my_bytes += 12 + 2 * sizeof(I);
-            continue;
-        }
-        if (BIASED && d > N && d > WBUF && !(g.cdf && g.cdf_bias == BIAS)) {
-            if (lane == 0) {
-                uint32_t h = atomicAdd(a.n_heavy, 1u);
-                a.heavy[h] = it;
+        // STREAM: a walk step (N = 1) whose next vertex lies in a partition of
+        // this round goes on in this warp instead of waiting for the next
+        // round (same draw keys: the child of slot 0 keeps lineage p); at
+        // most D steps
+        for (;;) {
+            const int64_t beg = row_begin<I>(g, v);
+            const int64_t d = row_begin<I>(g, v + 1) - beg;
+            if (d <= 0) {
+                my_items++;
+                my_bytes += 12 + 2 * sizeof(I);
+                break;
             }
-            continue;
-        }
-        my_items++;
-        const int k = d < N ? (int)d : N;
-        int sel = lane;
-        bool scanned = false;
-        if (d > N) {
-            scanned = BIASED && !(g.cdf && g.cdf_bias == BIAS);
-            const DrawCtx dc{a.k0, a.k1, p, (uint32_t)s, (uint32_t)l};
-            sel = select_warp<I, BIAS>(g, beg, d, N, dc, P, zb, zs, lane, WBUF);
-            if (sel == -2) {   // cached hub that needs a rebuild: the CTA path redoes it
-                my_items--;
+            if (BIASED && d > N && d > WBUF && !(g.cdf && g.cdf_bias == BIAS)) {
+                // never a continued step (those have d <= WBUF), so `it` is this item
                 if (lane == 0) {
                     uint32_t h = atomicAdd(a.n_heavy, 1u);
                     a.heavy[h] = it;
                 }
-                continue;
+                break;
             }
-        }
-        bool act = lane < k;
-        int32_t dst = 0;
-        if (act) {
-            dst = Update(&g.v, __ldg(g.v.col + beg + sel), v);
-            if (dst < 0 || dst >= g.v.n_vertices) {
-                atomicOr(a.err, ERR_UPDATE_RANGE);
-                dst = 0;
+            my_items++;
+            const int k = d < N ? (int)d : N;
+            int sel = lane;
+            bool scanned = false;
+            if (d > N) {
+                scanned = BIASED && !(g.cdf && g.cdf_bias == BIAS);
+                const DrawCtx dc{a.k0, a.k1, p, (uint32_t)s, (uint32_t)l};
+                sel = select_warp<I, BIAS>(g, beg, d, N, dc, P, zb, zs, lane, WBUF);
+                if (sel == -2) {   // cached hub that needs a rebuild: the CTA path redoes it
+                    // (only with a prefix cache, which streaming graphs do not have)
+                    my_items--;
+                    if (lane == 0) {
+                        uint32_t h = atomicAdd(a.n_heavy, 1u);
+                        a.heavy[h] = it;
+                    }
+                    break;
+                }
             }
-        }
-        stg.push(oa, act, v, dst, s, l, lane);
-        if (push) {
-            uint32_t q = 0;
-            if (lane == 0) q = atomicAdd(a.n_out, (uint32_t)k);
-            q = __shfl_sync(FULL, q, 0);
+            bool act = lane < k;
+            int32_t dst = 0;
             if (act) {
-                a.out_v[q + lane] = dst;
-                a.out_s[q + lane] = s;
-                a.out_p[q + lane] = p * (uint32_t)N + (uint32_t)lane;
-                if (a.out_dep) a.out_dep[q + lane] = l + 1;
+                dst = Update(&g.v, __ldg(g.v.col + beg + sel), v);
+                if (dst < 0 || dst >= g.v.n_vertices) {
+                    atomicOr(a.err, ERR_UPDATE_RANGE);
+                    dst = 0;
+                }
             }
+            stg.push(oa, act, v, dst, s, l, lane);
+            bool cont = false;
+            int32_t nv = 0;
+            if (STREAM && push && k == 1 && a.fan[l + 1] == 1) {
+                nv = __shfl_sync(FULL, dst, 0);
+                if (a.part_col[nv >> a.pbits]) {
+                    const int64_t nd = row_begin<I>(g, nv + 1) - row_begin<I>(g, nv);
+                    cont = !(BIASED && nd > 1 && nd > WBUF);   // the warp path can take it
+                }
+            }
+            if (push && !cont) {
+                uint32_t q = 0;
+                if (lane == 0) q = atomicAdd(a.n_out, (uint32_t)k);
+                q = __shfl_sync(FULL, q, 0);
+                if (act) {
+                    a.out_v[q + lane] = dst;
+                    a.out_s[q + lane] = s;
+                    a.out_p[q + lane] = p * (uint32_t)N + (uint32_t)lane;
+                    if (a.out_dep) a.out_dep[q + lane] = l + 1;
+                }
+            }
+            my_bytes += expansion_bytes<I, BIAS>(g, d, k, scanned, a, push && !cont);
+            if (!cont) break;
+            v = nv;
+            l += 1;
+            N = 1;
+            push = l + 1 < a.D;
+            g.v.col = a.part_col[v >> a.pbits];
+            g.v.weight = a.part_w[v >> a.pbits];
         }
-        my_bytes += expansion_bytes<I, BIAS>(g, d, k, scanned, a, push);
     }
     stg.flush(oa, lane);
     if (lane == 0) {

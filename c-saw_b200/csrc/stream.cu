@@ -31,6 +31,8 @@
 //     column/weight bases of its partition from a per-round table (re-based
 //     onto the partition's region, so col[e] of any edge of the partition is
 //     read from HBM), and items of partitions not in the round are skipped;
+//     a walk step whose next vertex is in a partition of the round goes on
+//     in the same warp;
 //   - walks are neighbor sampling with N = 1 (same keys, same output).
 // Because every draw is keyed by (sample, depth, lineage, slot, draw), the
 // output equals the in-memory output exactly, whatever the processing order.
