@@ -111,6 +111,8 @@ constexpr int64_t SCRATCH_BUDGET = 4ll << 30;        // bytes of high-degree scr
 constexpr int MDRW_MAX_F = 4096;
 constexpr int MAX_HOST_PARTS = 8;                   // parts of a host-buffer job (copy-out pipelining)
 constexpr int MAX_POSTS = 64;                       // edge-count posts of a host-buffer job
+constexpr size_t MAX_GRAPHS = 64;                   // cached CUDA graphs per graph handle
+constexpr size_t MAX_WARM = 1024;                   // batch keys remembered for capture
 
 // Per-job device state: counters, frontier queues, work lists and scratch.
 // Job 0 serves csaw_sample; csaw_sample_batch runs job i on context i, each
@@ -1459,6 +1461,12 @@ extern "C" int csaw_sample_batch(csaw_graph g, csaw_job *jobs, int n_jobs, void 
     if (graphable) {
         auto it = g->graphs.find(key);
         if (it == g->graphs.end() && g->warm.count(key)) {
+            if (g->graphs.size() >= MAX_GRAPHS) {   // callers cycling through many buffers: start over
+                for (auto &kv : g->graphs) cudaGraphExecDestroy(kv.second);
+                g->graphs.clear();
+                g->graph_kernels.clear();
+                it = g->graphs.end();
+            }
             cudaGraph_t graph = nullptr;
             cudaGraphExec_t exec = nullptr;
             if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
@@ -1508,7 +1516,11 @@ extern "C" int csaw_sample_batch(csaw_graph g, csaw_job *jobs, int n_jobs, void 
     pipe_copies(jobs, n_jobs, ctx, dev_out, st, copied);
     cudaError_t e = cudaStreamSynchronize(st);
     drain_profile(g);
-    if (e != cudaSuccess) return fail(CSAW_ERR_CUDA, std::string("stream sync: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) {
+        for (int i = 0; i < n_jobs; ++i)   // no copy into the caller's buffers outlives the call
+            if (jobs[i].host_buffers && ctx[i]) cudaStreamSynchronize(ctx[i]->copy);
+        return fail(CSAW_ERR_CUDA, std::string("stream sync: ") + cudaGetErrorString(e));
+    }
     for (int i = 0; i < n_jobs; ++i) {
         csaw_job &j = jobs[i];
         if (j.status) continue;
@@ -1525,6 +1537,7 @@ extern "C" int csaw_sample_batch(csaw_graph g, csaw_job *jobs, int n_jobs, void 
     if (first_rc) {
         g_err = first_msg;
     } else if (graphable && !launched) {
+        if (g->warm.size() >= MAX_WARM) g->warm.clear();   // keys of batches seen once
         g->warm.insert(key);
     }
     return first_rc;
