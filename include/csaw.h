@@ -194,10 +194,12 @@ int csaw_sample_batch(csaw_graph g, csaw_job *jobs, int n_jobs, void *stream);
 
 /* Graph options. */
 enum {
-    /* 1 (default): a batch of device-buffer jobs seen before with the same
-     * parameters and buffers is captured once into a CUDA graph and replayed
-     * as one launch afterwards; 0: always launch kernel by kernel.  Off while
-     * profiling is on. */
+    /* 1 (default): a batch seen before with the same parameters and buffers
+     * is captured once into a CUDA graph and replayed as one launch
+     * afterwards (host-buffer jobs too: their copies in and out stay outside
+     * the graph, so new seed values in the same arrays are used); at most 64
+     * graphs are kept per graph handle.  0: always launch kernel by kernel.
+     * Off while profiling is on. */
     CSAW_OPT_CUDA_GRAPHS = 1,
     /* n > 0: the next CSAW_SCHED_LEARNED runs record up to n execution
      * profiles (features, granularity, cycles) with a random valid
