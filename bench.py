@@ -376,7 +376,7 @@ def serving(args, n_slots=8):
         run_stream(csaw, S, serve_requests(csaw, g, n_slots, rng, kind=k, n_seeds=8192), 1e6, rng, pool)
     run_stream(csaw, S, serve_requests(csaw, g, 400, rng), SERVE_RATE, rng, pool)
     # and the 1024-seed 2-hop shape, so its page-locked output buffers exist
-    # before timing (allocating them takes the driver lock for milliseconds)
+    # before timing (allocating them takes the CUDA driver's lock for milliseconds)
     run_stream(csaw, S, serve_requests(csaw, g, 200, rng, kind=0, n_seeds=1024), SERVE_RATE, rng, pool)
     pool.prefill(1024 * (25 + 250), 64)   # a burst of late waits must not allocate mid-stream
     S.stats(reset=True)

@@ -224,9 +224,9 @@ enum {
 int csaw_graph_set_option(csaw_graph g, int option, int64_t value);
 
 /*
- * Autotuner of the launch shape for a recurring batch (north-star "tile
- * sizes from an autotuner"; the reference fixes n_blocks x n_threads by
- * hand, main.cu:219-224): times the batch under each candidate
+ * Autotuner of the launch shape for a recurring batch (the reference fixes
+ * n_blocks x n_threads by hand, main.cu:219-224): times the batch under
+ * each candidate
  * (grid 50/100/200 % x pairing on/off), device-timed, after one untimed run
  * each, and keeps the fastest in the graph's options.  The jobs' outputs are
  * overwritten by the runs (identical under every candidate).

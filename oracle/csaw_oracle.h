@@ -3,7 +3,7 @@
  *
  * TEST INFRASTRUCTURE ONLY.  Nothing in the product library links, loads or
  * calls this code.  Only tests/, __graft_entry__.smoke() and bench.py's CPU
- * baseline leg use it, as the checker.
+ * baseline leg use it, to check or to time against.
  *
  * PARITY UNPINNED against the reference: C-SAW ships no tests, no golden
  * vectors and no known-answer data (its only example graph, web-Google, is not

@@ -1,7 +1,7 @@
 """ctypes wrapper of the CPU oracle (libcsaw_oracle.so).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
-CPU-baseline leg of bench.py, as the checker.  The product library never
+CPU-baseline leg of bench.py, to check or to time against.  The product library never
 loads it.  Parity against the C-SAW reference itself is unpinned (the
 reference ships no tests or golden data and its sampler is cuRAND-driven
 device code); see csaw_oracle.h.

@@ -7,8 +7,8 @@ spreads its output over 65536 subsequences (counter word 2) and advances the
 position inside each subsequence in counter word 0.  That layout was found by
 matching the generator's output against this repository's oracle; the test
 then checks all listed blocks, so a wrong layout or a wrong Philox fails.
-Run here once (needs only libcurand, no GPU); the .npz is committed so the
-GPU box never needs cuRAND for this check.
+Run once on any machine with libcurand (no GPU needed); the .npz is
+committed so the test never needs cuRAND.
 """
 import ctypes
 import os
