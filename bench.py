@@ -1,34 +1,46 @@
 """Benchmark: sampled edges per second (SEPS) on one B200 (or N replicas).
 
-Workload (one step): the mid-size power-law graph -- a seeded synthetic
-directed graph with 875,713 vertices and 5,105,039 edges, out-degree power
-law exponent 2.1 capped at 460, int32 CSR, lognormal(0,1) weights -- run with
-  (a) degree-biased neighbor sampling: 4000 samples, FrontierSize 4,
-      NeighborSize 20, Depth 3;
-  (b) degree-biased random walks: 4000 walks of length 64.
+Default workload, one step -- the learned-scheduler configuration at scale 25:
+R-MAT (a=.6, b=.2, c=.15, d=.05) scale 25, edge factor 16, directed, with
+self-loops and duplicate edges removed (33,554,432 vertices, 516,609,074
+edges, max out-degree 986,212), int64 row offsets, int32 columns,
+Pareto(1.5) FP32 weights, generated on the GPU from a fixed seed, then
+  (a) edge-weight-biased neighbor sampling: 65,536 samples, FrontierSize 8,
+      NeighborSize 10, Depth 3;
+  (b) edge-weight-biased random walks: 1,048,576 walks of length 40.
 value = (edges of a + edges of b) / device time of the step.  Inputs are
-resident in HBM; between timed steps a 256 MiB buffer is written to flush L2.
-e2e = the same metric through the host-buffer entry points (csaw_sample_host
-for the plain form, csaw_sample_batch with host buffers for the batched form):
-host seeds in, host edge list (src, dst, sample) out, copies inside the timed
-region.
+resident in HBM and far larger than L2; a 256 MiB buffer is also written
+between timed steps.  e2e = the same metric through the host-buffer entry
+point (csaw_sample_batch with host jobs): host seeds in, host edge list
+(src, dst, sample) out, copies inside the timed region.
+
 Three forms run on the same graph, seeds and keys: "plain" (one warp per
-item, level by level, gathered degree bias, jobs one after the other),
-"batched" (load-balanced expansion, neighbor records, concurrent jobs,
-CUDA-graph replay, degree-rule granularity) and "learned" (batched with the
-learned granularity scheduler, trained on the GPU on profiles recorded on a
-few warm-up steps).  value is the last form of --forms (default: learned).
+item, level by level, the bias prefix recomputed per expansion, jobs one
+after the other), "batched" (load-balanced expansion, neighbor records,
+per-vertex prefix cache, concurrent jobs, CUDA-graph replay, degree-rule
+granularity, launch shape from the autotuner) and "learned" (batched with
+the learned granularity scheduler, trained on the GPU on profiles recorded
+on warm-up steps).  value is the last form of --forms (default: learned).
+Every form's edge multiset is hashed; differing hashes abort the run.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl csaw|reference]
+                  [--workload rmat25|powerlaw] [--scale S]
+
+--workload powerlaw: the mid-size power-law graph (875,713 vertices,
+5,105,039 edges, out-degree exponent 2.1 capped at 460, int32 CSR,
+lognormal(0,1) weights), (a) 4000 degree-biased samples F4 N20 D3 and (b)
+4000 degree-biased walks of 64.  The default run reports it, the request
+loop (serving) and MDRW as extra keys.
 
 --impl reference times the CPU oracle (a port of the reference's sampling
 semantics; the reference itself has no CPU implementation and its CUDA
 kernels read out of bounds, so they are not run) on all host threads, on a
-bounded sample of the same workload.
+bounded seed subsample of the same workload and graph.
 """
 import argparse
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -40,15 +52,41 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path[:0] = [os.path.join(ROOT, "c-saw_b200")]
 
-GRAPH = dict(n_vertices=875_713, n_edges=5_105_039, gamma=2.1, max_degree=460, seed=20, weight="lognormal")
-WORK_A = dict(mode=0, bias=1, n_samples=4000, frontier_size=4, neighbor_size=20, depth=3)
-WORK_B = dict(mode=1, bias=1, n_samples=4000, frontier_size=1, neighbor_size=1, depth=64)
-SEED_A, SEED_B = 0xC5A0, 0xC5A1
+WORKLOADS = {
+    "rmat25": dict(
+        name="rmat{scale}_ef16_a.6_b.2_c.15_pareto1.5",
+        generator="rmat_device",
+        graph=dict(scale=25, edge_factor=16, a=0.6, b=0.2, c=0.15, seed=25, symmetrize=False, weight="pareto:1.5"),
+        rowptr64=True,
+        a=dict(mode=0, bias=2, n_samples=65536, frontier_size=8, neighbor_size=10, depth=3),
+        b=dict(mode=1, bias=2, n_samples=1 << 20, frontier_size=1, neighbor_size=1, depth=40),
+        seeds=(0x25A, 0x25B),
+        cpu_fraction=1 / 512,   # oracle sample: this share of the samples of (a) and of the walks of (b)
+        plain_fraction=1 / 8,   # the plain form runs this share (it rebuilds every hub's prefix per expansion)
+        text="(a) edge-weight-biased neighbor sampling {na} samples F8 N10 D3 + (b) edge-weight-biased "
+             "random walks {nb} x 40"),
+    "powerlaw": dict(
+        name="powerlaw_v875713_e5105039",
+        generator="powerlaw_directed",
+        graph=dict(n_vertices=875_713, n_edges=5_105_039, gamma=2.1, max_degree=460, seed=20, weight="lognormal"),
+        rowptr64=False,
+        a=dict(mode=0, bias=1, n_samples=4000, frontier_size=4, neighbor_size=20, depth=3),
+        b=dict(mode=1, bias=1, n_samples=4000, frontier_size=1, neighbor_size=1, depth=64),
+        seeds=(0xC5A0, 0xC5A1),
+        cpu_fraction=1 / 4,
+        plain_fraction=1,
+        text="(a) degree-biased neighbor sampling {na} samples F4 N20 D3 + (b) degree-biased random walks {nb} x 64"),
+}
 FLUSH_BYTES = 256 << 20
-# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum, mean over
-# the three level launches of one step) from one full ncu capture of the
-# batched form of this workload; the capture is summarised under profiles/.
-DRAM_TRAFFIC = {"k_select_fast": 5.01e6, "k_coop_fast": 13.8e6, "k_walk_fast": 43.1e6}
+KINDS = ("expand", "select", "hub", "pair", "heavy", "walk", "walk_thread", "setup")
+TRAFFIC_TABLE = os.path.join(ROOT, "profiles", "dram_traffic_rmat22.md")
+
+
+def kernel_name(kind, batched):
+    return {"expand": "k_coop_fast" if batched else "k_expand_warp", "select": "k_select_fast",
+            "hub": "k_select_hub", "pair": "k_select_pair", "heavy": "k_expand_heavy",
+            "walk": "k_walk_fast" if batched else "k_walk_warp",
+            "walk_thread": "k_walk_thread_fast" if batched else "k_walk_thread", "setup": "setup"}[kind]
 
 
 def load_peaks():
@@ -58,6 +96,21 @@ def load_peaks():
             d = json.load(f)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def traffic_per_item():
+    """DRAM bytes per work item of each kernel, from the committed ncu summary
+    (a capture of the same step at R-MAT scale 22: dram__bytes_read.sum +
+    dram__bytes_write.sum over one step's launches / the step's items)."""
+    out = {}
+    if not os.path.exists(TRAFFIC_TABLE):
+        return out
+    with open(TRAFFIC_TABLE) as f:
+        for line in f:
+            m = re.match(r"\|\s*(k_\w+)\s*\|\s*([\d.]+)\s*\|\s*([\d.]+)\s*\|\s*([\d.]+)\s*\|\s*([\d.]+)\s*\|", line)
+            if m:
+                out[m.group(1)] = float(m.group(5))
+    return out
 
 
 class Clocks:
@@ -113,44 +166,82 @@ def dist_env():
     return int(os.environ.get("RANK", "0")), ws, int(os.environ.get("LOCAL_RANK", "0"))
 
 
-def build_graph():
+
+def workload(name, scale=25):
+    """The workload spec, with the R-MAT one scaled to 2^scale vertices
+    (samples and walks scaled alike) for smaller profiling runs."""
+    wl = {k: (dict(v) if isinstance(v, dict) else v) for k, v in WORKLOADS[name].items()}
+    if name == "rmat25" and scale != 25:
+        wl["graph"]["scale"] = scale
+        for j in ("a", "b"):
+            wl[j]["n_samples"] = max(1, wl[j]["n_samples"] >> (25 - scale))
+    wl["name"] = wl["name"].format(scale=wl["graph"].get("scale", 0))
+    wl["text"] = wl["text"].format(na=f"{wl['a']['n_samples']:,}", nb=f"{wl['b']['n_samples']:,}")
+    return wl
+
+
+def build_graph(wl):
     from csaw import graphgen
-    return graphgen.powerlaw_directed(**GRAPH)
+    return getattr(graphgen, wl["generator"])(**wl["graph"])
 
 
-def workload_desc():
-    return {"workload": "powerlaw_v875713_e5105039: (a) degree-biased neighbor sampling 4000 samples F4 N20 D3 "
-                        "+ (b) degree-biased random walks 4000 x 64",
-            "graph": GRAPH, "a": WORK_A, "b": WORK_B, "l2": "flushed between timed steps (256 MiB write)"}
+def workload_desc(wl):
+    return {"workload": f"{wl['name']}: {wl['text']}", "graph": wl["graph"], "rowptr": "int64" if wl["rowptr64"]
+            else "int32", "a": wl["a"], "b": wl["b"],
+            "l2": "inputs larger than L2, and a 256 MiB buffer written between timed steps"}
+
+
+def fanout(j):
+    return [j["neighbor_size"]] * j["depth"] if j["mode"] == 0 else None
+
+
+def oracle_sample(wl, g, threads):
+    """A bounded seed subsample of the workload for the CPU oracle: the first
+    cpu_fraction of the samples of (a) and of the walks of (b), with the
+    same seeds (and so the same edges) as the GPU run gives them."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    A, B = wl["a"], wl["b"]
+    na = max(1, int(A["n_samples"] * wl["cpu_fraction"]))
+    nb = max(1, int(B["n_samples"] * wl["cpu_fraction"]))
+    sa = oracle.make_seeds(g.rowptr, na * A["frontier_size"], wl["seeds"][0])
+    sb = oracle.make_seeds(g.rowptr, nb, wl["seeds"][1])
+
+    def rep():
+        ea = oracle.run(g.rowptr, g.col, g.weight, sa, A["mode"], A["bias"], na, A["frontier_size"], A["depth"],
+                        fanout(A), seed=wl["seeds"][0], n_threads=threads)
+        eb = oracle.run(g.rowptr, g.col, g.weight, sb, B["mode"], B["bias"], nb, 1, B["depth"], None,
+                        seed=wl["seeds"][1], n_threads=threads)
+        return len(ea[0]) + len(eb[0])
+
+    text = (f"the first {na:,} of {A['n_samples']:,} samples of (a) and {nb:,} of {B['n_samples']:,} walks of (b) "
+            f"(same seeds and graph)")
+    return rep, text
 
 
 def run_reference(args):
-    """CPU oracle on all host threads, bounded sample of the workload per step."""
+    """The CPU oracle on all host threads, one bounded seed subsample of the
+    workload per step.  The input graph is synthesised exactly as for the
+    GPU arm (torch on the GPU for the R-MAT graph: input generation only);
+    all sampling runs on the host."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    g = build_graph()
+    wl = workload(args.workload, args.scale)
+    g = build_graph(wl)
+    if wl["generator"] == "rmat_device":
+        import torch
+        torch.cuda.empty_cache()
     threads = os.cpu_count() or 1
-    na, nb = 1000, 1000   # a quarter of each workload per step
-    seeds_a = oracle.make_seeds(g.rowptr, na * WORK_A["frontier_size"], SEED_A)
-    seeds_b = oracle.make_seeds(g.rowptr, nb, SEED_B)
-
-    def step():
-        ea = oracle.run(g.rowptr, g.col, g.weight, seeds_a, 0, 1, na, 4, 3, [20, 20, 20], seed=SEED_A,
-                        n_threads=threads)
-        eb = oracle.run(g.rowptr, g.col, g.weight, seeds_b, 1, 1, nb, 1, 64, seed=SEED_B, n_threads=threads)
-        return len(ea[0]) + len(eb[0])
-
+    rep, text = oracle_sample(wl, g, threads)
     for _ in range(args.warmup):
-        step()
+        rep()
     t0 = time.perf_counter()
-    edges = sum(step() for _ in range(args.steps))
+    edges = sum(rep() for _ in range(args.steps))
     dt = time.perf_counter() - t0
     v = edges / dt
-    desc = workload_desc()
-    desc["sample"] = f"{na} of 4000 samples of (a) and {nb} of 4000 walks of (b) per step"
+    desc = workload_desc(wl)
+    desc["sample"] = text + " per step"
     line = {"impl": "reference", "metric": "sampled_edges_per_sec", "value": v, "unit": "edges/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -161,25 +252,332 @@ def run_reference(args):
     print(json.dumps(line))
 
 
-def cpu_baseline(g):
+def cpu_baseline(wl, g, seconds=10.0):
     """Oracle timed on the host cores on a bounded sample (reported baseline only)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
     threads = os.cpu_count() or 1
-    na, nb = 1000, 1000
-    sa = oracle.make_seeds(g.rowptr, na * 4, SEED_A)
-    sb = oracle.make_seeds(g.rowptr, nb, SEED_B)
+    rep, text = oracle_sample(wl, g, threads)
     edges, t0, reps = 0, time.perf_counter(), 0
     while True:
-        ea = oracle.run(g.rowptr, g.col, g.weight, sa, 0, 1, na, 4, 3, [20, 20, 20], seed=SEED_A, n_threads=threads)
-        eb = oracle.run(g.rowptr, g.col, g.weight, sb, 1, 1, nb, 1, 64, seed=SEED_B, n_threads=threads)
-        edges += len(ea[0]) + len(eb[0])
+        edges += rep()
         reps += 1
-        if time.perf_counter() - t0 > 10.0:
+        if time.perf_counter() - t0 > seconds:
             break
     dt = time.perf_counter() - t0
     return {"value": edges / dt, "unit": "edges/s", "cores": threads, "kind": "port",
-            "sample": f"{reps} x ({na} of 4000 samples of (a) + {nb} of 4000 walks of (b)), {dt:.1f} s"}
+            "sample": f"{reps} x ({text}), {dt:.1f} s"}
+
+
+_M64 = (1 << 64) - 1
+
+
+def _i64(c):
+    return c - (1 << 64) if c >= 1 << 63 else c
+
+
+def _mix(z):
+    """splitmix64 finaliser on int64 tensors (wrapping arithmetic, logical shifts)."""
+    z = z ^ ((z >> 30) & ((1 << 34) - 1))
+    z = z * _i64(0xBF58476D1CE4E5B9)
+    z = z ^ ((z >> 27) & ((1 << 37) - 1))
+    z = z * _i64(0x94D049BB133111EB)
+    return z ^ ((z >> 31) & ((1 << 33) - 1))
+
+
+def edge_hash(out, n):
+    """Order-independent hash of the multiset of (src, dst, sample) rows of an
+    output: the wrapping sums of two independent 64-bit hashes of each edge,
+    and the count (equal multisets give equal hashes in any order)."""
+    import torch
+    if n == 0:
+        return "0:0:0"
+    src, dst, smp = (out[i, :n].to(torch.int64) for i in range(3))
+    x = (src & 0xFFFFFFFF) | (dst << 32)
+    h1 = _mix(x ^ _mix(smp + 0x5851F42D))
+    h2 = _mix(h1 ^ _i64(0xD6E8FEB86659FD93))
+    return f"{n}:{int(h1.sum().item()) & _M64:016x}:{int(h2.sum().item()) & _M64:016x}"
+
+
+def measure(args, wl, rank, world, local, headline=True):
+    """Times the workload's forms and returns the JSON line's fields (rank 0)
+    or None.  headline=False: an extra workload (fewer side measurements)."""
+    import torch
+    import csaw
+    from csaw import dist as cdist
+    t_gen = time.perf_counter()
+    g = build_graph(wl)
+    gen_s = time.perf_counter() - t_gen
+    torch.cuda.empty_cache()
+    G = csaw.Graph(g, rowptr64=wl["rowptr64"])
+    stream = torch.cuda.current_stream()
+    A, B = wl["a"], wl["b"]
+    sa0, sb0 = wl["seeds"]
+    seeds_a = G.make_seeds(A["n_samples"] * A["frontier_size"], sa0 + 7919 * rank)
+    seeds_b = G.make_seeds(B["n_samples"], sb0 + 7919 * rank)
+    # replicas (weak scaling): same job shape, rank-disjoint global sample ids
+    scheds = (("plain", csaw.SCHED_PLAIN), ("batched", csaw.SCHED_BATCHED), ("learned", csaw.SCHED_LEARNED))
+    params = {f: (cdist.replica_params(csaw.make_params(**A, seed=sa0, schedule=s), rank),
+                  cdist.replica_params(csaw.make_params(**B, seed=sb0, schedule=s), rank)) for f, s in scheds}
+    pa, pb = params["batched"]
+    cap_a, cap_b = csaw.edge_bound(pa), csaw.edge_bound(pb)
+    out_a = torch.empty((3, cap_a), dtype=torch.int32, device="cuda")
+    out_b = torch.empty((3, cap_b), dtype=torch.int32, device="cuda")
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.int32, device="cuda")
+    batch_jobs = {f: [csaw.BatchJob(params[f][0], seeds_a, cap_a, out_a, with_depth=False),
+                      csaw.BatchJob(params[f][1], seeds_b, cap_b, out_b, with_depth=False)]
+                  for f in ("batched", "learned")}
+    last = {}
+    # the plain form runs the first plain_fraction of the samples and walks
+    # (same ids, seeds and so edges as in the full run); "sub" is the batched
+    # form on that subsample, for the edge-multiset check
+    frac = wl["plain_fraction"]
+    sub_n = (max(1, int(A["n_samples"] * frac)), max(1, int(B["n_samples"] * frac)))
+
+    def subsample(p, n):
+        q = cdist.replica_params(p, 0)   # a copy
+        q.n_samples = n
+        return q
+
+    params["sub"] = tuple(subsample(p, n) for p, n in zip(params["batched"], sub_n))
+    plain_params = tuple(subsample(p, n) for p, n in zip(params["plain"], sub_n))
+    sub_seeds = (seeds_a[:sub_n[0] * A["frontier_size"]], seeds_b[:sub_n[1]])
+    batch_jobs["sub"] = [csaw.BatchJob(params["sub"][0], sub_seeds[0], cap_a, out_a, with_depth=False),
+                         csaw.BatchJob(params["sub"][1], sub_seeds[1], cap_b, out_b, with_depth=False)]
+
+    def step(form):
+        if form == "plain":   # one job after the other, as the reference runs them
+            qa, qb = plain_params
+            a = G.sample(qa, sub_seeds[0], capacity=cap_a, out=out_a, with_depth=False)
+            b = G.sample(qb, sub_seeds[1], capacity=cap_b, out=out_b, with_depth=False)
+            last["n"] = (a[0].numel(), b[0].numel())
+        else:
+            res = G.sample_batch(batch_jobs[form])   # both workloads as one batch
+            last["n"] = (res[0][0].numel(), res[1][0].numel())
+        return sum(last["n"])
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def timed(form, steps, warmup, clocks=None, profile=False):
+        """steps device-timed steps (L2 flushed before each); returns edges, ms,
+        kernel stats, launches, clocks.  profile=True brackets every kernel with
+        CUDA events on its own stream (no CUDA-graph replay)."""
+        for _ in range(warmup):
+            step(form)
+        G.profile(profile)
+        launches0 = G.stats()["kernel_launches"]
+        if clocks:
+            clocks.start()
+        barrier()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        edges = 0
+        for i in range(steps):
+            flush.zero_()
+            evs[i][0].record(stream)
+            edges += step(form)
+            evs[i][1].record(stream)
+        barrier()
+        clk = clocks.stop() if clocks else None
+        launches = G.stats()["kernel_launches"] - launches0
+        ms = sum(x.elapsed_time(y) for x, y in evs)
+        ks = {k: G.kernel_stats(k) for k in KINDS}
+        G.profile(False)
+        return edges, ms, ks, launches, clk
+
+    def form_hash():
+        return edge_hash(out_a, last["n"][0]) + "|" + edge_hash(out_b, last["n"][1])
+
+    forms = [f.strip() for f in args.forms.split(",") if f.strip()]
+    main_form = forms[-1]
+    hashes, other, info = {}, {}, {}
+    plain_ms = plain_k = plain_edges = None
+    if "plain" in forms and main_form != "plain":
+        # the plain form recomputes every expanded hub's prefix: its steps are
+        # bounded by a time budget (first warm-up step measured)
+        t0 = time.perf_counter()
+        step("plain")
+        torch.cuda.synchronize()
+        one = time.perf_counter() - t0
+        k = max(2, min(args.steps, int(args.plain_budget_s / max(one, 1e-6))))
+        plain_edges, plain_ms, plain_k, _, _ = timed("plain", k, max(args.warmup - 1, 2), profile=True)
+        info["plain_steps"] = k
+        plain_edges, plain_ms = plain_edges / k, plain_ms / k
+        info["plain_sample"] = (f"first {sub_n[0]:,} of {A['n_samples']:,} samples of (a) and {sub_n[1]:,} of "
+                                f"{B['n_samples']:,} walks of (b)" if frac < 1 else "the whole step")
+        info["plain_edges_per_step"] = plain_edges
+        h_plain = form_hash()
+        step("sub")
+        if form_hash() != h_plain:
+            raise SystemExit("plain and batched forms emitted different edge multisets on the plain sample")
+        hashes["plain (sample)" if frac < 1 else "plain"] = h_plain
+    tune = None
+    if "batched" in forms:   # the launch-shape autotuner, on the batched form's own batch
+        for _ in range(args.warmup):
+            step("batched")
+        tune = G.autotune(batch_jobs["batched"])
+        if main_form != "batched":
+            e, ms, _, _, _ = timed("batched", args.steps, 1)
+            other["batched"] = ms / args.steps
+            hashes["batched"] = form_hash()
+    sched = None
+    if "learned" in forms:
+        # the learned scheduler: record execution profiles, train on the GPU
+        G.sched_record(400_000)
+        for _ in range(2):
+            step("learned")
+        t0 = time.perf_counter()
+        loss = G.sched_train(epochs=400, lr=3e-3, seed=rank)
+        train_s = time.perf_counter() - t0
+        for _ in range(6):   # timed trial of the model against the degree rule
+            step("learned")
+        si = G.sched_info()
+        sched = {"records": si["records"], "train_loss": loss, "train_s": train_s, "class_mask": si["class_mask"],
+                 "kept_model": si["class_mask"] != 0x3}
+    # per-kernel events for the roofline come from a profiled pass of the same
+    # steps; the reported value is the unprofiled pass (graph replay allowed)
+    _, prof_ms, kstats, _, _ = timed(main_form, args.steps, args.warmup, profile=True)
+    edges, ms, _, launches, clk = timed(main_form, args.steps, args.warmup, Clocks(local) if headline else None)
+    hashes[main_form] = form_hash()
+    edges_per_step = edges / args.steps
+    if frac == 1 and plain_edges is not None and plain_edges != edges_per_step:
+        raise SystemExit(f"plain and {main_form} forms emitted different edge counts: {plain_edges} vs "
+                         f"{edges_per_step}")
+    full = {k: v for k, v in hashes.items() if k != "plain (sample)"}
+    if len(set(full.values())) != 1:
+        raise SystemExit(f"forms emitted different edge multisets: {hashes}")
+    qa, qb = params[main_form]
+
+    # ---- end to end through the host-buffer entry point
+    seeds_a_h = seeds_a.cpu().numpy()
+    seeds_b_h = seeds_b.cpu().numpy()
+    host_a = torch.empty((3, cap_a), dtype=torch.int32).pin_memory().numpy()
+    host_b = torch.empty((3, cap_b), dtype=torch.int32).pin_memory().numpy()
+    sa_pin = torch.from_numpy(seeds_a_h).pin_memory().numpy()
+    sb_pin = torch.from_numpy(seeds_b_h).pin_memory().numpy()
+    host_jobs = [csaw.BatchJob(qa, sa_pin, cap_a, host_a, with_depth=False, host=True),
+                 csaw.BatchJob(qb, sb_pin, cap_b, host_b, with_depth=False, host=True)]
+
+    def e2e_step():
+        if main_form == "plain":
+            ra = G.sample_host(qa, sa_pin, capacity=cap_a, out=host_a, with_depth=False, stream=stream.cuda_stream)
+            rb = G.sample_host(qb, sb_pin, capacity=cap_b, out=host_b, with_depth=False, stream=stream.cuda_stream)
+        else:
+            ra, rb = G.sample_batch(host_jobs, stream=stream.cuda_stream)
+        return ra[0].size + rb[0].size
+
+    e2e_steps = max(3, args.steps // 2)
+
+    def e2e_time(parts):
+        # parts: CSAW_OPT_HOST_PARTS (0 = by output size; -1 = copy after sampling)
+        G.set_option(csaw._lib.OPT_HOST_PARTS, parts)
+        for _ in range(2):
+            e2e_step()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        n = 0
+        for _ in range(e2e_steps):
+            n += e2e_step()
+        e1.record(stream)
+        barrier()
+        return n, e0.elapsed_time(e1)
+
+    one_edges, one_ms = e2e_time(-1)
+    e2e_edges, e2e_ms = e2e_time(0)
+    if e2e_edges != edges_per_step * e2e_steps:
+        raise SystemExit(f"host-buffer run emitted {e2e_edges / e2e_steps} edges per step, device run "
+                         f"{edges_per_step}")
+
+    mdrw = None
+    if not headline:
+        # MDRW, as the reference dispatches FrontierSize > 1 (main.cu:281-288):
+        # 4000 degree-biased samples, frontier 4, 3 steps (timed separately)
+        pm = cdist.replica_params(csaw.make_params(2, 1, 4000, 4, 20, 3, seed=sa0 ^ 0x5A,
+                                                   schedule=csaw.SCHED_BATCHED), rank)
+        out_m = torch.empty((3, csaw.edge_bound(pm)), dtype=torch.int32, device="cuda")
+        for _ in range(args.warmup):
+            G.sample(pm, seeds_a, out=out_m, with_depth=False)
+        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m0.record(stream)
+        m_edges = 0
+        for _ in range(args.steps):
+            m_edges += G.sample(pm, seeds_a, out=out_m, with_depth=False)[0].numel()
+        m1.record(stream)
+        barrier()
+        mdrw = {"samples": 4000, "frontier_size": 4, "depth": 3, "bias": "degree",
+                "ms_per_step": m0.elapsed_time(m1) / args.steps, "edges_per_step": m_edges / args.steps,
+                "seps": m_edges / (m0.elapsed_time(m1) * 1e-3)}
+
+    # ---- whole-job totals: edges summed, device time max over ranks
+    t_s = ms / 1e3
+    if world > 1:
+        all_edges, t_max = cdist.reduce_totals(edges, t_s)
+        e2e_all, e2e_t = cdist.reduce_totals(e2e_edges, e2e_ms / 1e3)
+        one_all, one_t = cdist.reduce_totals(one_edges, one_ms / 1e3)
+        _, plain_t = cdist.reduce_totals(0, (plain_ms or 0.0) / 1e3)
+        _, batched_t = cdist.reduce_totals(0, other.get("batched", 0.0) / 1e3)
+    else:
+        all_edges, t_max, e2e_all, e2e_t = float(edges), t_s, float(e2e_edges), e2e_ms / 1e3
+        one_all, one_t = float(one_edges), one_ms / 1e3
+        plain_t = (plain_ms or 0.0) / 1e3
+        batched_t = other.get("batched", 0.0) / 1e3
+    value = all_edges / t_max
+    e2e_value = e2e_all / e2e_t
+    plain_value = plain_edges * world / plain_t if plain_t else None   # the plain form's own edges per second
+
+    peak, peak_kind = load_peaks()
+    batched_form = main_form != "plain"
+    timed_kinds = [k for k in KINDS if k != "setup" and kstats.get(k, {}).get("launches")]
+    dom = max(timed_kinds, key=lambda k: kstats[k]["ms"])
+    kd = kstats[dom]
+    dname = kernel_name(dom, batched_form)
+    achieved = kd["bytes"] / (kd["ms"] * 1e-3) / 1e9 if kd["ms"] > 0 else None
+    per_item = traffic_per_item().get(dname)
+    items_per_launch = kd["items"] / kd["launches"]
+    roofline = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind + " (hbm_gbs copy)",
+                "traffic": per_item * items_per_launch if per_item else None,
+                "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum per item of {dname}, "
+                                   f"{os.path.relpath(TRAFFIC_TABLE, ROOT)} (R-MAT scale 22 capture of the same "
+                                   f"step), x {items_per_launch:.0f} items per launch") if per_item else
+                                  "no committed capture for this kernel",
+                "algorithmic_bytes_per_launch": kd["bytes"] / kd["launches"],
+                "items_per_launch": items_per_launch, "launch_ms": kd["ms"] / kd["launches"],
+                "step_counted_bytes": sum(v["bytes"] for v in kstats.values()) / args.steps,
+                "step_frac": sum(v["bytes"] for v in kstats.values()) / args.steps / (ms / args.steps * 1e-3)
+                / 1e9 / peak,
+                "note": "per-kernel CUDA events on the job streams, from a profiled pass of the same steps "
+                        "(kernel by kernel, no graph replay); the neighbor and walk jobs overlap, so each "
+                        "kernel's time includes sharing the GPU; step_frac = all kernels' counted bytes / "
+                        "the unprofiled step time"}
+    res = {"value": value, "ms_per_step": ms / args.steps, "edges_per_step": all_edges / args.steps / world,
+           "config": workload_desc(wl), "graph_stats": {"n_vertices": g.n_vertices, "n_edges": g.n_edges,
+                                                        "max_degree": int(np.diff(g.rowptr).max()),
+                                                        "generate_s": gen_s},
+           "e2e": {"value": e2e_value, "unit": "edges/s",
+                   "h2d_bytes_per_step": 4 * (seeds_a_h.size + seeds_b_h.size),
+                   "d2h_bytes_per_step": int(12 * e2e_edges / e2e_steps)},
+           "e2e_detail": {"host_parts": "by output size (CSAW_OPT_HOST_PARTS 0; edges copied back after every hop "
+                                        "and every sample range)",
+                          "no_overlap_value": one_all / one_t,
+                          "note": "no_overlap_value: the same calls with every host job's edges copied back "
+                                  "after all of its sampling (CSAW_OPT_HOST_PARTS -1)"},
+           "gpu_launches": int(launches), "clocks": clk, "roofline": roofline,
+           "kernels": {k: v for k, v in kstats.items() if v["launches"]},
+           "profiled_pass_ms_per_step": prof_ms / args.steps,
+           "forms": {main_form: value, "plain": plain_value,
+                     "speedup_vs_plain": value / plain_value if plain_value else None,
+                     **({"batched": all_edges / batched_t} if batched_t else {}),
+                     **({"learned_vs_batched": batched_t / t_max} if batched_t and main_form == "learned" else {}),
+                     "edge_multiset_hash": hashes, "scheduler": sched, "autotune": tune, **info,
+                     "plain_kernels": {k: v for k, v in (plain_k or {}).items() if v["launches"]}}}
+    if mdrw:
+        res["mdrw"] = mdrw
+    G.close()
+    del host_a, host_b, out_a, out_b
+    torch.cuda.empty_cache()
+    return res, g
 
 
 def learned_gain(args):
@@ -402,88 +800,6 @@ def serving(args, n_slots=8):
     return res
 
 
-SCALE25_GRAPH = dict(scale=25, edge_factor=16, a=0.6, b=0.2, c=0.15, seed=25, symmetrize=False,
-                     weight="pareto:1.5")
-
-
-def scale25(args):
-    """Learned scheduler at scale: R-MAT (a=.6, b=.2, c=.15) scale 25, edge
-    factor 16, directed, int64 rowptr, int32 col, Pareto(1.5) weights
-    (generated on the GPU); one step = 65,536 edge-weight-biased samples
-    (F 8, N 10, D 3) and 1M edge-weight-biased walks of length 40 as one
-    batch.  The batched (degree rule) and learned forms are timed; the
-    learned one is trained on profiles recorded on warm-up steps."""
-    import torch
-    import csaw
-    from csaw import graphgen
-    torch.cuda.set_device(0)
-    t0 = time.perf_counter()
-    sc = args.s25_scale
-    g = graphgen.rmat_device(**dict(SCALE25_GRAPH, scale=sc))
-    gen_s = time.perf_counter() - t0
-    torch.cuda.empty_cache()
-    G = csaw.Graph(g, rowptr64=True)
-    ns, nw = 65536 >> (25 - sc), (1 << 20) >> (25 - sc)
-    seeds_a = G.make_seeds(ns * 8, 0x25A)
-    seeds_b = G.make_seeds(nw, 0x25B)
-    res = {"graph": {"workload": f"rmat{sc}_ef16_a.6_b.2_c.15_pareto1.5", "n_vertices": g.n_vertices,
-                     "n_edges": g.n_edges, "max_degree": int(np.diff(g.rowptr).max()), "generate_s": gen_s},
-           "a": dict(mode=0, bias=2, n_samples=ns, frontier_size=8, neighbor_size=10, depth=3),
-           "b": dict(mode=1, bias=2, n_samples=nw, depth=40)}
-    del g
-    peak, peak_kind = load_peaks()
-    outs = {}
-    forms = [f for f in (("batched", csaw.SCHED_BATCHED), ("learned", csaw.SCHED_LEARNED))
-             if f[0] in args.s25_forms.split(",")]
-    for form, sch in forms:
-        pa = csaw.make_params(0, 2, ns, 8, 10, 3, seed=0x25A, schedule=sch)
-        pb = csaw.make_params(1, 2, nw, 1, 1, 40, seed=0x25B, schedule=sch)
-        if "a" not in outs:
-            outs["a"] = torch.empty((3, csaw.edge_bound(pa)), dtype=torch.int32, device="cuda")
-            outs["b"] = torch.empty((3, csaw.edge_bound(pb)), dtype=torch.int32, device="cuda")
-        jobs = [csaw.BatchJob(pa, seeds_a, outs["a"].shape[1], outs["a"], with_depth=False),
-                csaw.BatchJob(pb, seeds_b, outs["b"].shape[1], outs["b"], with_depth=False)]
-        r = {}
-        if form == "learned":
-            G.sched_record(400_000)
-            for _ in range(2):
-                G.sample_batch(jobs)
-            r["train_loss"] = G.sched_train(epochs=400, lr=3e-3, seed=1)
-            for _ in range(6):   # timed trial of the model against the degree rule
-                G.sample_batch(jobs)
-            r["class_mask"] = G.sched_info()["class_mask"]
-        for _ in range(args.warmup):
-            G.sample_batch(jobs)
-        if form == "batched":
-            r["autotune"] = G.autotune(jobs)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        n = 0
-        for _ in range(args.steps):
-            res_b = G.sample_batch(jobs)
-            n += res_b[0][0].numel() + res_b[1][0].numel()
-        e1.record()
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / args.steps
-        G.profile(True)
-        G.sample_batch(jobs)
-        ks = {k: G.kernel_stats(k) for k in ("expand", "select", "hub", "pair", "heavy", "walk", "setup")}
-        G.profile(False)
-        tot_bytes = sum(v["bytes"] for v in ks.values())
-        r.update({"ms_per_step": ms, "edges_per_step": n / args.steps, "seps": n / args.steps / (ms * 1e-3),
-                  "algorithmic_bytes_per_step": tot_bytes,
-                  "achieved_gbs": tot_bytes / (ms * 1e-3) / 1e9,
-                  "roofline_frac": tot_bytes / (ms * 1e-3) / 1e9 / peak,
-                  "kernels": {k: v for k, v in ks.items() if v["launches"]}})
-        res[form] = r
-    res["peak_gbs"] = peak
-    res["peak_source"] = peak_kind
-    if "batched" in res and "learned" in res:
-        res["learned_speedup"] = res["batched"]["ms_per_step"] / res["learned"]["ms_per_step"]
-    G.close()
-    return res
-
 
 STREAM_GRAPH = dict(scale=26, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=29, symmetrize=False, weight="uniform")
 
@@ -549,22 +865,62 @@ def streaming(args):
     return res
 
 
+
+def profile_step(args):
+    """For ncu captures of one step: the batched form's batch, W warm-up steps,
+    one step, then one profiled step whose per-kernel items and counted bytes
+    are printed (the same for every step).  No autotuning, training, extra
+    workloads or host copies."""
+    import torch
+    import csaw
+    torch.cuda.set_device(0)
+    wl = workload(args.workload, args.scale)
+    g = build_graph(wl)
+    torch.cuda.empty_cache()
+    G = csaw.Graph(g, rowptr64=wl["rowptr64"])
+    G.set_option(csaw._lib.OPT_CUDA_GRAPHS, 0)   # every step launches its kernels (ncu counts launches)
+    A, B = wl["a"], wl["b"]
+    sa = G.make_seeds(A["n_samples"] * A["frontier_size"], wl["seeds"][0])
+    sb = G.make_seeds(B["n_samples"], wl["seeds"][1])
+    pa = csaw.make_params(**A, seed=wl["seeds"][0], schedule=csaw.SCHED_BATCHED)
+    pb = csaw.make_params(**B, seed=wl["seeds"][1], schedule=csaw.SCHED_BATCHED)
+    oa = torch.empty((3, csaw.edge_bound(pa)), dtype=torch.int32, device="cuda")
+    ob = torch.empty((3, csaw.edge_bound(pb)), dtype=torch.int32, device="cuda")
+    jobs = [csaw.BatchJob(pa, sa, oa.shape[1], oa, with_depth=False),
+            csaw.BatchJob(pb, sb, ob.shape[1], ob, with_depth=False)]
+    for _ in range(args.warmup):
+        G.sample_batch(jobs)
+    torch.cuda.synchronize()
+    r = G.sample_batch(jobs)
+    torch.cuda.synchronize()
+    G.profile(True)
+    G.sample_batch(jobs)
+    ks = {k: v for k, v in ((k, G.kernel_stats(k)) for k in KINDS) if v["launches"]}
+    G.profile(False)
+    print(json.dumps({"profile_step": {"workload": wl["name"], "edges": r[0][0].numel() + r[1][0].numel(),
+                                       "kernels": {kernel_name(k, True): v for k, v in ks.items()}}}))
+    G.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="csaw", choices=["csaw", "reference"])
+    ap.add_argument("--workload", default="rmat25", choices=sorted(WORKLOADS))
+    ap.add_argument("--scale", type=int, default=25,
+                    help="R-MAT scale of the rmat25 workload (samples and walks scale with 2^scale)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the power-law and serving extra keys")
+    ap.add_argument("--plain-budget-s", type=float, default=20.0,
+                    help="device time the plain form's timed steps may take (at least 2 steps)")
+    ap.add_argument("--profile-step", action="store_true",
+                    help="run W warm-up steps and one step of the batched form only (for ncu captures)")
     ap.add_argument("--learned-gain", action="store_true",
                     help="time the degree rule vs the learned scheduler on a heavy-tailed R-MAT graph instead")
     ap.add_argument("--serve", action="store_true", help="run only the serving (request loop) workload")
-    ap.add_argument("--no-serve", action="store_true", help="skip the serving workload in the default run")
-    ap.add_argument("--scale25", action="store_true", help="run only the R-MAT scale-25 learned-scheduler workload")
     ap.add_argument("--stream", action="store_true", help="run only the streaming (out-of-budget) workload")
-    ap.add_argument("--s25-scale", type=int, default=25,
-                    help="R-MAT scale for --scale25 (samples and walks scale with 2^scale; smaller for profiling)")
-    ap.add_argument("--s25-forms", default="batched,learned", help="forms timed by --scale25")
     ap.add_argument("--serve-requests", type=int, default=4000, help="requests per serving stream")
     ap.add_argument("--forms", default="plain,batched,learned",
                     help="forms to time; the last one is reported as value (profiling runs use one form)")
@@ -580,8 +936,8 @@ def main():
     if args.stream:
         print(json.dumps({"streaming": streaming(args)}))
         return
-    if args.scale25:
-        print(json.dumps({"scale25": scale25(args)}))
+    if args.profile_step:
+        profile_step(args)
         return
     if args.serve:
         import torch
@@ -590,223 +946,33 @@ def main():
         return
 
     import torch
-    import csaw
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    g = build_graph()
-    G = csaw.Graph(g)                       # one resident CSR for both forms
-    stream = torch.cuda.current_stream()
-    seeds_a = G.make_seeds(4000 * 4, SEED_A + 7919 * rank)
-    seeds_b = G.make_seeds(4000, SEED_B + 7919 * rank)
-    from csaw import dist as cdist
-    # replicas (weak scaling): same job shape, rank-disjoint global sample ids
-    params = {f: (cdist.replica_params(csaw.make_params(**WORK_A, seed=SEED_A, schedule=sch), rank),
-                  cdist.replica_params(csaw.make_params(**WORK_B, seed=SEED_B, schedule=sch), rank))
-              for f, sch in (("plain", csaw.SCHED_PLAIN), ("batched", csaw.SCHED_BATCHED),
-                             ("learned", csaw.SCHED_LEARNED))}
-    pa, pb = params["batched"]
-    cap_a, cap_b = csaw.edge_bound(pa), csaw.edge_bound(pb)
-    out_a = torch.empty((3, cap_a), dtype=torch.int32, device="cuda")
-    out_b = torch.empty((3, cap_b), dtype=torch.int32, device="cuda")
-    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.int32, device="cuda")
-
-    batch_jobs = {f: [csaw.BatchJob(params[f][0], seeds_a, cap_a, out_a, with_depth=False),
-                      csaw.BatchJob(params[f][1], seeds_b, cap_b, out_b, with_depth=False)]
-                  for f in ("batched", "learned")}
-
-    def step(form):
-        if form == "plain":   # one job after the other, as the reference runs them
-            qa, qb = params[form]
-            a = G.sample(qa, seeds_a, capacity=cap_a, out=out_a, with_depth=False)
-            b = G.sample(qb, seeds_b, capacity=cap_b, out=out_b, with_depth=False)
-            return a[0].numel() + b[0].numel()
-        res = G.sample_batch(batch_jobs[form])   # both workloads as one batch
-        return res[0][0].numel() + res[1][0].numel()
-
-    def barrier():
-        if world > 1:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
-
-    def timed(form, clocks=None, profile=False):
-        """K device-timed steps (L2 flushed before each); returns edges, ms, kernel stats, launches.
-        With profile=True every kernel is bracketed by CUDA events (and CUDA-graph replay is off)."""
-        for _ in range(args.warmup):
-            step(form)
-        G.profile(profile)
-        launches0 = G.stats()["kernel_launches"]
-        if clocks:
-            clocks.start()
-        barrier()
-        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-               for _ in range(args.steps)]
-        edges = 0
-        for i in range(args.steps):
-            flush.zero_()
-            evs[i][0].record(stream)
-            edges += step(form)
-            evs[i][1].record(stream)
-        barrier()
-        clk = clocks.stop() if clocks else None
-        launches = G.stats()["kernel_launches"] - launches0
-        ms = sum(x.elapsed_time(y) for x, y in evs)
-        ks = {k: G.kernel_stats(k) for k in ("expand", "select", "hub", "pair", "heavy", "walk", "setup")}
-        G.profile(False)
-        return edges, ms, ks, launches, clk
-
-    forms = [f.strip() for f in args.forms.split(",") if f.strip()]
-    main_form = forms[-1]
-    plain_ms, plain_k = None, {}
-    other = {}
-    if "plain" in forms and main_form != "plain":
-        plain_edges, plain_ms, plain_k, _, _ = timed("plain", profile=True)
-    tune = None
-    if "batched" in forms:   # the launch-shape autotuner, on the batched form's own batch
-        for _ in range(args.warmup):
-            step("batched")
-        tune = G.autotune(batch_jobs["batched"])
-    if "batched" in forms and main_form != "batched":
-        other["batched"] = timed("batched")[1]
-    sched = None
-    if "learned" in forms:
-        # the learned scheduler: record execution profiles, train on the GPU
-        G.sched_record(400_000)
-        for _ in range(3):
-            step("learned")
-        t0 = time.perf_counter()
-        loss = G.sched_train(epochs=400, lr=3e-3, seed=rank)
-        train_s = time.perf_counter() - t0
-        for _ in range(6):   # timed trial of the model against the degree rule
-            step("learned")
-        sched = {"records": G.sched_info()["records"], "train_loss": loss, "train_s": train_s,
-                 "class_mask": G.sched_info()["class_mask"]}
-    # per-kernel events for the roofline come from a profiled pass of the same
-    # steps; the reported value is the unprofiled pass (graph replay allowed)
-    _, prof_ms, kstats, _, _ = timed(main_form, profile=True)
-    edges, ms, _, launches, clk = timed(main_form, Clocks(local))
-    if plain_ms is not None and edges != plain_edges:
-        raise SystemExit(f"plain and {main_form} forms emitted different edge counts: {plain_edges} vs {edges}")
-    pa, pb = params[main_form]
-
-    # ---- end to end through the host-buffer entry point
-    seeds_a_h = seeds_a.cpu().numpy()
-    seeds_b_h = seeds_b.cpu().numpy()
-    host_a = torch.empty((3, cap_a), dtype=torch.int32).pin_memory().numpy()
-    host_b = torch.empty((3, cap_b), dtype=torch.int32).pin_memory().numpy()
-    sa_pin = torch.from_numpy(seeds_a_h).pin_memory().numpy()
-    sb_pin = torch.from_numpy(seeds_b_h).pin_memory().numpy()
-    host_jobs = [csaw.BatchJob(pa, sa_pin, cap_a, host_a, with_depth=False, host=True),
-                 csaw.BatchJob(pb, sb_pin, cap_b, host_b, with_depth=False, host=True)]
-
-    def e2e_step():
-        if main_form == "plain":
-            ra = G.sample_host(pa, sa_pin, capacity=cap_a, out=host_a, with_depth=False, stream=stream.cuda_stream)
-            rb = G.sample_host(pb, sb_pin, capacity=cap_b, out=host_b, with_depth=False, stream=stream.cuda_stream)
-        else:
-            ra, rb = G.sample_batch(host_jobs, stream=stream.cuda_stream)
-        return ra[0].size + rb[0].size
-
-    e2e_steps = max(3, args.steps // 2)
-
-    def e2e_time(parts):
-        # parts: CSAW_OPT_HOST_PARTS (0 = by output size; -1 = copy after sampling)
-        G.set_option(csaw._lib.OPT_HOST_PARTS, parts)
-        e2e_step()
-        barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        n = 0
-        for _ in range(e2e_steps):
-            n += e2e_step()
-        e1.record(stream)
-        barrier()
-        return n, e0.elapsed_time(e1)
-
-    one_edges, one_ms = e2e_time(-1)
-    e2e_edges, e2e_ms = e2e_time(0)
-
-    # ---- MDRW, as the reference dispatches FrontierSize > 1 (main.cu:281-288):
-    # 4000 degree-biased samples, frontier 4, 3 steps (timed separately)
-    pm = cdist.replica_params(csaw.make_params(2, 1, 4000, 4, 20, 3, seed=SEED_A ^ 0x5A, schedule=csaw.SCHED_BATCHED),
-                              rank)
-    out_m = torch.empty((3, csaw.edge_bound(pm)), dtype=torch.int32, device="cuda")
-    for _ in range(args.warmup):
-        G.sample(pm, seeds_a, out=out_m, with_depth=False)
-    m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    m0.record(stream)
-    m_edges = 0
-    for _ in range(args.steps):
-        m_edges += G.sample(pm, seeds_a, out=out_m, with_depth=False)[0].numel()
-    m1.record(stream)
-    barrier()
-    mdrw = {"samples": 4000, "frontier_size": 4, "depth": 3, "bias": "degree",
-            "ms_per_step": m0.elapsed_time(m1) / args.steps, "edges_per_step": m_edges / args.steps,
-            "seps": m_edges / (m0.elapsed_time(m1) * 1e-3)}
-
-    # ---- whole-job totals: edges summed, device time max over ranks
-    t_s = ms / 1e3
-    if world > 1:
-        all_edges, t_max = cdist.reduce_totals(edges, t_s)
-        e2e_all, e2e_t = cdist.reduce_totals(e2e_edges, e2e_ms / 1e3)
-        one_all, one_t = cdist.reduce_totals(one_edges, one_ms / 1e3)
-        _, plain_t = cdist.reduce_totals(0, (plain_ms or 0.0) / 1e3)
-    else:
-        all_edges, t_max, e2e_all, e2e_t = float(edges), t_s, float(e2e_edges), e2e_ms / 1e3
-        one_all, one_t = float(one_edges), one_ms / 1e3
-        plain_t = (plain_ms or 0.0) / 1e3
-    value = all_edges / t_max
-    e2e_value = e2e_all / e2e_t
-
-    peak, peak_kind = load_peaks()
-    kernel_names = {"expand": "k_coop_fast" if main_form != "plain" else "k_expand_warp",
-                    "select": "k_select_fast", "hub": "k_select_hub", "pair": "k_select_pair", "heavy": "k_expand_heavy",
-                    "walk": "k_walk_fast" if main_form != "plain" else "k_walk_warp"}
-    timed_kinds = [k for k in kernel_names if kstats.get(k, {}).get("launches")]
-    dom = max(timed_kinds, key=lambda k: kstats[k]["ms"])
-    kd = kstats[dom]
-    achieved = kd["bytes"] / (kd["ms"] * 1e-3) / 1e9 if kd["ms"] > 0 else None
-    roofline = {"bound": "hbm", "kernel": kernel_names[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind + " (hbm_gbs copy)",
-                "traffic": DRAM_TRAFFIC.get(kernel_names[dom]),
-                "algorithmic_bytes_per_launch": kd["bytes"] / kd["launches"],
-                "launch_ms": kd["ms"] / kd["launches"],
-                "note": "per-kernel CUDA events on the job streams, from a profiled pass of the same steps "
-                        "(kernel by kernel, no graph replay); in the batched form the neighbor and walk jobs "
-                        "overlap, so each kernel's time includes sharing the GPU"}
-
+    wl = workload(args.workload, args.scale)
+    res, g = measure(args, wl, rank, world, local, headline=True)
     if rank == 0:
-        line = {"metric": "sampled_edges_per_sec", "value": value, "unit": "edges/s", "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        line = {"metric": "sampled_edges_per_sec", "value": res["value"], "unit": "edges/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+int32",
-                "data": "synthetic", "config": workload_desc(),
-                "e2e": {"value": e2e_value, "unit": "edges/s",
-                        "h2d_bytes_per_step": 4 * (seeds_a_h.size + seeds_b_h.size),
-                        "d2h_bytes_per_step": int(12 * e2e_edges / e2e_steps)},
-                "e2e_detail": {"host_parts": "by output size (one sample range per job here; edges copied back after every hop)",
-                               "no_overlap_value": one_all / one_t,
-                               "note": "no_overlap_value: the same calls with every host job's edges "
-                                       "copied back after all of its sampling (CSAW_OPT_HOST_PARTS -1)"},
-                "gpu_launches": int(launches), "clocks": clk, "roofline": roofline,
-                "kernels": {k: v for k, v in kstats.items() if v["launches"]},
-                "profiled_pass_ms_per_step": prof_ms / args.steps,
-                "forms": {main_form: value, "plain": all_edges / plain_t if plain_t else None,
-                          "speedup_vs_plain": plain_t / t_max if plain_t else None,
-                          **{f: all_edges / (ms_f / 1e3) for f, ms_f in other.items()},
-                          **({"learned_vs_batched": (other["batched"] / ms)} if "batched" in other else {}),
-                          "scheduler": sched, "autotune": tune,
-                          "plain_kernels": {k: v for k, v in plain_k.items() if v["launches"]}},
-                "edges_per_step": all_edges / args.steps / world, "mdrw": mdrw}
-        if not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(g)
-        if world == 1 and not args.no_serve:
+                "data": "synthetic (seeded generators; no dataset)", "config": res["config"],
+                "e2e": res["e2e"], "gpu_launches": res["gpu_launches"], "clocks": res["clocks"],
+                "roofline": res["roofline"]}
+        line.update({k: v for k, v in res.items() if k not in line})
+        if not args.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline(wl, g)
+        del g
+        if world == 1 and not args.no_extras:
+            if args.workload != "powerlaw":
+                extra, _ = measure(args, workload("powerlaw"), rank, world, local, headline=False)
+                line["powerlaw"] = {k: extra[k] for k in ("value", "ms_per_step", "edges_per_step", "config", "e2e",
+                                                          "e2e_detail", "roofline", "kernels", "forms", "mdrw",
+                                                          "gpu_launches")}
             line["serving"] = serving(args)
         print(json.dumps(line))
-    G.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -16,7 +16,8 @@ SCHED_PLAIN, SCHED_BATCHED, SCHED_LEARNED = 0, 1, 2
 GRAPH_DEGREE_BIAS, GRAPH_CDF_CACHE, GRAPH_NO_CDF_CACHE = 1, 2, 4
 PARAM_DEDUP = 1
 MAX_DEPTH = 64
-KERNEL_KINDS = {"expand": 0, "heavy": 1, "walk": 2, "mdrw": 3, "setup": 4, "select": 5, "hub": 6, "pair": 7}
+KERNEL_KINDS = {"expand": 0, "heavy": 1, "walk": 2, "mdrw": 3, "setup": 4, "select": 5, "hub": 6, "pair": 7,
+                "walk_thread": 8}
 
 # Every symbol include/csaw.h declares (tests check the library exports them).
 EXPORTS = [

@@ -53,7 +53,7 @@ int fail(int code, const std::string &msg) {
     } while (0)
 
 enum { KK_EXPAND = 0, KK_HEAVY = 1, KK_WALK = 2, KK_MDRW = 3, KK_INIT = 4, KK_SELECT = 5, KK_HUB = 6, KK_PAIR = 7,
-       KK_COUNT = 8 };
+       KK_WALK_THREAD = 8, KK_COUNT = 9 };
 
 struct Counters {
     unsigned long long out_count;
@@ -725,7 +725,7 @@ int run_walk_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int32_t *
         int gmax = plain ? grid_for(k_walk_thread<I>, WALK_THREADS, 0, g->sm_count)
                          : grid_for(k_walk_thread_fast<I, CSAW_BIAS_UNBIASED>, WALK_THREADS, 0, g->sm_count);
         if (grid > gmax) grid = gmax;
-        LaunchScope ls(g, KK_WALK, st);
+        LaunchScope ls(g, KK_WALK_THREAD, st);
         if (plain) k_walk_thread<I><<<grid, WALK_THREADS, 0, st>>>(dg, a);
         else k_walk_thread_fast<I, CSAW_BIAS_UNBIASED><<<grid, WALK_THREADS, 0, st>>>(dg, a);
     } else if (!plain && dg.cdf && (int64_t)p->n_samples >= 16ll * grid_for(k_walk_fast<I, BIAS>, FAST_THREADS, 0,
@@ -734,7 +734,7 @@ int run_walk_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int32_t *
         int grid = (p->n_samples + WALK_THREADS - 1) / WALK_THREADS;
         const int gmax = grid_for(k_walk_thread_fast<I, BIAS>, WALK_THREADS, 0, g->sm_count);
         if (grid > gmax) grid = gmax;
-        LaunchScope ls(g, KK_WALK, st);
+        LaunchScope ls(g, KK_WALK_THREAD, st);
         k_walk_thread_fast<I, BIAS><<<grid, WALK_THREADS, 0, st>>>(dg, a);
     } else {
         int gmax = plain ? grid_for(k_walk_warp<I, BIAS>, WALK_THREADS, 0, g->sm_count)

@@ -1024,8 +1024,8 @@ k_walk_thread_fast(DevGraph g, WalkArgs a) {
     }
     if (lane == 0) {
         unsigned long long per = 4 + sizeof(I) + 4 + 4ull * (2 + (a.o_smp != nullptr) + (a.o_dep != nullptr));
-        atomicAdd(&a.bytes[2], tot * per + 4 * pr);   // + prefix probes (biased)
-        atomicAdd(&a.items[2], tot);
+        atomicAdd(&a.bytes[8], tot * per + 4 * pr);   // + prefix probes (biased)
+        atomicAdd(&a.items[8], tot);
     }
 }
 

@@ -437,8 +437,8 @@ k_walk_thread(DevGraph g, WalkArgs a) {
     for (int off = 16; off; off >>= 1) tot += __shfl_xor_sync(FULL, tot, off);
     if (lane == 0) {
         unsigned long long per = 2 * sizeof(I) + 4 + 4ull * (2 + (a.o_smp != nullptr) + (a.o_dep != nullptr));
-        atomicAdd(&a.bytes[2], tot * per);
-        atomicAdd(&a.items[2], tot);
+        atomicAdd(&a.bytes[8], tot * per);
+        atomicAdd(&a.items[8], tot);
     }
 }
 

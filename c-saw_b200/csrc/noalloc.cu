@@ -23,8 +23,12 @@
 //     two calls whose work overlaps on the GPU (different streams, or host
 //     threads) race on the same queues -- serialise them;
 //   - the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress, with that device current); make that first call
-//     before any stream capture.
+//     (cudaGetSymbolAddress, with that device current); with CUDA's lazy
+//     module loading that call may also load this library's device code and
+//     reserve the array, so make the first call during set-up, before any
+//     stream capture;
+//   - p->schedule is ignored: the plain level loop always runs (every
+//     schedule gives the same output).
 #include <cuda_runtime.h>
 
 #include <mutex>

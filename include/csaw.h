@@ -139,7 +139,9 @@ int csaw_graph_stats(csaw_graph g, csaw_stats *out);
  * Kinds: 0 level expansion (batched: take-all pass), 1 high-degree (CTA)
  * expansion, 2 walk, 3 MDRW, 4 queue/seed/residency setup, 5 batched
  * warp-granularity selection pass, 6 batched hub selection (cached prefix),
- * 7 batched two-items-per-warp selection (cached prefix, N <= 16).
+ * 7 batched two-items-per-warp selection (cached prefix, N <= 16), 8 walk
+ * with one thread per walk (unbiased walks; many biased walks over a cached
+ * prefix).
  */
 int csaw_graph_profile(csaw_graph g, int enable);
 int csaw_graph_kernel_stats(csaw_graph g, int kind, double *ms, int64_t *launches,
@@ -282,7 +284,11 @@ int csaw_mlp_grad_host(const float *params, const float *norm, const void *recor
  * frontier level exceeds 1398090 items, and biased jobs on graphs with a
  * vertex of degree above 1024.  All calls on a device share the array:
  * calls whose GPU work overlaps race -- serialise them.  The first call on
- * a device looks up the array's address; make it before any stream capture.
+ * a device looks up the array's address and, with CUDA's lazy module
+ * loading, may be the point where the library's device code is loaded and
+ * the 32 MiB array reserved: make that first call during set-up, before any
+ * stream capture.  The schedule field of p is ignored (the plain level loop
+ * always runs; its output equals every schedule's).
  */
 int csaw_sample_noalloc(csaw_graph g, const csaw_params *p, const int32_t *seeds,
                         int32_t *out_src, int32_t *out_dst, int32_t *out_sample,

@@ -34,6 +34,34 @@ def powerlaw_small():
                                       weight="lognormal")
 
 
+def make_skewed_hubs():
+    """Power-law graph (60k vertices) plus six hub rows of 600 to 50,000
+    distinct neighbors: rows above 4096 edges (one-CTA prefix build), above
+    1024 (both prefix index levels) and above 512 (hub and pair paths)."""
+    from csaw import graphgen
+    base = graphgen.powerlaw_directed(n_vertices=60_000, n_edges=300_000, gamma=2.1, max_degree=300, seed=11,
+                                      weight="none")
+    V = base.n_vertices
+    src = np.repeat(np.arange(V, dtype=np.int64), np.diff(base.rowptr))
+    dst = base.col.astype(np.int64)
+    rng = np.random.default_rng(12)
+    hubs = rng.choice(V, 6, replace=False)
+    hs, hd = [src], [dst]
+    for h, d in zip(hubs, (50_000, 12_000, 5_000, 2_100, 1_100, 600)):
+        nb = rng.choice(V, d, replace=False)
+        nb = nb[nb != h]
+        hs.append(np.full(nb.size, h, dtype=np.int64))
+        hd.append(nb.astype(np.int64))
+    key = np.unique(np.concatenate(hs) * V + np.concatenate(hd))
+    rowptr, col = graphgen._csr_from_edges(key // V, key % V, V)
+    return graphgen.CSR(rowptr, col, graphgen.weights("pareto:1.5", col.size, 13), name="skewed_hubs")
+
+
+@pytest.fixture(scope="session")
+def skewed_hubs():
+    return make_skewed_hubs()
+
+
 def sort_edges(src, dst, smp, dep):
     src, dst, smp, dep = (np.asarray(x, dtype=np.int64) for x in (src, dst, smp, dep))
     o = np.lexsort((dst, src, dep, smp))

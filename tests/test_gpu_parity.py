@@ -160,13 +160,26 @@ def test_bad_seed_is_rejected(csaw, powerlaw_small):
 
 
 def test_reference_compatible_sampler(csaw, powerlaw_small, tmp_path):
+    """Sampler() on int64 beg.bin/csr.bin files: its edge count equals the
+    oracle's on the file-loaded graph (the entry draws make_seeds(n * F, 56)
+    and samples with the default hooks, i.e. degree bias, seed 56), and the
+    same call through the handle API gives the oracle's edges."""
+    import torch
     from csaw import graphgen
     beg, csr = tmp_path / "beg.bin", tmp_path / "csr.bin"
     graphgen.write_reference_format(powerlaw_small, beg, csr)
-    r = csaw.Sampler(beg, csr, 400, 128, 100, 1, 5, 3)
-    assert r.sampled_edges > 0 and r.time > 0
-    r2 = csaw.Sampler(beg, csr, 400, 128, 50, 4, 1, 30)   # FrontierSize > 1: MDRW
-    assert 0 < r2.sampled_edges <= 50 * 30
+    g = graphgen.read_reference_format(beg, csr)
+    G = csaw.Graph(g, rowptr64=True, degree_bias=True)   # what the entry builds from the files
+    for n, F, N, D in ((100, 1, 5, 3), (50, 4, 1, 30)):   # FrontierSize > 1: MDRW, as main.cu:281-288
+        r = csaw.Sampler(beg, csr, 400, 128, n, F, N, D)
+        mode = 2 if F > 1 else 0
+        seeds = oracle.make_seeds(g.rowptr, n * F, 56)
+        ref = oracle.run(g.rowptr, g.col, None, seeds, mode, 1, n, F, D, [N] * D if mode == 0 else None, seed=56,
+                         n_threads=8)
+        assert r.sampled_edges == len(ref[0]) > 0 and r.time > 0
+        p = csaw.make_params(mode, 3, n, F, N, D, None, seed=56)
+        out = [x.cpu().numpy() for x in G.sample(p, torch.from_numpy(seeds).cuda())]
+        assert_parity(out, ref)
 
 
 def test_repeat_runs_identical(csaw, rmat12_pareto):
