@@ -568,8 +568,10 @@ def measure(args, wl, rank, world, local, headline=True):
            "profiled_pass_ms_per_step": prof_ms / args.steps,
            "forms": {main_form: value, "plain": plain_value,
                      "speedup_vs_plain": value / plain_value if plain_value else None,
-                     **({"batched": all_edges / batched_t} if batched_t else {}),
-                     **({"learned_vs_batched": batched_t / t_max} if batched_t and main_form == "learned" else {}),
+                     # batched_t: seconds per step (max over ranks); t_max: all K steps
+                     **({"batched": all_edges / args.steps / batched_t} if batched_t else {}),
+                     **({"learned_vs_batched": batched_t / (t_max / args.steps)}
+                        if batched_t and main_form == "learned" else {}),
                      "edge_multiset_hash": hashes, "scheduler": sched, "autotune": tune, **info,
                      "plain_kernels": {k: v for k, v in (plain_k or {}).items() if v["launches"]}}}
     if mdrw:
@@ -725,29 +727,45 @@ def run_closed(csaw, S, reqs, window, pool):
 
 
 class PinnedPool:
-    """Page-locked (2, cap) int32 buffers by power-of-two size class."""
+    """Page-locked (2, cls) int32 output buffers by power-of-two size class,
+    carved from page-locked arenas allocated before timing: allocating
+    page-locked memory takes the CUDA driver's lock for milliseconds, which
+    would stall the request loop's worker mid-stream.  A class that runs out
+    falls back to a fresh allocation, counted in `misses`."""
 
     def __init__(self):
         self.free = {}
+        self.arenas = []
+        self.misses = 0
+
+    @staticmethod
+    def cls_of(cap):
+        return max(1 << 12, 1 << int(np.ceil(np.log2(max(cap, 1)))))
 
     def get(self, cap):
         import torch
-        cls = max(1 << 12, 1 << int(np.ceil(np.log2(max(cap, 1)))))
+        cls = self.cls_of(cap)
         lst = self.free.setdefault(cls, [])
         if lst:
             return cls, lst.pop()
+        self.misses += 1
         return cls, torch.empty((2, cls), dtype=torch.int32).pin_memory()
 
     def put(self, cls, buf):
         self.free[cls].append(buf)
 
-    def prefill(self, cap, n):
-        """n buffers of cap's class, allocated before timing."""
+    def prefill(self, counts):
+        """counts: {class: buffers}; one page-locked arena holds them all."""
         import torch
-        cls = max(1 << 12, 1 << int(np.ceil(np.log2(max(cap, 1)))))
-        lst = self.free.setdefault(cls, [])
-        while len(lst) < n:
-            lst.append(torch.empty((2, cls), dtype=torch.int32).pin_memory())
+        total = sum(2 * c * n for c, n in counts.items())
+        arena = torch.empty(total, dtype=torch.int32).pin_memory()
+        self.arenas.append(arena)
+        off = 0
+        for c, n in sorted(counts.items()):
+            lst = self.free.setdefault(c, [])
+            for _ in range(n):
+                lst.append(arena[off:off + 2 * c].view(2, c))
+                off += 2 * c
 
 
 def serving(args, n_slots=8):
@@ -765,6 +783,11 @@ def serving(args, n_slots=8):
     S = csaw.Server(G, n_slots=n_slots, device_budget=2 << 30)
     rng = np.random.default_rng(2000)
     pool = PinnedPool()
+    # every output class a request can need, with room for bursts of
+    # outstanding requests (the waiter returns buffers in submission order)
+    top = PinnedPool.cls_of(8192 * (15 + 150 + 750))
+    pool.prefill({1 << k: (64 if (1 << k) <= (1 << 19) else 32 if (1 << k) <= (1 << 21) else 16)
+                  for k in range(12, int(np.log2(top)) + 1)})
     res = {"graph": {"workload": f"rmat{SERVE_GRAPH['scale']}_ef{SERVE_GRAPH['edge_factor']}",
                      "n_vertices": g.n_vertices, "n_edges": g.n_edges,
                      "max_degree": int(np.diff(g.rowptr).max())},
@@ -776,7 +799,7 @@ def serving(args, n_slots=8):
     # and the 1024-seed 2-hop shape, so its page-locked output buffers exist
     # before timing (allocating them takes the CUDA driver's lock for milliseconds)
     run_stream(csaw, S, serve_requests(csaw, g, 200, rng, kind=0, n_seeds=1024), SERVE_RATE, rng, pool)
-    pool.prefill(1024 * (25 + 250), 64)   # a burst of late waits must not allocate mid-stream
+    misses0 = pool.misses
     S.stats(reset=True)
     for name, rate, reqs in (
             ("mixed", SERVE_RATE, serve_requests(csaw, g, args.serve_requests, rng)),
@@ -794,7 +817,11 @@ def serving(args, n_slots=8):
                      "p99_launch_ms": st["p99_launch_ms"], "p99_gpu_ms": st["p99_gpu_ms"], "edges": int(edges.sum()),
                      "seps": float(edges.sum()) / (st["last_done_s"] - st["first_submit_s"]),
                      "offered_rate": len(reqs) / wall, "failed": st["failed"],
-                     "peak_device_bytes": st["peak_device_bytes"]}
+                     "peak_device_bytes": st["peak_device_bytes"],
+                     "max_worker_call_ms": st["max_worker_call_ms"],
+                     "worker_calls_over_1ms": st["worker_calls_over_1ms"],
+                     "pinned_allocations_while_timed": pool.misses - misses0}
+        misses0 = pool.misses
     S.close()
     G.close()
     return res

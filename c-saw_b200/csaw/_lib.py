@@ -68,7 +68,9 @@ class ServerStats(ctypes.Structure):
     _fields_ = [(f, ctypes.c_int64) for f in ("submitted", "completed", "failed", "queued", "in_flight", "edges",
                                                "peak_device_bytes", "workspace_bytes")] + \
                [(f, ctypes.c_double) for f in ("p50_ms", "p90_ms", "p99_ms", "max_ms", "mean_ms", "p99_queue_ms",
-                                                "p99_launch_ms", "p99_gpu_ms", "first_submit_s", "last_done_s")]
+                                                "p99_launch_ms", "p99_gpu_ms", "first_submit_s", "last_done_s",
+                                                "max_worker_call_ms")] + \
+               [("worker_calls_over_1ms", ctypes.c_int64)]
 
 
 class TuneResult(ctypes.Structure):

@@ -158,8 +158,7 @@ struct csaw_graph_s {
     uint32_t class_mask = 0x3f;   // classes the trained model picks (bit c)
     int32_t *big_verts = nullptr; // vertices above CDF_BIG (the cache builds them one CTA each)
     int64_t n_big = 0;
-    void *nbr_beg = nullptr;      // per-edge neighbor records (batched schedules)
-    int32_t *nbr_deg = nullptr;
+    NbrRec *nrec = nullptr;       // per-edge neighbor records (batched schedules)
     int32_t *nonisolated = nullptr;
     int64_t dev_bytes = 0;
     std::vector<JobCtx *> jobs;
@@ -221,8 +220,7 @@ DevGraph dev_view(const csaw_graph_s *g, int schedule = CSAW_SCHED_BATCHED, int 
     d.cdf1 = d.cdf ? d.cdf + g->E : nullptr;
     d.cdf2 = d.cdf ? d.cdf + g->E + ((g->E + 31) >> 5) : nullptr;
     d.cdf_bias = bias;
-    d.nbr_beg = fast ? g->nbr_beg : nullptr;
-    d.nbr_deg = fast ? g->nbr_deg : nullptr;
+    d.nrec = fast ? g->nrec : nullptr;
     return d;
 }
 
@@ -280,18 +278,16 @@ int grid_for(K kernel, int threads, size_t dyn_smem, int sm_count) {
 }
 
 // Per-edge neighbor records, built once per graph on first batched use
-// (E * (sizeof(rowptr) + 4) bytes of HBM).
+// (16 E bytes of HBM).
 int ensure_nbr(csaw_graph_s *g, cudaStream_t st) {
-    if (g->nbr_beg || g->E == 0) return 0;
+    if (g->nrec || g->E == 0) return 0;
     ++g_alloc_epoch;
-    const size_t bsz = g->idx64 ? 8 : 4;
-    CK(cudaMalloc(&g->nbr_beg, bsz * (size_t)g->E));
-    CK(cudaMalloc((void **)&g->nbr_deg, sizeof(int32_t) * (size_t)g->E));
-    g->dev_bytes += (int64_t)(bsz + 4) * g->E;
+    CK(cudaMalloc((void **)&g->nrec, sizeof(NbrRec) * (size_t)g->E));
+    g->dev_bytes += (int64_t)sizeof(NbrRec) * g->E;
     DevGraph dg = dev_view(g);
     LaunchScope ls(g, KK_INIT, st);
-    if (g->idx64) k_nbr_records<int64_t><<<g->sm_count * 8, 256, 0, st>>>(dg, (int64_t *)g->nbr_beg, g->nbr_deg);
-    else k_nbr_records<int32_t><<<g->sm_count * 8, 256, 0, st>>>(dg, (int32_t *)g->nbr_beg, g->nbr_deg);
+    if (g->idx64) k_nbr_records<int64_t><<<g->sm_count * 8, 256, 0, st>>>(dg, g->nrec);
+    else k_nbr_records<int32_t><<<g->sm_count * 8, 256, 0, st>>>(dg, g->nrec);
     CK(cudaGetLastError());
     return 0;
 }
@@ -309,7 +305,9 @@ int ensure_cdf(csaw_graph_s *g, cudaStream_t st) {
     float *cdf = nullptr;   // prefix [E], then its search index levels [n1] and [n2]
     const int64_t n1 = (g->E + 31) >> 5, n2 = (g->E + 1023) >> 10;
     ++g_alloc_epoch;
-    CK(cudaMalloc((void **)&cdf, sizeof(float) * (size_t)(g->E + n1 + n2)));
+    // + 16 floats: a row's 16-byte-aligned bulk-copy window may end up to 12
+    // bytes past the row (kernels_fast.cuh, k_select_pair)
+    CK(cudaMalloc((void **)&cdf, sizeof(float) * (size_t)(g->E + n1 + n2 + 16)));
     const DevGraph dg = dev_view(g);
     {
         LaunchScope ls(g, KK_INIT, st);
@@ -604,7 +602,7 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
             a.sched_tab = tabled ? (const uint8_t *)c->stab.p : nullptr;
             a.hub_list = (SelEntry *)c->hubsel.p;
             a.n_hub = &c->ctr->n_hub;
-            const bool paired = cached && g->maxdeg > WF && fan[l] <= 16 && g->pair;
+            const bool paired = !plain && cached && g->maxdeg > WF && fan[l] <= 16 && g->pair;
             a.pair_list = paired ? (SelEntry *)c->pairsel.p : nullptr;
             a.n_pair = &c->ctr->n_pair;
             a.refill_list = (SelEntry *)c->sel.p;   // free once k_select_fast has run
@@ -957,6 +955,8 @@ int finish_job(csaw_graph_s *g, JobCtx *c, int64_t cap, int64_t *n_out) {
     *n_out = (int64_t)k.out_count;
     if (k.err & ERR_SEED_RANGE) return fail(CSAW_ERR_INVALID, "a seed vertex is out of range");
     if (k.err & ERR_UPDATE_RANGE) return fail(CSAW_ERR_DEVICE, "Update() returned a vertex out of range");
+    if (k.err & ERR_COPY_WAIT)
+        return fail(CSAW_ERR_DEVICE, "an asynchronous row copy did not complete within its bounded wait");
     if (k.err) return fail(CSAW_ERR_DEVICE, "kernel error flag " + std::to_string(k.err));
     if ((int64_t)k.out_count > cap)
         return fail(CSAW_ERR_CAPACITY, "output capacity " + std::to_string(cap) + " < " +
@@ -1159,8 +1159,7 @@ extern "C" int csaw_graph_destroy(csaw_graph g) {
     cudaFree(g->ebias);
     for (float *c : g->cdf) cudaFree(c);
     cudaFree(g->big_verts);
-    cudaFree(g->nbr_beg);
-    cudaFree(g->nbr_deg);
+    cudaFree(g->nrec);
     cudaFree(g->nonisolated);
     for (auto &kv : g->graphs) cudaGraphExecDestroy(kv.second);
     for (JobCtx *c : g->jobs) free_job(c);

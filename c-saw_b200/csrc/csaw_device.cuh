@@ -18,6 +18,27 @@ namespace csaw {
 constexpr unsigned FULL = 0xffffffffu;
 
 // --------------------------------------------------------------- graph view
+// Per-edge neighbor record (batched schedules): the column of edge e with the
+// row begin and degree of that column vertex, one 16-byte record, so a
+// selected edge costs one 32-byte sector and one 128-bit load for its
+// neighbor, its adjacency range and its degree.
+struct __align__(16) NbrRec {
+    int32_t col;
+    int32_t deg;
+    long long beg;
+};
+
+static_assert(sizeof(NbrRec) == 16, "one 128-bit load per record");
+
+__device__ __forceinline__ NbrRec load_rec(const NbrRec *r, int64_t e) {
+    const int4 x = __ldg(reinterpret_cast<const int4 *>(r) + e);
+    NbrRec o;
+    o.col = x.x;
+    o.deg = x.y;
+    o.beg = (long long)(((unsigned long long)(uint32_t)x.w << 32) | (uint32_t)x.z);
+    return o;
+}
+
 struct DevGraph {
     csaw_graph_view v;     // what the user hooks see
     const float *ebias;    // materialised neighbor degree per edge, or null
@@ -25,11 +46,10 @@ struct DevGraph {
     const float *cdf1;     // cdf[32k + 31] (search index, level 1), with cdf
     const float *cdf2;     // cdf[1024u + 1023] (search index, level 2), with cdf
     int cdf_bias;          // bias kind the cdf was built for
-    // Per-edge neighbor records (batched schedules): row begin and degree of
-    // col[e], so a selected neighbor carries its own adjacency range and the
-    // next expansion or walk step skips the dependent rowptr load.
-    const void *nbr_beg;   // I[E] or null
-    const int32_t *nbr_deg;  // int32[E] or null
+    // Per-edge neighbor records (batched schedules): a selected neighbor
+    // carries its own adjacency range, so the next expansion or walk step
+    // skips the dependent rowptr loads.
+    const NbrRec *nrec;    // [E] or null
 };
 
 template <typename I>
@@ -49,7 +69,7 @@ __device__ __forceinline__ float edge_bias(const DevGraph &g, int64_t e) {
     if constexpr (BIAS == CSAW_BIAS_EDGE_WEIGHT) {
         return __ldg(g.v.weight + e);
     } else if constexpr (BIAS == CSAW_BIAS_DEGREE) {
-        if (g.nbr_deg) return __int2float_rn(__ldg(g.nbr_deg + e));
+        if (g.nrec) return __int2float_rn(__ldg(&g.nrec[e].deg));
         if (g.ebias) return __ldg(g.ebias + e);
         return degree_f<I>(g, __ldg(g.v.col + e));
     } else {

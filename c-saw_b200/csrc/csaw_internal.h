@@ -148,6 +148,6 @@ struct WalkArgs {
     uint32_t k0, k1;
 };
 
-enum : int { ERR_SEED_RANGE = 1, ERR_UPDATE_RANGE = 2, ERR_SCRATCH = 4 };
+enum : int { ERR_SEED_RANGE = 1, ERR_UPDATE_RANGE = 2, ERR_SCRATCH = 4, ERR_COPY_WAIT = 8 };
 
 }  // namespace csaw

@@ -19,6 +19,7 @@
 //   - batch size shrinks on small levels so every warp gets work.
 #pragma once
 
+#include "bulk_copy.cuh"
 #include "kernels_sample.cuh"
 
 namespace csaw {
@@ -65,14 +66,25 @@ __device__ __forceinline__ int warp_incl_scan(int x, int lane) {
     return x;
 }
 
-// Row begin and degree of vertex u: from the neighbor record of edge e when
-// the record describes u, else from rowptr.
+// Neighbor of edge e with its row begin and degree: one 128-bit record load
+// with the neighbor records, else the column and two rowptr loads.
 template <typename I>
-__device__ __forceinline__ void row_of(const DevGraph &g, int64_t e, int32_t col_u, int32_t u, int64_t &beg,
-                                       int32_t &deg) {
-    if (g.nbr_beg && u == col_u) {
-        beg = (int64_t)__ldg(((const I *)g.nbr_beg) + e);
-        deg = __ldg(g.nbr_deg + e);
+__device__ __forceinline__ NbrRec edge_rec(const DevGraph &g, int64_t e) {
+    if (g.nrec) return load_rec(g.nrec, e);
+    NbrRec r;
+    r.col = __ldg(g.v.col + e);
+    r.beg = row_begin<I>(g, r.col);
+    r.deg = (int32_t)(row_begin<I>(g, r.col + 1) - r.beg);
+    return r;
+}
+
+// Row begin and degree of u = Update(col[e]): the record's when Update kept
+// the neighbor, else from rowptr.
+template <typename I>
+__device__ __forceinline__ void row_of(const DevGraph &g, const NbrRec &r, int32_t u, int64_t &beg, int32_t &deg) {
+    if (u == r.col) {
+        beg = r.beg;
+        deg = r.deg;
     } else {
         beg = row_begin<I>(g, u);
         deg = (int32_t)(row_begin<I>(g, u + 1) - beg);
@@ -354,8 +366,10 @@ __global__ void k_init_queue_fast(DevGraph g, const int32_t *seeds, uint32_t n, 
 template <typename I>
 __device__ __forceinline__ void emit_edge(const DevGraph &g, const LevelArgs &a, int64_t e, int32_t v, int32_t s,
                                           uint32_t child_p, int64_t pos, uint32_t q) {
-    const int32_t u = __ldg(g.v.col + e);
-    int32_t dst = Update(&g.v, u, v);
+    NbrRec r;
+    if (a.push) r = edge_rec<I>(g, e);   // the child's adjacency range comes with it
+    else r.col = __ldg(g.v.col + e);     // last level: the column alone (4-byte stride over a row)
+    int32_t dst = Update(&g.v, r.col, v);
     if (dst < 0 || dst >= g.v.n_vertices) {
         atomicOr(a.err, ERR_UPDATE_RANGE);
         dst = 0;
@@ -369,7 +383,7 @@ __device__ __forceinline__ void emit_edge(const DevGraph &g, const LevelArgs &a,
     if (a.push) {
         int64_t nb;
         int32_t nd;
-        row_of<I>(g, e, u, dst, nb, nd);
+        row_of<I>(g, r, dst, nb, nd);
         a.out_v[q] = dst;
         a.out_s[q] = s;
         a.out_p[q] = child_p;
@@ -665,18 +679,28 @@ __device__ __forceinline__ bool half_select(const Half &h, int N, const DrawCtx 
 // Level expansion, part 2 for items over a cached prefix with N <= 16 and
 // d >= 4N (a rebuild is rare): two items per warp, one per half-warp, lanes
 // N..15 of a half idle instead of N..31 of a warp.  Rows up to WF edges are
-// staged in shared memory and searched there; larger rows are searched in
-// global memory through the prefix index.  Items that need a rebuild are
+// staged in shared memory by the bulk copy engine and searched there; the
+// next item's row is requested as soon as the current item's draws are
+// resolved, so its transfer overlaps the current item's edge emission
+// (dependent neighbor-record gathers and stores).  Larger rows are searched
+// in global memory through the prefix index.  Items that need a rebuild are
 // redone from scratch: rows up to WF by k_select_fast on the refill list
 // (written over the consumed warp list), larger ones by the CTA pass.
 template <typename I, int BIAS>
 __global__ void __launch_bounds__(FAST_THREADS, 4)
 k_select_pair(DevGraph g, LevelArgs a) {
     constexpr int NH = FAST_THREADS / 16;
-    __shared__ float s_P[NH * WF];
+    constexpr int ROW = WF + 4;   // floats: a row of up to WF plus its 16-byte alignment window
+    __shared__ __align__(16) float s_P[NH * ROW];
+    __shared__ __align__(8) uint64_t s_bar[NH];
     const int lane = threadIdx.x & 31;
     const Half h(lane);
-    float *P = s_P + (threadIdx.x >> 4) * WF;
+    const int hid = threadIdx.x >> 4;
+    float *buf = s_P + hid * ROW;
+    uint64_t *bar = s_bar + hid;
+    if (h.sl == 0) mbar_init(bar);
+    mbar_init_fence();
+    __syncthreads();
     const uint32_t gh = (blockIdx.x * blockDim.x + threadIdx.x) >> 4;
     const uint32_t nh = (gridDim.x * blockDim.x) >> 4;
     const uint32_t n = *a.n_pair;
@@ -684,7 +708,29 @@ k_select_pair(DevGraph g, LevelArgs a) {
     const int N = a.N;
     const int nout = 2 + (a.o_smp != nullptr) + (a.o_dep != nullptr);
     unsigned long long my_bytes = 0, my_items = 0;
-    for (uint32_t i = gh; i < n; i += nh) {
+    uint32_t parity = 0;
+    // requests the staged copy of a row (rows up to WF only); returns the
+    // row's offset in the buffer
+    auto request = [&](long long rbeg, int rd) -> int {
+        if (rd > WF) return 0;
+        const RowWindow w = row_window(g.cdf + rbeg, rd);
+        if (h.sl == 0) {
+            fence_async_smem();   // this half's reads of buf precede the copy's writes
+            bulk_load(buf, w.start, w.bytes, bar);
+        }
+        return w.off;
+    };
+    int off = 0;
+    uint32_t i = gh;
+    if (i < n) off = request(__ldg(&a.pair_list[i].beg), __ldg(&a.pair_list[i].d));
+    for (; i < n; i += nh) {
+        const uint32_t inext = i + nh;
+        long long nbeg = 0;
+        int nd = 0;
+        if (inext < n) {   // the next row's range: its load overlaps this item
+            nbeg = __ldg(&a.pair_list[inext].beg);
+            nd = __ldg(&a.pair_list[inext].d);
+        }
         const SelEntry en = a.pair_list[i];
         const int64_t beg = en.beg, d = en.d;
         const DrawCtx dc{a.k0, a.k1, en.p, (uint32_t)en.s, (uint32_t)a.depth};
@@ -694,30 +740,23 @@ k_select_pair(DevGraph g, LevelArgs a) {
         int sel;
         bool ok;
         if (d <= WF) {
-            const float *cp = g.cdf + beg;
-            const int dd = (int)d;
-            for (int i0 = 0; i0 < dd; i0 += 128) {
-                float r[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const int k = i0 + u * 16 + h.sl;
-                    r[u] = k < dd ? __ldg(cp + k) : 0.f;
-                }
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const int k = i0 + u * 16 + h.sl;
-                    if (k < dd) P[k] = r[u];
-                }
+            if (!mbar_wait(bar, parity)) {   // bounded: report instead of spinning on
+                if (h.sl == 0) atomicOr(a.err, ERR_COPY_WAIT);
+                mbar_wait(bar, parity);       // let the copy in flight land before leaving
+                break;
             }
-            __syncwarp(h.mask);
+            parity ^= 1u;
+            const float *P = buf + off;
+            const int dd = (int)d;
             const float T = P[dd - 1];
             ok = half_select(h, N, dc, T, [&](uint32_t x) { return search_upper32(P, dd, its_target(x, T)); }, sel);
-            __syncwarp(h.mask);
+            __syncwarp(h.mask);   // every read of this row is done: the buffer is free
         } else {
             const float T = __ldg(g.cdf + beg + d - 1);
             ok = half_select(h, N, dc, T, [&](uint32_t x) { return (int)cdf_search(g, beg, d, its_target(x, T)); },
                              sel);
         }
+        if (inext < n) off = request(nbeg, nd);
         if (!ok) {   // rebuild needed: a whole warp redoes the item (in shared memory up to WF)
             if (h.sl == 0) {
                 if (d <= WF) a.refill_list[atomicAdd(a.n_refill, 1u)] = en;
@@ -736,14 +775,14 @@ k_select_pair(DevGraph g, LevelArgs a) {
         if (h.sl == 0) {
             my_items++;
             const unsigned long long row = d <= WF ? 4ull * d : (unsigned long long)N * 4ull * (64 - __clzll(d));
-            my_bytes += 16 + row + (unsigned long long)N * (4ull + 4ull * nout + (a.push ? 12ull + 2 * (sizeof(I) + 4)
-                                                                                          : 0ull));
+            my_bytes += 16 + row + (unsigned long long)N * (4ull + 4ull * nout +
+                                                            (a.push ? 12ull + 2 * (sizeof(I) + 4) : 0ull));
         }
     }
 #pragma unroll
-    for (int off = 16; off; off >>= 1) {
-        my_bytes += __shfl_xor_sync(FULL, my_bytes, off);
-        my_items += __shfl_xor_sync(FULL, my_items, off);
+    for (int o = 16; o; o >>= 1) {
+        my_bytes += __shfl_xor_sync(FULL, my_bytes, o);
+        my_items += __shfl_xor_sync(FULL, my_items, o);
     }
     if (lane == 0 && my_items) {
         atomicAdd(&a.bytes[7], my_bytes);
@@ -868,11 +907,15 @@ k_walk_fast(DevGraph g, WalkArgs a) {
                 int32_t ul = 0, dl = 0;
                 int64_t bl = 0;
                 if (lane < d) {
-                    wl = edge_bias<I, BIAS>(g, beg + lane);
-                    ul = __ldg(g.v.col + beg + lane);
-                    if (g.nbr_beg) {
-                        bl = (int64_t)__ldg(((const I *)g.nbr_beg) + beg + lane);
-                        dl = __ldg(g.nbr_deg + beg + lane);
+                    if (g.nrec) {   // one 128-bit record per lane, coalesced
+                        const NbrRec r = load_rec(g.nrec, beg + lane);
+                        ul = r.col;
+                        dl = r.deg;
+                        bl = r.beg;
+                        wl = BIAS == CSAW_BIAS_DEGREE ? __int2float_rn(dl) : edge_bias<I, BIAS>(g, beg + lane);
+                    } else {
+                        wl = edge_bias<I, BIAS>(g, beg + lane);
+                        ul = __ldg(g.v.col + beg + lane);
                     }
                 }
                 // canonical prefix of one tile; the first lane above t is the
@@ -886,7 +929,7 @@ k_walk_fast(DevGraph g, WalkArgs a) {
                 u = __shfl_sync(FULL, ul, idx);
                 nb = __shfl_sync(FULL, bl, idx);
                 nd = __shfl_sync(FULL, dl, idx);
-                have = g.nbr_beg != nullptr;
+                have = g.nrec != nullptr;
                 bytes += (mat ? 4ull : 4ull + 2ull * sizeof(I)) * d + rec * (d - 1);
             } else if (cached) {
                 const float *cp = g.cdf + beg;
@@ -914,10 +957,13 @@ k_walk_fast(DevGraph g, WalkArgs a) {
                 bytes += (mat ? 4ull : 4ull + 2ull * sizeof(I)) * d;
             }
             if (!have) {
-                u = __ldg(g.v.col + e);
-                if (g.nbr_beg) {
-                    nb = (int64_t)__ldg(((const I *)g.nbr_beg) + e);
-                    nd = __ldg(g.nbr_deg + e);
+                if (g.nrec) {
+                    const NbrRec r = load_rec(g.nrec, e);
+                    u = r.col;
+                    nb = r.beg;
+                    nd = r.deg;
+                } else {
+                    u = __ldg(g.v.col + e);
                 }
             }
             int32_t dst = Update(&g.v, u, v);
@@ -925,7 +971,7 @@ k_walk_fast(DevGraph g, WalkArgs a) {
                 if (lane == 0) atomicOr(a.err, ERR_UPDATE_RANGE);
                 dst = 0;
             }
-            if (!g.nbr_beg || dst != u) {
+            if (!g.nrec || dst != u) {
                 nb = row_begin<I>(g, dst);
                 nd = (int32_t)(row_begin<I>(g, dst + 1) - nb);
             }
@@ -998,16 +1044,15 @@ k_walk_thread_fast(DevGraph g, WalkArgs a) {
                         idx = mulhi(b.x, (uint32_t)d);
                     }
                 }
-                const int64_t e = beg + idx;
-                const int32_t u = __ldg(g.v.col + e);
-                dst = Update(&g.v, u, v);
+                const NbrRec r = edge_rec<I>(g, beg + idx);
+                dst = Update(&g.v, r.col, v);
                 if (dst < 0 || dst >= g.v.n_vertices) {
                     atomicOr(a.err, ERR_UPDATE_RANGE);
                     dst = 0;
                 }
                 int64_t nb;
                 int32_t nd;
-                row_of<I>(g, e, u, dst, nb, nd);
+                row_of<I>(g, r, dst, nb, nd);
                 beg = nb;
                 d = nd;
                 ++steps;
@@ -1030,14 +1075,15 @@ k_walk_thread_fast(DevGraph g, WalkArgs a) {
 }
 
 template <typename I>
-__global__ void k_nbr_records(DevGraph g, I *nbeg, int32_t *ndeg) {
+__global__ void k_nbr_records(DevGraph g, NbrRec *rec) {
     const I *r = (const I *)g.v.rowptr;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < g.v.n_edges;
          e += (int64_t)gridDim.x * blockDim.x) {
         const int32_t u = __ldg(g.v.col + e);
         const I b = __ldg(r + u);
-        nbeg[e] = b;
-        ndeg[e] = (int32_t)(__ldg(r + u + 1) - b);
+        const unsigned long long ub = (unsigned long long)(long long)b;
+        reinterpret_cast<int4 *>(rec)[e] =
+            make_int4(u, (int32_t)(__ldg(r + u + 1) - b), (int32_t)(uint32_t)ub, (int32_t)(uint32_t)(ub >> 32));
     }
 }
 

@@ -176,6 +176,8 @@ struct csaw_server_s {
     int64_t submitted = 0, completed = 0, failed = 0, edges = 0;
     std::vector<double> lat_ms, queue_ms, launch_ms, gpu_ms;
     double first_submit = 0, last_done = 0;
+    double max_call_ms = 0;        // longest worker step (launch or completion) since reset
+    int64_t calls_over_1ms = 0;
 };
 
 namespace {
@@ -313,6 +315,13 @@ bool advance(csaw_server_s *s, Slot *sl, int *rc) {
     return true;
 }
 
+// Records the duration of one worker step (under the lock).
+void note_call(csaw_server_s *s, double seconds) {
+    const double ms = seconds * 1e3;
+    if (ms > s->max_call_ms) s->max_call_ms = ms;
+    if (ms > 1.0) ++s->calls_over_1ms;
+}
+
 void worker_main(csaw_server_s *s) {
     cudaSetDevice(s->device);
     std::unique_lock<std::mutex> lk(s->mu);
@@ -332,6 +341,7 @@ void worker_main(csaw_server_s *s) {
             r->t_launched = now_s();
             const std::string err = rc ? csaw_last_error() : "";
             lk.lock();
+            note_call(s, r->t_launched - r->t_admit);
             if (rc) finish(s, &sl, r, rc, err.c_str());
             progressed = true;
         }
@@ -341,6 +351,7 @@ void worker_main(csaw_server_s *s) {
             const cudaError_t q = cudaEventQuery(sl.ev);
             if (q == cudaErrorNotReady) continue;
             lk.unlock();
+            const double t0 = now_s();
             int rc = 0;
             bool done;
             if (q != cudaSuccess) {
@@ -351,7 +362,9 @@ void worker_main(csaw_server_s *s) {
                 done = advance(s, &sl, &rc);
             }
             const std::string err = rc ? csaw_last_error() : "";
+            const double t1 = now_s();
             lk.lock();
+            note_call(s, t1 - t0);
             if (done) finish(s, &sl, sl.req, rc, err.c_str());
             progressed = true;
         }
@@ -529,7 +542,11 @@ extern "C" int csaw_server_get_stats(csaw_server s, int reset, csaw_server_stats
     }
     st.first_submit_s = s->first_submit;
     st.last_done_s = s->last_done;
+    st.max_worker_call_ms = s->max_call_ms;
+    st.worker_calls_over_1ms = s->calls_over_1ms;
     if (reset) {
+        s->max_call_ms = 0;
+        s->calls_over_1ms = 0;
         s->lat_ms.clear();
         s->queue_ms.clear();
         s->launch_ms.clear();
