@@ -676,6 +676,62 @@ __device__ __forceinline__ bool half_select(const Half &h, int N, const DrawCtx 
     return true;
 }
 
+// What the pair kernel stages in shared memory for an item over a cached
+// prefix: its whole prefix row (d <= WF), else the row's entries of the
+// first prefix index level (cdf1, one per 32 edges) when they fit in WF
+// floats, else those of the second level (cdf2, one per 1024 edges), else
+// nothing (rows above ~512 K edges search the global index).
+enum : int { STAGE_NONE = 0, STAGE_ROW = 1, STAGE_CDF1 = 2, STAGE_CDF2 = 3 };
+struct StagePlan {
+    int mode;
+    const float *src;
+    int count;
+};
+
+__device__ __forceinline__ StagePlan stage_plan(const DevGraph &g, int64_t beg, int d) {
+    const int64_t end = beg + d;
+    if (d <= WF) return StagePlan{STAGE_ROW, g.cdf + beg, d};
+    const int64_t ka = beg >> 5, kb = (end - 1) >> 5;
+    if (kb - ka + 1 <= WF) return StagePlan{STAGE_CDF1, g.cdf1 + ka, (int)(kb - ka + 1)};
+    const int64_t ua = beg >> 10, ub = (end - 1) >> 10;
+    if (ub - ua + 1 <= WF) return StagePlan{STAGE_CDF2, g.cdf2 + ua, (int)(ub - ua + 1)};
+    return StagePlan{STAGE_NONE, nullptr, 0};
+}
+
+// cdf_search with the plan's index level staged in S (shared): the same
+// index (the first i with P[i] > t is unique), the staged level searched in
+// shared memory, the rest in global memory one 128-byte line per level.
+// As in cdf_search, no level probes its last candidate.
+__device__ __forceinline__ int64_t staged_cdf_search(const DevGraph &g, const StagePlan &sp, const float *S,
+                                                     int64_t beg, int64_t d, float t) {
+    const int64_t end = beg + d;
+    if (sp.mode == STAGE_NONE) return cdf_search(g, beg, d, t);
+    int64_t k;
+    if (sp.mode == STAGE_CDF1) {
+        k = (beg >> 5) + search_upper32(S, sp.count, t);
+    } else {
+        const int64_t u = (beg >> 10) + search_upper32(S, sp.count, t);
+        const int64_t ka = (u << 5) > (beg >> 5) ? (u << 5) : (beg >> 5);
+        const int64_t kb = (u << 5) + 31 < ((end - 1) >> 5) ? (u << 5) + 31 : ((end - 1) >> 5);
+        k = ka + search_upper(g.cdf1 + ka, kb - ka + 1, t);
+    }
+    const int64_t ia = (k << 5) > beg ? (k << 5) : beg;
+    const int64_t ib = (k << 5) + 31 < end - 1 ? (k << 5) + 31 : end - 1;
+    return ia + search_upper(g.cdf + ia, ib - ia + 1, t) - beg;
+}
+
+// Counted bytes of the prefix reads of one item (4 bytes per element staged
+// or probed): the staged entries, plus per draw the probes of the levels
+// searched in global memory (a 32-entry line: 5 probes each).
+__device__ __forceinline__ unsigned long long staged_bytes(const StagePlan &sp, int64_t d, int N) {
+    switch (sp.mode) {
+        case STAGE_ROW: return 4ull * d;
+        case STAGE_CDF1: return 4ull * sp.count + (unsigned long long)N * 4ull * 5;
+        case STAGE_CDF2: return 4ull * sp.count + (unsigned long long)N * 4ull * 10;
+        default: return (unsigned long long)N * 4ull * (64 - __clzll((unsigned long long)d));
+    }
+}
+
 // Level expansion, part 2 for items over a cached prefix with N <= 16 and
 // d >= 4N (a rebuild is rare): two items per warp, one per half-warp, lanes
 // N..15 of a half idle instead of N..31 of a warp.  Rows up to WF edges are
@@ -709,11 +765,12 @@ k_select_pair(DevGraph g, LevelArgs a) {
     const int nout = 2 + (a.o_smp != nullptr) + (a.o_dep != nullptr);
     unsigned long long my_bytes = 0, my_items = 0;
     uint32_t parity = 0;
-    // requests the staged copy of a row (rows up to WF only); returns the
-    // row's offset in the buffer
+    // requests the staged copy of what an item searches (stage_plan); returns
+    // the copy's offset in the buffer
     auto request = [&](long long rbeg, int rd) -> int {
-        if (rd > WF) return 0;
-        const RowWindow w = row_window(g.cdf + rbeg, rd);
+        const StagePlan sp = stage_plan(g, rbeg, rd);
+        if (sp.mode == STAGE_NONE) return 0;
+        const RowWindow w = row_window(sp.src, sp.count);
         if (h.sl == 0) {
             fence_async_smem();   // this half's reads of buf precede the copy's writes
             bulk_load(buf, w.start, w.bytes, bar);
@@ -737,25 +794,27 @@ k_select_pair(DevGraph g, LevelArgs a) {
         const bool rec = a.sched && a.sched->mode == SCHED_RECORD;
         long long t0 = 0;
         if (rec) t0 = clock64();
+        const StagePlan sp = stage_plan(g, beg, (int)d);
+        if (sp.mode != STAGE_NONE && !mbar_wait(bar, parity)) {   // bounded: report instead of spinning on
+            if (h.sl == 0) atomicOr(a.err, ERR_COPY_WAIT);
+            mbar_wait(bar, parity);                                 // let the copy in flight land first
+            break;
+        }
+        if (sp.mode != STAGE_NONE) parity ^= 1u;
+        const float *S = buf + off;   // the staged row or index entries
         int sel;
         bool ok;
-        if (d <= WF) {
-            if (!mbar_wait(bar, parity)) {   // bounded: report instead of spinning on
-                if (h.sl == 0) atomicOr(a.err, ERR_COPY_WAIT);
-                mbar_wait(bar, parity);       // let the copy in flight land before leaving
-                break;
-            }
-            parity ^= 1u;
-            const float *P = buf + off;
+        if (sp.mode == STAGE_ROW) {
             const int dd = (int)d;
-            const float T = P[dd - 1];
-            ok = half_select(h, N, dc, T, [&](uint32_t x) { return search_upper32(P, dd, its_target(x, T)); }, sel);
-            __syncwarp(h.mask);   // every read of this row is done: the buffer is free
+            const float T = S[dd - 1];
+            ok = half_select(h, N, dc, T, [&](uint32_t x) { return search_upper32(S, dd, its_target(x, T)); }, sel);
         } else {
             const float T = __ldg(g.cdf + beg + d - 1);
-            ok = half_select(h, N, dc, T, [&](uint32_t x) { return (int)cdf_search(g, beg, d, its_target(x, T)); },
+            ok = half_select(h, N, dc, T, [&](uint32_t x) { return (int)staged_cdf_search(g, sp, S, beg, d,
+                                                                                          its_target(x, T)); },
                              sel);
         }
+        __syncwarp(h.mask);   // every read of the buffer is done: it is free
         if (inext < n) off = request(nbeg, nd);
         if (!ok) {   // rebuild needed: a whole warp redoes the item (in shared memory up to WF)
             if (h.sl == 0) {
@@ -774,7 +833,7 @@ k_select_pair(DevGraph g, LevelArgs a) {
         }
         if (h.sl == 0) {
             my_items++;
-            const unsigned long long row = d <= WF ? 4ull * d : (unsigned long long)N * 4ull * (64 - __clzll(d));
+            const unsigned long long row = staged_bytes(sp, d, N);
             my_bytes += 16 + row + (unsigned long long)N * (4ull + 4ull * nout +
                                                             (a.push ? 12ull + 2 * (sizeof(I) + 4) : 0ull));
         }
