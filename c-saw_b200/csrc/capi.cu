@@ -293,6 +293,7 @@ int ensure_nbr(csaw_graph_s *g, cudaStream_t st) {
 }
 
 constexpr int64_t CDF_BIG = 4096;   // vertices above are built by one CTA each
+constexpr int RETRY_SMEM_BYTES = 96 << 10;   // dynamic shared memory of the cached-hub retry pass
 
 // Per-vertex CDF cache: the canonical prefix of every vertex's biases for bias
 // kind BIAS (4E bytes, plus its search index), built on first biased use by a
@@ -550,6 +551,14 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
     }
     const DevGraph dg = dev_view(g, p->schedule, BIAS);
     const uint64_t seed = p->seed;
+    if (!plain && cached && g->maxdeg > WF) {
+        static uint64_t smem_set = 0;   // per instantiation: bit = device
+        if (g->device < 64 && !((smem_set >> g->device) & 1u)) {
+            CK(cudaFuncSetAttribute(k_expand_heavy<I, BIAS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    RETRY_SMEM_BYTES));
+            smem_set |= 1ull << g->device;
+        }
+    }
     const int grid = plain ? grid_for(k_expand_warp<I, BIAS>, EXPAND_THREADS, 0, g->sm_count)
                            : shaped(grid_for(k_coop_fast<I, BIAS>, FAST_THREADS, 0, g->sm_count));
     for (int64_t s0 = 0; s0 < S; s0 += B) {
@@ -611,6 +620,7 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
             a.n_retry = &c->ctr->n_retry;
             a.heavy_scratch = (float *)c->hscratch.p;
             a.heavy_stride = hstride;
+            a.heavy_smem = 0;   // only the retry launch below has dynamic shared memory
             a.o_src = o.src;
             a.o_dst = o.dst;
             a.o_smp = o.smp;
@@ -657,7 +667,9 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
                 if (cached) k_select_fast<I, BIAS, true><<<sgrid, FAST_THREADS, 0, st>>>(dg, a);
                 else k_select_fast<I, BIAS, false><<<sgrid, FAST_THREADS, 0, st>>>(dg, a);
             }
-            if (!plain && cached && g->maxdeg > WF) {
+            // with the pair list, every cached hub (d > WF >= 4N) is paired:
+            // the hub list stays empty
+            if (!plain && cached && g->maxdeg > WF && !paired) {
                 LaunchScope ls(g, KK_HUB, st);
                 k_select_hub<I, BIAS><<<hgrid, FAST_THREADS, 0, st>>>(dg, a);
             }
@@ -682,8 +694,9 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
                 ar.heavy_list = (SelEntry *)c->retry.p;
                 ar.n_heavy = &c->ctr->n_retry;
                 ar.cta_class = 1;
+                ar.heavy_smem = RETRY_SMEM_BYTES / 4;   // rows up to ~22 K edges rebuild in shared memory
                 LaunchScope ls(g, KK_HEAVY, st);
-                k_expand_heavy<I, BIAS><<<cta_grid[1], 256, 0, st>>>(dg, ar);
+                k_expand_heavy<I, BIAS><<<cta_grid[1], 256, RETRY_SMEM_BYTES, st>>>(dg, ar);
             }
             if (side) CK(cudaStreamWaitEvent(st, c->join, 0));
             if (dedup && l + 1 < D) TRY(dedup_level(nxt, l + 1));

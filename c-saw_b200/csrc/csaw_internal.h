@@ -94,6 +94,7 @@ struct LevelArgs {
     const SchedArgs *sched;   // learned scheduler, or null (degree rule)
     float *heavy_scratch;     // per-CTA scratch for the heavy kernel
     int64_t heavy_stride;     // floats per CTA
+    int64_t heavy_smem;       // floats of dynamic shared memory the heavy launch has (0: none)
     int32_t *o_src, *o_dst, *o_smp, *o_dep;
     unsigned long long *o_count;
     int64_t cap;

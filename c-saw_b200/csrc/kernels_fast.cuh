@@ -25,6 +25,10 @@
 namespace csaw {
 
 constexpr int WF = 512;  // per-warp shared prefix capacity of the fast kernels
+// Resident CTAs per SM the pair kernel is compiled for (register budget).
+#ifndef CSAW_PAIR_MIN_BLOCKS
+#define CSAW_PAIR_MIN_BLOCKS 4
+#endif
 constexpr int FAST_THREADS = 256;
 
 // Canonical prefix of a single tile held one element per lane (w = 0 for
@@ -743,7 +747,7 @@ __device__ __forceinline__ unsigned long long staged_bytes(const StagePlan &sp, 
 // redone from scratch: rows up to WF by k_select_fast on the refill list
 // (written over the consumed warp list), larger ones by the CTA pass.
 template <typename I, int BIAS>
-__global__ void __launch_bounds__(FAST_THREADS, 4)
+__global__ void __launch_bounds__(FAST_THREADS, CSAW_PAIR_MIN_BLOCKS)
 k_select_pair(DevGraph g, LevelArgs a) {
     constexpr int NH = FAST_THREADS / 16;
     constexpr int ROW = WF + 4;   // floats: a row of up to WF plus its 16-byte alignment window

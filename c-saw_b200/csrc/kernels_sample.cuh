@@ -246,15 +246,23 @@ k_expand_warp(DevGraph g0, LevelArgs a) {
 }
 
 // ------------------------------------------------ high-degree expansion
+// Floats of prefix scratch a CTA rebuild of a degree-d row needs: the
+// prefix, tile sums, group carries and the exclusion bitmap.
+__host__ __device__ __forceinline__ int64_t heavy_need(int64_t d) {
+    return d + (d >> 5) + (d >> 10) + (d >> 5) + 8;
+}
+
 // One CTA per deferred item: the canonical prefix is built by the whole CTA in
+// shared memory when the launch has room for the row (a.heavy_smem), else in
 // global scratch (same canonical order, so bit-identical to the warp path);
 // warp 0 runs the slot resolver; every rebuild is a CTA-wide rescan.
 template <typename I, int BIAS, bool STREAM = false>
 __global__ void __launch_bounds__(1024)
 k_expand_heavy(DevGraph g0, LevelArgs a) {
     __shared__ int s_flag, s_j;
+    extern __shared__ float s_heavy[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    float *P = a.heavy_scratch + (int64_t)blockIdx.x * a.heavy_stride;
+    float *const P_global = a.heavy_scratch + (int64_t)blockIdx.x * a.heavy_stride;
     const uint32_t nh = *a.n_heavy;
     unsigned long long my_bytes = 0, my_items = 0;
     for (uint32_t h = blockIdx.x; h < nh; h += gridDim.x) {
@@ -276,10 +284,12 @@ k_expand_heavy(DevGraph g0, LevelArgs a) {
         const uint32_t p = a.in_p[it];
         const int64_t beg = row_begin<I>(g, v);
         const int64_t d = row_begin<I>(g, v + 1) - beg;
-        if (d + (d >> 5) + (d >> 10) + (d >> 5) + 8 > a.heavy_stride) {
+        const bool in_smem = heavy_need(d) <= a.heavy_smem;
+        if (!in_smem && heavy_need(d) > a.heavy_stride) {
             if (threadIdx.x == 0) atomicOr(a.err, ERR_SCRATCH);
             continue;
         }
+        float *P = in_smem ? s_heavy : P_global;
         float *tsum = P + d;
         float *gcar = tsum + (d >> 5) + 1;
         uint32_t *zb = (uint32_t *)(gcar + (d >> 10) + 1);
