@@ -34,6 +34,7 @@ OPT_SCHED_RECORD = 2
 OPT_GRID_PCT = 3
 OPT_PAIR = 4
 OPT_HOST_PARTS = 5
+OPT_RETRY_SMEM = 6
 MLP_NPARAM, MLP_NORM = 1542, 18
 
 

@@ -155,6 +155,7 @@ struct csaw_graph_s {
     int grid_pct = 100;           // CSAW_OPT_GRID_PCT
     bool pair = true;             // CSAW_OPT_PAIR
     int host_parts = 0;           // CSAW_OPT_HOST_PARTS (0: by output size; -1: copy after the job)
+    int retry_smem = 0;           // CSAW_OPT_RETRY_SMEM (bytes)
     uint32_t class_mask = 0x3f;   // classes the trained model picks (bit c)
     int32_t *big_verts = nullptr; // vertices above CDF_BIG (the cache builds them one CTA each)
     int64_t n_big = 0;
@@ -293,7 +294,7 @@ int ensure_nbr(csaw_graph_s *g, cudaStream_t st) {
 }
 
 constexpr int64_t CDF_BIG = 4096;   // vertices above are built by one CTA each
-constexpr int RETRY_SMEM_BYTES = 96 << 10;   // dynamic shared memory of the cached-hub retry pass
+constexpr int RETRY_SMEM_MAX = 96 << 10;   // CSAW_OPT_RETRY_SMEM upper bound (bytes)
 
 // Per-vertex CDF cache: the canonical prefix of every vertex's biases for bias
 // kind BIAS (4E bytes, plus its search index), built on first biased use by a
@@ -555,7 +556,7 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
         static uint64_t smem_set = 0;   // per instantiation: bit = device
         if (g->device < 64 && !((smem_set >> g->device) & 1u)) {
             CK(cudaFuncSetAttribute(k_expand_heavy<I, BIAS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    RETRY_SMEM_BYTES));
+                                    RETRY_SMEM_MAX));
             smem_set |= 1ull << g->device;
         }
     }
@@ -694,9 +695,9 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
                 ar.heavy_list = (SelEntry *)c->retry.p;
                 ar.n_heavy = &c->ctr->n_retry;
                 ar.cta_class = 1;
-                ar.heavy_smem = RETRY_SMEM_BYTES / 4;   // rows up to ~22 K edges rebuild in shared memory
+                ar.heavy_smem = g->retry_smem / 4;   // rows whose rebuild fits use shared memory
                 LaunchScope ls(g, KK_HEAVY, st);
-                k_expand_heavy<I, BIAS><<<cta_grid[1], 256, RETRY_SMEM_BYTES, st>>>(dg, ar);
+                k_expand_heavy<I, BIAS><<<cta_grid[1], 256, g->retry_smem, st>>>(dg, ar);
             }
             if (side) CK(cudaStreamWaitEvent(st, c->join, 0));
             if (dedup && l + 1 < D) TRY(dedup_level(nxt, l + 1));
@@ -1613,6 +1614,11 @@ extern "C" int csaw_graph_set_option(csaw_graph g, int option, int64_t value) {
         case CSAW_OPT_HOST_PARTS:
             if (value < -1 || value > MAX_HOST_PARTS) return fail(CSAW_ERR_INVALID, "host parts must be in [-1, 8]");
             g->host_parts = (int)value;
+            return 0;
+        case CSAW_OPT_RETRY_SMEM:
+            if (value < 0 || value > RETRY_SMEM_MAX) return fail(CSAW_ERR_INVALID, "retry shared memory must be in [0, 98304]");
+            g->retry_smem = (int)(value & ~15ll);
+            ++g_alloc_epoch;   // launch shapes are baked into cached graphs
             return 0;
         default:
             return fail(CSAW_ERR_INVALID, "unknown option");

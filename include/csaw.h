@@ -221,7 +221,13 @@ enum {
      * edges and each range has 16384 samples (walks: 256 per SM), else 1;
      * -1: one range, copied back after all of its sampling.  Never changes
      * the edge multiset. */
-    CSAW_OPT_HOST_PARTS = 5
+    CSAW_OPT_HOST_PARTS = 5,
+    /* Bytes of shared memory (0..98304, default 0) the CTA pass that retries
+     * cached hub items may use to rebuild a row's prefix: rows whose
+     * rebuild fits are done in shared memory, larger ones in global scratch.
+     * More shared memory means fewer resident CTAs; never changes the
+     * output. */
+    CSAW_OPT_RETRY_SMEM = 6
 };
 int csaw_graph_set_option(csaw_graph g, int option, int64_t value);
 
@@ -356,6 +362,10 @@ typedef struct {
     double p99_launch_ms;          /* admitted -> kernels enqueued (host) */
     double p99_gpu_ms;             /* enqueued -> edge count read back */
     double first_submit_s, last_done_s;               /* steady clock, seconds */
+    double max_worker_call_ms;     /* longest single launch or completion step of the
+                                      worker thread since reset: a host-side stall
+                                      (a blocking CUDA call) shows here */
+    int64_t worker_calls_over_1ms; /* such steps longer than 1 ms since reset */
 } csaw_server_stats;
 int csaw_server_create(csaw_graph g, const csaw_server_config *cfg, csaw_server *out);
 /* Waits for every submitted request, then frees the server. */

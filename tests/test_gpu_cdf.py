@@ -164,3 +164,22 @@ def test_many_biased_walks_thread_per_walk(csaw, rmat12_pareto, powerlaw_small, 
         assert len(a[0]) > n
         assert_parity(a, b)
         G.close()
+
+
+@pytest.mark.parametrize("retry_smem", [16384, 98304])
+@pytest.mark.parametrize("bias", [1, 2])
+def test_retry_rebuild_in_shared_memory(csaw, skewed_hubs, retry_smem, bias):
+    """The cached-hub retry pass rebuilding prefixes in shared memory
+    (CSAW_OPT_RETRY_SMEM) gives the oracle's edges, for rows that fit and
+    rows that do not."""
+    from csaw import _lib
+    g = skewed_hubs
+    G = csaw.Graph(g)
+    G.set_option(_lib.OPT_RETRY_SMEM, retry_smem)
+    hubs = np.repeat(np.arange(len(HUB_DEGREES), dtype=np.int32), 24)
+    seeds = np.concatenate([hubs, oracle.make_seeds(g.rowptr, 400 - hubs.size, 5)]).astype(np.int32)
+    fan = [32, 32, 4]
+    a = run_gpu(csaw, G, 0, bias, 400, 1, fan, 0xC0FFEE, seeds, 1)
+    b = run_oracle(g, 0, bias, 400, 1, fan, 0xC0FFEE, seeds)
+    assert_parity(a, b)
+    G.close()
