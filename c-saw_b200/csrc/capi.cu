@@ -23,6 +23,7 @@
 #include "csaw.h"
 #include "csaw_internal.h"
 #include "kernels_fast.cuh"
+#include "kernels_persist.cuh"
 #include "sched_mlp.cuh"
 
 using namespace csaw;
@@ -53,7 +54,7 @@ int fail(int code, const std::string &msg) {
     } while (0)
 
 enum { KK_EXPAND = 0, KK_HEAVY = 1, KK_WALK = 2, KK_MDRW = 3, KK_INIT = 4, KK_SELECT = 5, KK_HUB = 6, KK_PAIR = 7,
-       KK_WALK_THREAD = 8, KK_COUNT = 9 };
+       KK_WALK_THREAD = 8, KK_PERSIST = 9, KK_COUNT = 10 };
 
 struct Counters {
     unsigned long long out_count;
@@ -118,7 +119,8 @@ constexpr size_t MAX_WARM = 1024;                   // batch keys remembered for
 // Job 0 serves csaw_sample; csaw_sample_batch runs job i on context i, each
 // on its own stream, so independent jobs overlap on the device.
 struct JobCtx {
-    DevBuf q[2][5], heavy, sel, hlist, hscratch, wscratch, seeds_in, out_dev, cta[4], retry, stab, hubsel, pairsel, dedup;
+    DevBuf q[2][5], heavy, sel, hlist, hscratch, wscratch, seeds_in, out_dev, cta[4], retry, stab, hubsel, pairsel, dedup,
+        pctr;   // per-level counters and barrier words of a persistent job
     Counters *ctr = nullptr, *hctr = nullptr;
     cudaStream_t stream = nullptr;   // owned (batch jobs); job 0 uses the caller's
     cudaEvent_t done = nullptr;
@@ -156,6 +158,7 @@ struct csaw_graph_s {
     bool pair = true;             // CSAW_OPT_PAIR
     int host_parts = 0;           // CSAW_OPT_HOST_PARTS (0: by output size; -1: copy after the job)
     int retry_smem = 0;           // CSAW_OPT_RETRY_SMEM (bytes)
+    bool persistent = false;      // CSAW_OPT_PERSISTENT
     uint32_t class_mask = 0x3f;   // classes the trained model picks (bit c)
     int32_t *big_verts = nullptr; // vertices above CDF_BIG (the cache builds them one CTA each)
     int64_t n_big = 0;
@@ -562,6 +565,86 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
     }
     const int grid = plain ? grid_for(k_expand_warp<I, BIAS>, EXPAND_THREADS, 0, g->sm_count)
                            : shaped(grid_for(k_coop_fast<I, BIAS>, FAST_THREADS, 0, g->sm_count));
+    // Persistent job kernel: every level in one cooperative launch (batched
+    // degree-rule jobs over a cached prefix, or unbiased; not with dedup,
+    // learned routing or more than PERSIST_MAX_LEVELS levels).
+    int jgrid = 0;
+    bool persist = !plain && g->persistent && !dedup && D <= PERSIST_MAX_LEVELS &&
+                   (!sched || g->sched_host.mode == SCHED_THRESHOLD) && (!BIASED || cached);
+    if (persist) {
+        static uint64_t attr_set = 0;   // per instantiation: bit = device
+        if (g->device < 64 && !((attr_set >> g->device) & 1u)) {
+            CK(cudaFuncSetAttribute(k_persist<I, BIAS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)PERSIST_SMEM));
+            attr_set |= 1ull << g->device;
+        }
+        int per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persist<I, BIAS>, FAST_THREADS, PERSIST_SMEM));
+        jgrid = per_sm * g->sm_count;   // all CTAs resident (cooperative launch)
+        const bool retries = cached && g->maxdeg > WF;
+        if (jgrid < 1 || (retries && (int64_t)jgrid * hstride * 4 > SCRATCH_BUDGET)) persist = false;
+        if (persist) {
+            TRY(ensure(c->pctr, sizeof(PersistLevelCtr) * PERSIST_MAX_LEVELS + sizeof(unsigned) * 3 * PERSIST_MAX_LEVELS,
+                       st));
+            if (retries) TRY(ensure(c->hscratch, sizeof(float) * hstride * (size_t)std::max(hblocks, jgrid), st));
+        }
+    }
+    // Launch arguments of level l (queues ping-pong by level parity).
+    auto make_level = [&](int l) {
+        const int cur = l & 1, nxt = cur ^ 1;
+        LevelArgs a;
+        a.in_dep = nullptr;   // every item of this level is at depth l
+        a.out_dep = nullptr;
+        a.D = D;
+        a.in_v = (const int32_t *)c->q[cur][0].p;
+        a.in_s = (const int32_t *)c->q[cur][1].p;
+        a.in_p = (const uint32_t *)c->q[cur][2].p;
+        a.n_in = &c->ctr->nq[cur];
+        a.out_v = (int32_t *)c->q[nxt][0].p;
+        a.out_s = (int32_t *)c->q[nxt][1].p;
+        a.out_p = (uint32_t *)c->q[nxt][2].p;
+        a.n_out = &c->ctr->nq[nxt];
+        a.in_beg = plain ? nullptr : c->q[cur][3].p;
+        a.in_deg = plain ? nullptr : (const int32_t *)c->q[cur][4].p;
+        a.out_beg = plain ? nullptr : c->q[nxt][3].p;
+        a.out_deg = plain ? nullptr : (int32_t *)c->q[nxt][4].p;
+        a.heavy = (uint32_t *)c->heavy.p;
+        a.n_heavy = &c->ctr->n_heavy;
+        a.sel_list = plain ? nullptr : (SelEntry *)c->sel.p;
+        a.n_sel = &c->ctr->n_sel;
+        a.heavy_list = nullptr;
+        for (int k = 0; k < 4; ++k) a.cta_list[k] = (SelEntry *)c->cta[k].p;
+        a.n_cta = c->ctr->n_cta;
+        a.sched = sched;
+        a.sched_tab = tabled ? (const uint8_t *)c->stab.p : nullptr;
+        a.hub_list = (SelEntry *)c->hubsel.p;
+        a.n_hub = &c->ctr->n_hub;
+        const bool paired = !plain && cached && g->maxdeg > WF && fan[l] <= 16 && g->pair;
+        a.pair_list = paired ? (SelEntry *)c->pairsel.p : nullptr;
+        a.n_pair = &c->ctr->n_pair;
+        a.refill_list = (SelEntry *)c->sel.p;   // free once k_select_fast has run
+        a.n_refill = &c->ctr->n_refill;
+        a.retry_list = (SelEntry *)c->retry.p;
+        a.n_retry = &c->ctr->n_retry;
+        a.heavy_scratch = (float *)c->hscratch.p;
+        a.heavy_stride = hstride;
+        a.heavy_smem = 0;   // only the retry launch below has dynamic shared memory
+        a.o_src = o.src;
+        a.o_dst = o.dst;
+        a.o_smp = o.smp;
+        a.o_dep = o.dep;
+        a.o_count = o.count;
+        a.cap = o.cap;
+        a.bytes = c->ctr->bytes;
+        a.items = c->ctr->items;
+        a.err = &c->ctr->err;
+        a.k0 = (uint32_t)seed;
+        a.k1 = (uint32_t)(seed >> 32);
+        a.depth = l;
+        a.N = fan[l];
+        a.push = l + 1 < D;
+        return a;
+    };
     for (int64_t s0 = 0; s0 < S; s0 += B) {
         const int64_t nb = (S - s0 < B) ? S - s0 : B;
         const uint32_t n0 = (uint32_t)(nb * F);
@@ -577,6 +660,56 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
                     (uint32_t *)c->q[0][2].p, (I *)c->q[0][3].p, (int32_t *)c->q[0][4].p, &c->ctr->nq[0],
                     &c->ctr->err);
         }
+        if (persist) {
+            PersistArgs pa{};
+            PersistLevelCtr *pc = (PersistLevelCtr *)c->pctr.p;
+            CK(cudaMemsetAsync(c->pctr.p, 0, c->pctr.n, st));
+            const bool retries = cached && g->maxdeg > WF;
+            for (int l = 0; l < D; ++l) {
+                LevelArgs a = make_level(l);
+                a.n_in = l == 0 ? &c->ctr->nq[0] : &pc[l - 1].n_out;
+                a.n_out = &pc[l].n_out;
+                a.n_heavy = &pc[l].n_heavy;
+                a.n_sel = &pc[l].n_sel;
+                a.n_cta = pc[l].n_cta;
+                a.n_retry = &pc[l].n_retry;
+                a.n_hub = &pc[l].n_hub;
+                a.n_pair = &pc[l].n_pair;
+                a.n_refill = &pc[l].n_refill;
+                a.refill_list = (SelEntry *)c->cta[1].p;   // the warp list is still being read beside the pair pass
+                pa.lv[l] = a;
+                LevelArgs ar = a;
+                ar.sel_list = a.refill_list;
+                ar.n_sel = a.n_refill;
+                pa.refill[l] = ar;
+                LevelArgs at = a;
+                at.heavy_list = (SelEntry *)c->retry.p;
+                at.n_heavy = a.n_retry;
+                at.cta_class = 1;
+                at.heavy_smem = 0;
+                pa.retry[l] = at;
+                uint32_t f = 0;
+                if (retries) f |= (a.pair_list ? PF_PAIR : PF_HUB) | PF_RETRY;
+                pa.flags[l] = f;
+                pa.posts[l] = (c->posting && l + 1 < D && c->n_posts < MAX_POSTS) ? &c->posts[c->n_posts++] : nullptr;
+            }
+            pa.D = D;
+            pa.arrive = (unsigned *)(pc + PERSIST_MAX_LEVELS);
+            pa.err = &c->ctr->err;
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3((unsigned)jgrid);
+            cfg.blockDim = dim3(FAST_THREADS);
+            cfg.dynamicSmemBytes = PERSIST_SMEM;
+            cfg.stream = st;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeCooperative;
+            attr[0].val.cooperative = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            LaunchScope ls(g, KK_PERSIST, st);
+            CK(cudaLaunchKernelEx(&cfg, k_persist<I, BIAS>, dg, pa));
+            continue;
+        }
         if (dedup) {
             CK(cudaMemsetAsync(dkeys, 0xff, 16 * (size_t)(dmask + 1), st));
             TRY(dedup_level(0, 0));
@@ -585,57 +718,7 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
             const int cur = l & 1, nxt = cur ^ 1;
             CK(cudaMemsetAsync(&c->ctr->nq[nxt], 0, sizeof(uint32_t), st));
             CK(cudaMemsetAsync(&c->ctr->n_heavy, 0, 10 * sizeof(uint32_t), st));  // n_heavy .. n_refill
-            LevelArgs a;
-            a.in_dep = nullptr;   // every item of this level is at depth l
-            a.out_dep = nullptr;
-            a.D = D;
-            a.in_v = (const int32_t *)c->q[cur][0].p;
-            a.in_s = (const int32_t *)c->q[cur][1].p;
-            a.in_p = (const uint32_t *)c->q[cur][2].p;
-            a.n_in = &c->ctr->nq[cur];
-            a.out_v = (int32_t *)c->q[nxt][0].p;
-            a.out_s = (int32_t *)c->q[nxt][1].p;
-            a.out_p = (uint32_t *)c->q[nxt][2].p;
-            a.n_out = &c->ctr->nq[nxt];
-            a.in_beg = plain ? nullptr : c->q[cur][3].p;
-            a.in_deg = plain ? nullptr : (const int32_t *)c->q[cur][4].p;
-            a.out_beg = plain ? nullptr : c->q[nxt][3].p;
-            a.out_deg = plain ? nullptr : (int32_t *)c->q[nxt][4].p;
-            a.heavy = (uint32_t *)c->heavy.p;
-            a.n_heavy = &c->ctr->n_heavy;
-            a.sel_list = plain ? nullptr : (SelEntry *)c->sel.p;
-            a.n_sel = &c->ctr->n_sel;
-            a.heavy_list = nullptr;
-            for (int k = 0; k < 4; ++k) a.cta_list[k] = (SelEntry *)c->cta[k].p;
-            a.n_cta = c->ctr->n_cta;
-            a.sched = sched;
-            a.sched_tab = tabled ? (const uint8_t *)c->stab.p : nullptr;
-            a.hub_list = (SelEntry *)c->hubsel.p;
-            a.n_hub = &c->ctr->n_hub;
-            const bool paired = !plain && cached && g->maxdeg > WF && fan[l] <= 16 && g->pair;
-            a.pair_list = paired ? (SelEntry *)c->pairsel.p : nullptr;
-            a.n_pair = &c->ctr->n_pair;
-            a.refill_list = (SelEntry *)c->sel.p;   // free once k_select_fast has run
-            a.n_refill = &c->ctr->n_refill;
-            a.retry_list = (SelEntry *)c->retry.p;
-            a.n_retry = &c->ctr->n_retry;
-            a.heavy_scratch = (float *)c->hscratch.p;
-            a.heavy_stride = hstride;
-            a.heavy_smem = 0;   // only the retry launch below has dynamic shared memory
-            a.o_src = o.src;
-            a.o_dst = o.dst;
-            a.o_smp = o.smp;
-            a.o_dep = o.dep;
-            a.o_count = o.count;
-            a.cap = o.cap;
-            a.bytes = c->ctr->bytes;
-            a.items = c->ctr->items;
-            a.err = &c->ctr->err;
-            a.k0 = (uint32_t)seed;
-            a.k1 = (uint32_t)(seed >> 32);
-            a.depth = l;
-            a.N = fan[l];
-            a.push = l + 1 < D;
+            LevelArgs a = make_level(l);
             if (tabled) {
                 LaunchScope ls(g, KK_INIT, st);
                 k_sched_table<<<TAB_N * 32 / 256, 256, 0, st>>>(sched, a.n_in, a.N, l, (uint8_t *)c->stab.p);
@@ -670,7 +753,7 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
             }
             // with the pair list, every cached hub (d > WF >= 4N) is paired:
             // the hub list stays empty
-            if (!plain && cached && g->maxdeg > WF && !paired) {
+            if (!plain && cached && g->maxdeg > WF && !a.pair_list) {
                 LaunchScope ls(g, KK_HUB, st);
                 k_select_hub<I, BIAS><<<hgrid, FAST_THREADS, 0, st>>>(dg, a);
             }
@@ -969,6 +1052,8 @@ int finish_job(csaw_graph_s *g, JobCtx *c, int64_t cap, int64_t *n_out) {
     *n_out = (int64_t)k.out_count;
     if (k.err & ERR_SEED_RANGE) return fail(CSAW_ERR_INVALID, "a seed vertex is out of range");
     if (k.err & ERR_UPDATE_RANGE) return fail(CSAW_ERR_DEVICE, "Update() returned a vertex out of range");
+    if (k.err & ERR_BARRIER)
+        return fail(CSAW_ERR_DEVICE, "a grid barrier of the persistent job kernel expired (bounded wait)");
     if (k.err & ERR_COPY_WAIT)
         return fail(CSAW_ERR_DEVICE, "an asynchronous row copy did not complete within its bounded wait");
     if (k.err) return fail(CSAW_ERR_DEVICE, "kernel error flag " + std::to_string(k.err));
@@ -1614,6 +1699,10 @@ extern "C" int csaw_graph_set_option(csaw_graph g, int option, int64_t value) {
         case CSAW_OPT_HOST_PARTS:
             if (value < -1 || value > MAX_HOST_PARTS) return fail(CSAW_ERR_INVALID, "host parts must be in [-1, 8]");
             g->host_parts = (int)value;
+            return 0;
+        case CSAW_OPT_PERSISTENT:
+            g->persistent = value != 0;
+            ++g_alloc_epoch;   // launch structure is baked into cached graphs
             return 0;
         case CSAW_OPT_RETRY_SMEM:
             if (value < 0 || value > RETRY_SMEM_MAX) return fail(CSAW_ERR_INVALID, "retry shared memory must be in [0, 98304]");

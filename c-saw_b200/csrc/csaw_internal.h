@@ -149,6 +149,6 @@ struct WalkArgs {
     uint32_t k0, k1;
 };
 
-enum : int { ERR_SEED_RANGE = 1, ERR_UPDATE_RANGE = 2, ERR_SCRATCH = 4, ERR_COPY_WAIT = 8 };
+enum : int { ERR_SEED_RANGE = 1, ERR_UPDATE_RANGE = 2, ERR_SCRATCH = 4, ERR_COPY_WAIT = 8, ERR_BARRIER = 16 };
 
 }  // namespace csaw

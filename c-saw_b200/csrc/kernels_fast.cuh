@@ -401,13 +401,12 @@ __device__ __forceinline__ void emit_edge(const DevGraph &g, const LevelArgs &a,
 // (d <= N) expanded cooperatively, items needing a draw appended with their
 // reserved slots to the warp list (or the CTA list when biased and d > WF).
 template <typename I, int BIAS>
-__global__ void __launch_bounds__(FAST_THREADS)
-k_coop_fast(DevGraph g, LevelArgs a) {
+__device__ __forceinline__ void coop_body(const DevGraph &g, const LevelArgs &a) {
     constexpr bool BIASED = BIAS != CSAW_BIAS_UNBIASED;
     const int lane = threadIdx.x & 31;
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t n = *a.n_in;
+    const uint32_t n = __ldcg(a.n_in);
     const int N = a.N;
     const bool cached = BIASED && g.cdf && g.cdf_bias == BIAS;
     const bool routed = BIASED && a.sched && a.sched->mode != SCHED_THRESHOLD;
@@ -423,11 +422,11 @@ k_coop_fast(DevGraph g, LevelArgs a) {
         uint32_t p = 0;
         int64_t beg = 0, d = 0;
         if (valid) {
-            v = a.in_v[it];
-            s = a.in_s[it];
-            p = a.in_p[it];
-            beg = (int64_t)((const I *)a.in_beg)[it];
-            d = a.in_deg[it];
+            v = __ldcg(a.in_v + it);
+            s = __ldcg(a.in_s + it);
+            p = __ldcg(a.in_p + it);
+            beg = (int64_t)__ldcg((const I *)a.in_beg + it);
+            d = __ldcg(a.in_deg + it);
         }
         const int k = (valid && d > 0) ? (int)(d < N ? d : N) : 0;
         const bool drawn = k > 0 && d > N;
@@ -548,13 +547,18 @@ k_coop_fast(DevGraph g, LevelArgs a) {
     }
 }
 
+template <typename I, int BIAS>
+__global__ void __launch_bounds__(FAST_THREADS)
+k_coop_fast(DevGraph g, LevelArgs a) {
+    coop_body<I, BIAS>(g, a);
+}
+
 // Level expansion, part 2: one warp per listed item (N < d <= WF when
 // biased); writes into the slots reserved by part 1.  CACHED: the graph holds
 // the prefix cache for BIAS, so no shared copy of the raw biases is kept
 // (half the shared memory, more resident warps).
 template <typename I, int BIAS, bool CACHED>
-__global__ void __launch_bounds__(FAST_THREADS, 4)
-k_select_fast(DevGraph g, LevelArgs a) {
+__device__ __forceinline__ void select_fast_body(const DevGraph &g, const LevelArgs &a) {
     constexpr bool BIASED = BIAS != CSAW_BIAS_UNBIASED;
     constexpr int NW = FAST_THREADS / 32;
     __shared__ float s_W[BIASED && !CACHED ? NW * WF : 1];
@@ -568,14 +572,14 @@ k_select_fast(DevGraph g, LevelArgs a) {
     float *P = s_P + (BIASED ? wib * WF : 0);
     uint32_t *zb = s_z + (BIASED ? wib * (WF / 32) : 0);
     int *zs = s_zs + wib * 32;
-    const uint32_t n = *a.n_sel;
-    const uint32_t n_level = *a.n_in;
+    const uint32_t n = __ldcg(a.n_sel);
+    const uint32_t n_level = __ldcg(a.n_in);
     const int N = a.N;
     constexpr bool cached = BIASED && CACHED;
     const int nout = 2 + (a.o_smp != nullptr) + (a.o_dep != nullptr);
     unsigned long long my_bytes = 0, my_items = 0;
     for (uint32_t i = gw; i < n; i += nw) {
-        const SelEntry en = a.sel_list[i];
+        const SelEntry en = load_sel(a.sel_list + i);
         const int32_t v = en.v, s = en.s;
         const uint32_t p = en.p;
         const int64_t beg = en.beg, d = en.d;
@@ -621,6 +625,12 @@ k_select_fast(DevGraph g, LevelArgs a) {
         atomicAdd(&a.bytes[5], my_bytes);
         atomicAdd(&a.items[5], my_items);
     }
+}
+
+template <typename I, int BIAS, bool CACHED>
+__global__ void __launch_bounds__(FAST_THREADS, 4)
+k_select_fast(DevGraph g, LevelArgs a) {
+    select_fast_body<I, BIAS, CACHED>(g, a);
 }
 
 // Half-warp primitives: a warp runs two independent items, lanes 0-15 and
@@ -747,28 +757,17 @@ __device__ __forceinline__ unsigned long long staged_bytes(const StagePlan &sp, 
 // redone from scratch: rows up to WF by k_select_fast on the refill list
 // (written over the consumed warp list), larger ones by the CTA pass.
 template <typename I, int BIAS>
-__global__ void __launch_bounds__(FAST_THREADS, CSAW_PAIR_MIN_BLOCKS)
-k_select_pair(DevGraph g, LevelArgs a) {
-    constexpr int NH = FAST_THREADS / 16;
-    constexpr int ROW = WF + 4;   // floats: a row of up to WF plus its 16-byte alignment window
-    __shared__ __align__(16) float s_P[NH * ROW];
-    __shared__ __align__(8) uint64_t s_bar[NH];
+__device__ __forceinline__ void pair_body(const DevGraph &g, const LevelArgs &a, float *buf, uint64_t *bar,
+                                          uint32_t &parity) {
     const int lane = threadIdx.x & 31;
     const Half h(lane);
-    const int hid = threadIdx.x >> 4;
-    float *buf = s_P + hid * ROW;
-    uint64_t *bar = s_bar + hid;
-    if (h.sl == 0) mbar_init(bar);
-    mbar_init_fence();
-    __syncthreads();
     const uint32_t gh = (blockIdx.x * blockDim.x + threadIdx.x) >> 4;
     const uint32_t nh = (gridDim.x * blockDim.x) >> 4;
-    const uint32_t n = *a.n_pair;
-    const uint32_t n_level = *a.n_in;
+    const uint32_t n = __ldcg(a.n_pair);
+    const uint32_t n_level = __ldcg(a.n_in);
     const int N = a.N;
     const int nout = 2 + (a.o_smp != nullptr) + (a.o_dep != nullptr);
     unsigned long long my_bytes = 0, my_items = 0;
-    uint32_t parity = 0;
     // requests the staged copy of what an item searches (stage_plan); returns
     // the copy's offset in the buffer
     auto request = [&](long long rbeg, int rd) -> int {
@@ -783,16 +782,16 @@ k_select_pair(DevGraph g, LevelArgs a) {
     };
     int off = 0;
     uint32_t i = gh;
-    if (i < n) off = request(__ldg(&a.pair_list[i].beg), __ldg(&a.pair_list[i].d));
+    if (i < n) off = request(__ldcg(&a.pair_list[i].beg), __ldcg(&a.pair_list[i].d));
     for (; i < n; i += nh) {
         const uint32_t inext = i + nh;
         long long nbeg = 0;
         int nd = 0;
         if (inext < n) {   // the next row's range: its load overlaps this item
-            nbeg = __ldg(&a.pair_list[inext].beg);
-            nd = __ldg(&a.pair_list[inext].d);
+            nbeg = __ldcg(&a.pair_list[inext].beg);
+            nd = __ldcg(&a.pair_list[inext].d);
         }
-        const SelEntry en = a.pair_list[i];
+        const SelEntry en = load_sel(a.pair_list + i);
         const int64_t beg = en.beg, d = en.d;
         const DrawCtx dc{a.k0, a.k1, en.p, (uint32_t)en.s, (uint32_t)a.depth};
         const bool rec = a.sched && a.sched->mode == SCHED_RECORD;
@@ -853,24 +852,41 @@ k_select_pair(DevGraph g, LevelArgs a) {
     }
 }
 
+// Shared staging buffers of the pair pass: one row window per half-warp,
+// each with its bulk-copy barrier.
+constexpr int PAIR_HALVES = FAST_THREADS / 16;
+constexpr int PAIR_ROW = WF + 4;   // floats: a row of up to WF plus its 16-byte alignment window
+
+template <typename I, int BIAS>
+__global__ void __launch_bounds__(FAST_THREADS, CSAW_PAIR_MIN_BLOCKS)
+k_select_pair(DevGraph g, LevelArgs a) {
+    __shared__ __align__(16) float s_P[PAIR_HALVES * PAIR_ROW];
+    __shared__ __align__(8) uint64_t s_bar[PAIR_HALVES];
+    const int hid = threadIdx.x >> 4;
+    if ((threadIdx.x & 15) == 0) mbar_init(s_bar + hid);
+    mbar_init_fence();
+    __syncthreads();
+    uint32_t parity = 0;
+    pair_body<I, BIAS>(g, a, s_P + hid * PAIR_ROW, s_bar + hid, parity);
+}
+
 // Level expansion, part 2 for hub items (d > WF) over a cached prefix: one
 // warp per item, each draw a search of the prefix through its index
 // (cdf_search) taken one attempt at a time, since a search costs dependent
 // loads; no shared memory.  An item whose draws need a rebuild of its prefix
 // goes to the retry list (the CTA pass rebuilds it in global scratch).
 template <typename I, int BIAS>
-__global__ void __launch_bounds__(FAST_THREADS, 4)
-k_select_hub(DevGraph g, LevelArgs a) {
+__device__ __forceinline__ void hub_body(const DevGraph &g, const LevelArgs &a) {
     const int lane = threadIdx.x & 31;
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t n = *a.n_hub;
-    const uint32_t n_level = *a.n_in;
+    const uint32_t n = __ldcg(a.n_hub);
+    const uint32_t n_level = __ldcg(a.n_in);
     const int N = a.N;
     const int nout = 2 + (a.o_smp != nullptr) + (a.o_dep != nullptr);
     unsigned long long my_bytes = 0, my_items = 0;
     for (uint32_t i = gw; i < n; i += nw) {
-        const SelEntry en = a.hub_list[i];
+        const SelEntry en = load_sel(a.hub_list + i);
         const DrawCtx dc{a.k0, a.k1, en.p, (uint32_t)en.s, (uint32_t)a.depth};
         const bool rec = a.sched && a.sched->mode == SCHED_RECORD;
         long long t0 = 0;
@@ -900,6 +916,12 @@ k_select_hub(DevGraph g, LevelArgs a) {
         atomicAdd(&a.bytes[6], my_bytes);
         atomicAdd(&a.items[6], my_items);
     }
+}
+
+template <typename I, int BIAS>
+__global__ void __launch_bounds__(FAST_THREADS, 4)
+k_select_hub(DevGraph g, LevelArgs a) {
+    hub_body<I, BIAS>(g, a);
 }
 
 // Biased walks: one warp per walk.  A step with d <= 32 is one round trip:

@@ -14,6 +14,26 @@
 
 namespace csaw {
 
+// A listed frontier item, read around L1 (the list may have been written by
+// other blocks earlier in the same launch).
+__device__ __forceinline__ SelEntry load_sel(const SelEntry *e) {
+    static_assert(sizeof(SelEntry) == 48, "three 16-byte loads");
+    const int4 *q = reinterpret_cast<const int4 *>(e);
+    const int4 x = __ldcg(q), y = __ldcg(q + 1), z = __ldcg(q + 2);
+    SelEntry r;
+    r.it = (uint32_t)x.x;
+    r.q = (uint32_t)x.y;
+    r.ob = ((unsigned long long)(uint32_t)x.w << 32) | (uint32_t)x.z;
+    r.v = y.x;
+    r.s = y.y;
+    r.p = (uint32_t)y.z;
+    r.d = y.w;
+    r.beg = (long long)(((unsigned long long)(uint32_t)z.y << 32) | (uint32_t)z.x);
+    r.cls = z.z;
+    r.pad = z.w;
+    return r;
+}
+
 // Algorithmic bytes of one expansion (what the algorithm must touch; sector
 // waste not counted): queue item 12 B, rowptr pair, bias reads when the
 // prefix is scanned, the selected col entries, the output edges and the pushed
@@ -257,31 +277,30 @@ __host__ __device__ __forceinline__ int64_t heavy_need(int64_t d) {
 // global scratch (same canonical order, so bit-identical to the warp path);
 // warp 0 runs the slot resolver; every rebuild is a CTA-wide rescan.
 template <typename I, int BIAS, bool STREAM = false>
-__global__ void __launch_bounds__(1024)
-k_expand_heavy(DevGraph g0, LevelArgs a) {
+__device__ __forceinline__ void heavy_body(const DevGraph &g0, const LevelArgs &a) {
     __shared__ int s_flag, s_j;
     extern __shared__ float s_heavy[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float *const P_global = a.heavy_scratch + (int64_t)blockIdx.x * a.heavy_stride;
-    const uint32_t nh = *a.n_heavy;
+    const uint32_t nh = __ldcg(a.n_heavy);
     unsigned long long my_bytes = 0, my_items = 0;
     for (uint32_t h = blockIdx.x; h < nh; h += gridDim.x) {
-        const uint32_t it = a.heavy_list ? a.heavy_list[h].it : a.heavy[h];
+        const uint32_t it = a.heavy_list ? __ldcg(&a.heavy_list[h].it) : __ldcg(a.heavy + h);
         int l, N;
         bool push;
         item_level(a, it, l, N, push);
         const bool rec = a.sched && a.sched->mode == SCHED_RECORD;
         long long t0 = 0;
         if (rec && threadIdx.x == 0) t0 = clock64();
-        const int32_t v = a.in_v[it];
+        const int32_t v = __ldcg(a.in_v + it);
         DevGraph g = g0;
         if (STREAM) {   // deferred by the warp pass, so its partition is resident
             const int part = v >> a.pbits;
             g.v.col = a.part_col[part];
             g.v.weight = a.part_w[part];
         }
-        const int32_t s = a.in_s[it];
-        const uint32_t p = a.in_p[it];
+        const int32_t s = __ldcg(a.in_s + it);
+        const uint32_t p = __ldcg(a.in_p + it);
         const int64_t beg = row_begin<I>(g, v);
         const int64_t d = row_begin<I>(g, v + 1) - beg;
         const bool in_smem = heavy_need(d) <= a.heavy_smem;
@@ -344,8 +363,8 @@ k_expand_heavy(DevGraph g0, LevelArgs a) {
             unsigned long long ob = 0;
             uint32_t q = 0;
             if (a.heavy_list) {  // slots reserved by the batched first pass
-                ob = a.heavy_list[h].ob;
-                q = a.heavy_list[h].q;
+                ob = __ldcg(&a.heavy_list[h].ob);
+                q = __ldcg(&a.heavy_list[h].q);
             } else {
                 if (lane == 0) {
                     ob = atomicAdd(a.o_count, (unsigned long long)N);
@@ -379,12 +398,18 @@ k_expand_heavy(DevGraph g0, LevelArgs a) {
         my_bytes += expansion_bytes<I, BIAS>(g, d, N, true, a, push);
         __syncthreads();
         if (rec && threadIdx.x == 0)
-            record_profile(a.sched, d, N, a.sched->vstats[v], *a.n_in, l, 2 + a.cta_class, clock64() - t0);
+            record_profile(a.sched, d, N, a.sched->vstats[v], __ldcg(a.n_in), l, 2 + a.cta_class, clock64() - t0);
     }
     if (threadIdx.x == 0) {
         atomicAdd(&a.bytes[1], my_bytes);
         atomicAdd(&a.items[1], my_items);
     }
+}
+
+template <typename I, int BIAS, bool STREAM = false>
+__global__ void __launch_bounds__(1024)
+k_expand_heavy(DevGraph g0, LevelArgs a) {
+    heavy_body<I, BIAS, STREAM>(g0, a);
 }
 
 // ------------------------------------------------------------ walks

@@ -141,7 +141,9 @@ int csaw_graph_stats(csaw_graph g, csaw_stats *out);
  * warp-granularity selection pass, 6 batched hub selection (cached prefix),
  * 7 batched two-items-per-warp selection (cached prefix, N <= 16), 8 walk
  * with one thread per walk (unbiased walks; many biased walks over a cached
- * prefix).
+ * prefix), 9 persistent job kernel (every level of a batched neighbor job in
+ * one launch; its bytes and items are counted under the kinds of the passes
+ * it runs).
  */
 int csaw_graph_profile(csaw_graph g, int enable);
 int csaw_graph_kernel_stats(csaw_graph g, int kind, double *ms, int64_t *launches,
@@ -227,7 +229,14 @@ enum {
      * rebuild fits are done in shared memory, larger ones in global scratch.
      * More shared memory means fewer resident CTAs; never changes the
      * output. */
-    CSAW_OPT_RETRY_SMEM = 6
+    CSAW_OPT_RETRY_SMEM = 6,
+    /* 1: batched neighbor jobs run all their levels in one persistent
+     * cooperative kernel (items pushed for the next level are consumed in
+     * the same launch; grid barriers with bounded waits between passes);
+     * 0 (default): one launch per pass and level.  Applies to degree-rule
+     * jobs over a cached prefix (or unbiased) without dedup, up to 4 levels;
+     * others use the per-level launches.  Never changes the output. */
+    CSAW_OPT_PERSISTENT = 7
 };
 int csaw_graph_set_option(csaw_graph g, int option, int64_t value);
 
