@@ -77,7 +77,7 @@ class ServerStats(ctypes.Structure):
 
 class TuneResult(ctypes.Structure):
     _fields_ = [("grid_pct", ctypes.c_int32), ("pair", ctypes.c_int32), ("best_ms", ctypes.c_double),
-                ("default_ms", ctypes.c_double), ("candidates", ctypes.c_int32)]
+                ("default_ms", ctypes.c_double), ("candidates", ctypes.c_int32), ("persistent", ctypes.c_int32)]
 
 
 class Job(ctypes.Structure):

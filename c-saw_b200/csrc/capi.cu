@@ -1720,52 +1720,59 @@ extern "C" int csaw_graph_autotune(csaw_graph g, csaw_job *jobs, int n_jobs, voi
     cudaStream_t st = (cudaStream_t)stream;
     const int pcts[3] = {100, 50, 200};
     const int old_pct = g->grid_pct;
-    const bool old_pair = g->pair, old_graphs = g->use_graphs;
+    const bool old_pair = g->pair, old_graphs = g->use_graphs, old_persist = g->persistent;
     g->use_graphs = false;   // each candidate timed launch by launch
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     double best = 1e300, dflt = 0.0;
     int best_pct = old_pct, n = 0;
-    bool best_pair = old_pair;
+    bool best_pair = old_pair, best_persist = old_persist;
     int rc = 0;
-    for (int pair = 1; pair >= 0 && !rc; --pair)
-        for (int k = 0; k < 3 && !rc; ++k) {
-            g->grid_pct = pcts[k];
-            g->pair = pair != 0;
-            rc = csaw_sample_batch(g, jobs, n_jobs, stream);   // untimed: workspace, caches
-            if (rc) break;
-            cudaEventRecord(e0, st);
-            rc = csaw_sample_batch(g, jobs, n_jobs, stream);
-            cudaEventRecord(e1, st);
-            if (rc) break;
-            cudaEventSynchronize(e1);
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            ++n;
-            if (pair == 1 && pcts[k] == 100) dflt = ms;
-            if (ms < best) {
-                best = ms;
-                best_pct = pcts[k];
-                best_pair = pair != 0;
-            }
+    // candidates: per-level launches (grid % x pairing), then the persistent
+    // job kernel (its grid is the occupancy-filled one) with pairing
+    for (int cand = 0; cand < 7 && !rc; ++cand) {
+        const int pair = cand < 3 || cand == 6 ? 1 : 0, k = cand % 3;
+        g->persistent = cand == 6;
+        g->grid_pct = cand == 6 ? 100 : pcts[k];
+        g->pair = pair != 0;
+        rc = csaw_sample_batch(g, jobs, n_jobs, stream);   // untimed: workspace, caches
+        if (rc) break;
+        cudaEventRecord(e0, st);
+        rc = csaw_sample_batch(g, jobs, n_jobs, stream);
+        cudaEventRecord(e1, st);
+        if (rc) break;
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ++n;
+        if (cand == 0) dflt = ms;
+        if (ms < best) {
+            best = ms;
+            best_pct = g->grid_pct;
+            best_pair = pair != 0;
+            best_persist = g->persistent;
         }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     g->use_graphs = old_graphs;
     if (rc) {
         g->grid_pct = old_pct;
         g->pair = old_pair;
+        g->persistent = old_persist;
         return rc;
     }
     g->grid_pct = best_pct;
     g->pair = best_pair;
+    g->persistent = best_persist;
     ++g_alloc_epoch;
     out->grid_pct = best_pct;
     out->pair = best_pair ? 1 : 0;
     out->best_ms = best;
     out->default_ms = dflt;
     out->candidates = n;
+    out->persistent = best_persist ? 1 : 0;
     return 0;
 }
 

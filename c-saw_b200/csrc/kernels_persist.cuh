@@ -13,7 +13,7 @@
 //            a warp that runs out of one list starts on the next)
 //   phase 3  refill list (pair items that need a rebuild, a warp each) and
 //            the retry list (hub rebuilds, a CTA each)
-// separated by grid barriers.  A barrier counts arriving warps (a counter per
+// separated by grid barriers.  A barrier counts arriving CTAs (a counter per
 // barrier, zero at launch, so none is ever reset) and waits with a bounded
 // spin: if it expires, the error flag is set and the warp goes on, so a
 // failure ends the launch with an error instead of a hang.  Each level's
@@ -51,7 +51,7 @@ struct PersistArgs {
     uint32_t flags[PERSIST_MAX_LEVELS];
     unsigned long long *posts[PERSIST_MAX_LEVELS];   // page-locked slot for the edge count after level l, or null
     int D;
-    unsigned *arrive;   // [3 * D] warp arrivals per barrier
+    unsigned *arrive;   // [3 * D] CTA arrivals per barrier
     int *err;
 };
 
@@ -61,38 +61,40 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
     return v;
 }
 
-// Every warp of the grid arrives at `arrive` (zero before the first
-// arrival); returns once all have, or sets ERR_BARRIER after the bounded wait.
-__device__ __forceinline__ void grid_barrier(unsigned *arrive, unsigned nwarps, int *err) {
-    __syncwarp();
-    if ((threadIdx.x & 31) == 0) {
+// Every CTA of the grid arrives at `arrive` (zero before the first
+// arrival) once all its warps are done; returns once all CTAs have, or sets
+// ERR_BARRIER after the bounded wait.
+__device__ __forceinline__ void grid_barrier(unsigned *arrive, unsigned nblocks, int *err) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
         __threadfence();
         atomicAdd(arrive, 1u);
         int spins = 0;
-        while (ld_acquire_u32(arrive) < nwarps) {
+        while (ld_acquire_u32(arrive) < nblocks) {
             if (++spins > PERSIST_BARRIER_SPINS) {
                 atomicOr(err, ERR_BARRIER);
                 break;
             }
-            __nanosleep(128);
+            __nanosleep(64);
         }
+        __threadfence();
     }
-    __syncwarp();
-    __threadfence();
+    __syncthreads();
 }
 
 // Bytes of dynamic shared memory of k_persist: the pair pass's row windows
 // and their barriers.
 constexpr size_t PERSIST_SMEM = sizeof(float) * PAIR_HALVES * PAIR_ROW + sizeof(uint64_t) * PAIR_HALVES;
 
-// The passes as calls, not inlined: each keeps the register allocation it
-// has as a kernel of its own instead of sharing one across all passes.
+// The passes: the frequent ones inlined into the one kernel, the hub and
+// CTA-retry passes (rare, with large state of their own) as calls, so their
+// registers do not weigh on the inlined loops.
 template <typename I, int BIAS>
-__device__ __noinline__ void call_coop(const DevGraph &g, const LevelArgs &a) {
+__device__ __forceinline__ void call_coop(const DevGraph &g, const LevelArgs &a) {
     coop_body<I, BIAS>(g, a);
 }
 template <typename I, int BIAS, bool CACHED>
-__device__ __noinline__ void call_select(const DevGraph &g, const LevelArgs &a) {
+__device__ __forceinline__ void call_select(const DevGraph &g, const LevelArgs &a) {
     select_fast_body<I, BIAS, CACHED>(g, a);
 }
 template <typename I, int BIAS>
@@ -100,7 +102,7 @@ __device__ __noinline__ void call_hub(const DevGraph &g, const LevelArgs &a) {
     hub_body<I, BIAS>(g, a);
 }
 template <typename I, int BIAS>
-__device__ __noinline__ void call_pair(const DevGraph &g, const LevelArgs &a, float *buf, uint64_t *bar,
+__device__ __forceinline__ void call_pair(const DevGraph &g, const LevelArgs &a, float *buf, uint64_t *bar,
                                        uint32_t &parity) {
     pair_body<I, BIAS>(g, a, buf, bar, parity);
 }
@@ -109,8 +111,12 @@ __device__ __noinline__ void call_heavy(const DevGraph &g, const LevelArgs &a) {
     heavy_body<I, BIAS>(g, a);
 }
 
+#ifndef CSAW_PERSIST_MIN_BLOCKS
+#define CSAW_PERSIST_MIN_BLOCKS 4
+#endif
+
 template <typename I, int BIAS>
-__global__ void __launch_bounds__(FAST_THREADS, 4)
+__global__ void __launch_bounds__(FAST_THREADS, CSAW_PERSIST_MIN_BLOCKS)
 k_persist(const __grid_constant__ DevGraph g, const __grid_constant__ PersistArgs pa) {
     constexpr bool BIASED = BIAS != CSAW_BIAS_UNBIASED;
     extern __shared__ float s_heavy[];   // the same dynamic region heavy_body names (unused by it here)
@@ -123,22 +129,22 @@ k_persist(const __grid_constant__ DevGraph g, const __grid_constant__ PersistArg
     }
     __syncthreads();
     uint32_t parity = 0;
-    const unsigned nwarps = gridDim.x * (blockDim.x >> 5);
+    const unsigned nblocks = gridDim.x;
     int k = 0;
     for (int l = 0; l < pa.D; ++l) {
         const uint32_t fl = pa.flags[l];
         call_coop<I, BIAS>(g, pa.lv[l]);
-        grid_barrier(pa.arrive + k++, nwarps, pa.err);
+        grid_barrier(pa.arrive + k++, nblocks, pa.err);
         call_select<I, BIAS, BIASED>(g, pa.lv[l]);
         if (fl & PF_HUB) call_hub<I, BIAS>(g, pa.lv[l]);
         if (BIASED && (fl & PF_PAIR)) call_pair<I, BIAS>(g, pa.lv[l], pairP + hid * PAIR_ROW, bars + hid, parity);
-        grid_barrier(pa.arrive + k++, nwarps, pa.err);
+        grid_barrier(pa.arrive + k++, nblocks, pa.err);
         if (BIASED && (fl & PF_PAIR)) call_select<I, BIAS, true>(g, pa.refill[l]);
         if (fl & PF_RETRY) {
             __syncthreads();   // the whole CTA enters the retry pass
             call_heavy<I, BIAS>(g, pa.retry[l]);
         }
-        if (l + 1 < pa.D || pa.posts[l]) grid_barrier(pa.arrive + k++, nwarps, pa.err);
+        if (l + 1 < pa.D || pa.posts[l]) grid_barrier(pa.arrive + k++, nblocks, pa.err);
         if (pa.posts[l] && blockIdx.x == 0 && threadIdx.x == 0) {   // this level's edges are final
             *(volatile unsigned long long *)pa.posts[l] = *(volatile unsigned long long *)pa.lv[l].o_count;
             __threadfence_system();

@@ -56,8 +56,8 @@ def test_autotune_keeps_fastest_and_output(csaw, rmat12_pareto):
     jobs = jobs_for(csaw, rmat12_pareto)
     ref = edges(G.sample_batch(jobs))
     r = G.autotune(jobs)
-    assert r["candidates"] == 6
-    assert r["grid_pct"] in (50, 100, 200) and r["pair"] in (0, 1)
+    assert r["candidates"] == 7   # 3 grid sizes x pairing on/off, and the persistent job kernel
+    assert r["grid_pct"] in (50, 100, 200) and r["pair"] in (0, 1) and r["persistent"] in (0, 1)
     assert 0 < r["best_ms"] <= r["default_ms"]
     got = edges(G.sample_batch(jobs))
     assert all(np.array_equal(a, b) for a, b in zip(got, ref))
