@@ -929,6 +929,76 @@ def profile_step(args):
     G.close()
 
 
+def profile_kernels(args):
+    """Every kernel family once, on a graph far above L2, for per-kernel ncu
+    captures (bench.py --profile-kernels under ncu --metrics): R-MAT
+    (.6/.2/.15) scale 22, edge factor 16, int64 row offsets, Pareto(1.5)
+    weights.  Runs, in order: the graph's prefix cache and neighbor records
+    (first batched biased job), a batched F8 N10 D3 step with walks of 40
+    (take-all, warp-list, pair, retry, thread-per-walk passes), a batched
+    N 20 job (hub list), the plain schedule (warp expansion, CTA expansion,
+    warp walks), batched warp walks, MDRW, per-sample dedup, profile
+    recording and training of the learned scheduler, streaming through a
+    512 MiB partition budget, and the allocation-free entry.  Prints the
+    per-kind kernel statistics of each part."""
+    import torch
+    import csaw
+    from csaw import _lib, graphgen
+    torch.cuda.set_device(0)
+    g = graphgen.rmat_device(scale=22, edge_factor=16, a=0.6, b=0.2, c=0.15, seed=25, symmetrize=False,
+                             weight="pareto:1.5")
+    torch.cuda.empty_cache()
+    G = csaw.Graph(g, rowptr64=True)
+    G.set_option(_lib.OPT_CUDA_GRAPHS, 0)
+    out = {}
+
+    def part(name, fn):
+        G.profile(True)
+        fn()
+        torch.cuda.synchronize()
+        out[name] = {k: v for k, v in ((k, G.kernel_stats(k)) for k in KINDS + ("mdrw", "persist")) if v["launches"]}
+        G.profile(False)
+
+    def job(mode, bias, n, F, N, D, fan=None, sched=csaw.SCHED_BATCHED, dedup=False, seed=1):
+        p = csaw.make_params(mode, bias, n, F, N, D, fan, seed=seed, schedule=sched, dedup=dedup)
+        seeds = G.make_seeds(n * (1 if mode == 1 else F), seed)
+        o = torch.empty((3, csaw.edge_bound(p)), dtype=torch.int32, device="cuda")
+        return csaw.BatchJob(p, seeds, o.shape[1], o, with_depth=False)
+
+    step = [job(0, 2, 8192, 8, 10, 3, seed=2), job(1, 2, 131072, 1, 1, 40, seed=3)]
+    part("cache_build_and_first_step", lambda: G.sample_batch(step))
+    part("batched_step", lambda: G.sample_batch(step))
+    part("batched_n20_hubs", lambda: G.sample_batch([job(0, 2, 2048, 4, 20, 2, seed=4)]))
+    part("plain", lambda: G.sample_batch([job(0, 2, 256, 8, 10, 3, sched=csaw.SCHED_PLAIN, seed=5),
+                                          job(1, 2, 2048, 1, 1, 40, sched=csaw.SCHED_PLAIN, seed=6)]))
+    part("batched_warp_walks", lambda: G.sample_batch([job(1, 2, 4096, 1, 1, 40, seed=7)]))
+    part("mdrw", lambda: G.sample_batch([job(2, 1, 8192, 8, 1, 20, seed=8)]))
+    part("dedup", lambda: G.sample_batch([job(0, 2, 4096, 4, 10, 3, dedup=True, seed=9)]))
+    learn = [job(0, 2, 4096, 8, 10, 3, sched=csaw.SCHED_LEARNED, seed=10)]
+    G.sched_record(100_000)
+
+    def learned():
+        G.sample_batch(learn)
+        G.sched_train(epochs=20, lr=3e-3, seed=1)
+        G.sample_batch(learn)
+    part("learned_record_train", learned)
+    S = csaw.StreamGraph(g, partition_bits=16, slot_budget_bytes=512 << 20, rowptr64=True)
+    ps = csaw.make_params(0, 2, 2048, 1, 10, 2, seed=11)
+    pw = csaw.make_params(1, 2, 8192, 1, 1, 20, seed=12)
+    ss, sw = G.make_seeds(2048, 11), G.make_seeds(8192, 12)
+    S.sample(ps, ss)
+    S.sample(pw, sw)
+    torch.cuda.synchronize()
+    out["stream"] = {"partition_loads": S.info()["partition_loads"], "kernel_launches": S.info()["kernel_launches"]}
+    S.close()
+    pn = csaw.make_params(0, 0, 2048, 2, 10, 3, seed=13)
+    on = torch.empty((4, csaw.edge_bound(pn)), dtype=torch.int32, device="cuda")
+    G.sample_noalloc(pn, G.make_seeds(4096, 13), on)
+    torch.cuda.synchronize()
+    G.close()
+    print(json.dumps({"profile_kernels": out}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -944,6 +1014,8 @@ def main():
                     help="device time the plain form's timed steps may take (at least 2 steps)")
     ap.add_argument("--profile-step", action="store_true",
                     help="run W warm-up steps and one step of the batched form only (for ncu captures)")
+    ap.add_argument("--profile-kernels", action="store_true",
+                    help="run every kernel family once on R-MAT scale 22 (for per-kernel ncu captures)")
     ap.add_argument("--learned-gain", action="store_true",
                     help="time the degree rule vs the learned scheduler on a heavy-tailed R-MAT graph instead")
     ap.add_argument("--serve", action="store_true", help="run only the serving (request loop) workload")
@@ -965,6 +1037,9 @@ def main():
         return
     if args.profile_step:
         profile_step(args)
+        return
+    if args.profile_kernels:
+        profile_kernels(args)
         return
     if args.serve:
         import torch
