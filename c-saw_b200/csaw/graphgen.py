@@ -150,6 +150,75 @@ def rmat_device(scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=0, symmetrize=T
     return out
 
 
+def rmat_device_bucketed(scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=0, weight="uniform", buckets=16,
+                         device="cuda", chunk=1 << 26):
+    """Directed R-MAT as rmat_device() for graphs whose edge keys do not fit
+    one on-device sort (scales 27-29): the edge stream (same quadrant rule,
+    one torch Philox generator seeded with `seed`) is generated once per
+    source range of V / buckets vertices, keeping only that range's edges,
+    which are deduplicated and turned into that range's CSR rows, then
+    moved to host memory.  Every pass replays the same stream, so the
+    buckets partition one graph; self-loops and duplicates are removed.
+    Weights come from a generator seeded with seed + 1 + bucket."""
+    import torch
+    V = 1 << scale
+    E = edge_factor * V
+    shift = scale - int(np.log2(buckets))
+    assert buckets & (buckets - 1) == 0 and shift > 0
+    ab, abc = a + b, a + b + c
+    rowptr = np.zeros(V + 1, dtype=np.int64)
+    cols, ws = [], []
+    total = 0
+    for bk in range(buckets):
+        gen = torch.Generator(device=device)
+        gen.manual_seed(seed)
+        keys = []
+        for off in range(0, E, chunk):
+            n = min(chunk, E - off)
+            s = torch.zeros(n, dtype=torch.int64, device=device)
+            d = torch.zeros(n, dtype=torch.int64, device=device)
+            for bit in range(scale):
+                r = torch.rand(n, generator=gen, device=device)
+                s |= (r >= ab).to(torch.int64) << bit
+                d |= (((r >= a) & (r < ab)) | (r >= abc)).to(torch.int64) << bit
+                del r
+            keep = ((s >> shift) == bk) & (s != d)
+            keys.append(torch.unique(s[keep] * V + d[keep]))
+            del s, d, keep
+        key = torch.unique(torch.cat(keys))
+        del keys
+        src = key // V
+        col = (key % V).to(torch.int32)
+        del key
+        lo = bk << shift
+        counts = torch.bincount(src - lo, minlength=1 << shift)
+        del src
+        rowptr[lo + 1:lo + 1 + (1 << shift)] = total + torch.cumsum(counts, 0).cpu().numpy()
+        m = col.numel()
+        total += m
+        cols.append(col.cpu().numpy())
+        del col
+        wgen = torch.Generator(device=device)
+        wgen.manual_seed(seed + 1 + bk)
+        if weight == "uniform":
+            w = 1.0 - torch.rand(m, generator=wgen, device=device)
+        elif weight.startswith("pareto"):
+            alpha = float(weight.split(":")[1]) if ":" in weight else 1.5
+            w = torch.pow(1.0 - torch.rand(m, generator=wgen, device=device), -1.0 / alpha)
+        elif weight == "none":
+            w = None
+        else:
+            raise ValueError(weight)
+        ws.append(None if w is None else w.float().cpu().numpy())
+        del w
+        torch.cuda.empty_cache()
+    col = np.concatenate(cols)
+    del cols
+    w = None if ws[0] is None else np.concatenate(ws)
+    del ws
+    return CSR(rowptr, col, w, name=f"rmat{scale}_ef{edge_factor}_dev")
+
+
 def powerlaw_directed(n_vertices=875_713, n_edges=5_105_039, gamma=2.1, max_degree=460, zipf=0.6,
                       seed=0, weight="lognormal"):
     """Directed graph whose out-degrees follow P(d) ~ d^-gamma on [1, max_degree]."""
