@@ -828,69 +828,99 @@ def serving(args, n_slots=8):
 
 
 
-STREAM_GRAPH = dict(scale=26, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=29, symmetrize=False, weight="uniform")
+STREAM_GRAPH = dict(edge_factor=16, a=0.57, b=0.19, c=0.19, seed=29, weight="uniform")
 
 
 def streaming(args):
-    """Streaming (out-of-budget) workload at 1/8 of the scale-29 configuration:
-    R-MAT scale 26, edge factor 16, directed, U(0,1] weights (generated on the
-    GPU), adjacency in page-locked host memory with the device partition
-    budget capped at 4 GiB (under half of the 8.5 GB adjacency) and 2^17-vertex
-    partitions (512, as many as the scale-29 configuration has); one step = 131,072 edge-weight-biased walks of length 20 and
-    32,768 edge-weight-biased samples F1 N10 D2.  The same jobs on the
-    in-memory graph give the reference time and check the edge counts."""
+    """Streaming (out-of-budget) workload: R-MAT (.57/.19/.19) at
+    --stream-scale (default 26), edge factor 16, directed, U(0,1] weights
+    (generated on the GPU; scales >= 27 per source range), adjacency in
+    page-locked host memory, the device partition budget capped at
+    --stream-budget-gb with 2^--stream-pbits-vertex partitions; one step =
+    --stream-walks edge-weight-biased walks of length 20 and --stream-samples
+    edge-weight-biased samples F1 N10 D2.  The defaults are 1/8 of the
+    scale-29 configuration (131,072 walks, 32,768 samples, 4 GiB, 2^17-vertex
+    partitions: 512, as many as scale 29 has); the configuration's own shape
+    is --stream-scale 28 --stream-budget-gb 32 --stream-pbits 20
+    --stream-walks 1048576 --stream-samples 262144.  The same jobs on the
+    in-memory graph (plain schedule; the batched one too when the graph is
+    small enough) check the edges by multiset hash and give the reference
+    time."""
     import torch
     import csaw
     from csaw import graphgen
     torch.cuda.set_device(0)
-    g = graphgen.rmat_device(**STREAM_GRAPH)
+    sc = args.stream_scale
+    t0 = time.perf_counter()
+    if sc >= 27:
+        g = graphgen.rmat_device_bucketed(scale=sc, **{k: v for k, v in STREAM_GRAPH.items()})
+    else:
+        g = graphgen.rmat_device(scale=sc, symmetrize=False, **STREAM_GRAPH)
+    gen_s = time.perf_counter() - t0
     torch.cuda.empty_cache()
-    budget = 4 << 30
-    res = {"graph": {"workload": "rmat26_ef16_uniform", "n_vertices": g.n_vertices, "n_edges": g.n_edges,
+    budget = int(args.stream_budget_gb * (1 << 30))
+    nw, ns, pbits = args.stream_walks, args.stream_samples, args.stream_pbits
+    res = {"graph": {"workload": f"rmat{sc}_ef16_uniform", "n_vertices": g.n_vertices, "n_edges": g.n_edges,
+                     "max_degree": int(np.diff(g.rowptr).max()), "generate_s": gen_s,
                      "host_adjacency_bytes": int(g.col.nbytes + g.weight.nbytes + g.rowptr.nbytes)},
-           "partition_bits": 17, "device_budget": budget,
-           "walks": dict(n=1 << 17, length=20), "samples": dict(n=1 << 15, F=1, N=10, D=2)}
-    pw = csaw.make_params(1, 2, 1 << 17, 1, 1, 20, seed=0x29A)
-    ps = csaw.make_params(0, 2, 1 << 15, 1, 10, 2, seed=0x29B)
-    # the in-memory reference also runs the batched schedule (cache, records)
-    pwb = csaw.make_params(1, 2, 1 << 17, 1, 1, 20, seed=0x29A, schedule=csaw.SCHED_BATCHED)
-    psb = csaw.make_params(0, 2, 1 << 15, 1, 10, 2, seed=0x29B, schedule=csaw.SCHED_BATCHED)
-    S = csaw.StreamGraph(g, partition_bits=17, slot_budget_bytes=budget, rowptr64=True)
+           "partition_bits": pbits, "device_budget": budget,
+           "walks": dict(n=nw, length=20), "samples": dict(n=ns, F=1, N=10, D=2)}
+    pw = csaw.make_params(1, 2, nw, 1, 1, 20, seed=0x29A)
+    ps = csaw.make_params(0, 2, ns, 1, 10, 2, seed=0x29B)
+    pwb = csaw.make_params(1, 2, nw, 1, 1, 20, seed=0x29A, schedule=csaw.SCHED_BATCHED)
+    psb = csaw.make_params(0, 2, ns, 1, 10, 2, seed=0x29B, schedule=csaw.SCHED_BATCHED)
+    t0 = time.perf_counter()
+    S = csaw.StreamGraph(g, partition_bits=pbits, slot_budget_bytes=budget, rowptr64=True)
+    res["stream_setup_s"] = time.perf_counter() - t0
     G = csaw.Graph(g, rowptr64=True)
-    sw = G.make_seeds(1 << 17, 0x29C)
-    ss = G.make_seeds(1 << 15, 0x29D)
-    outs = {k: torch.empty((4, csaw.edge_bound(p)), dtype=torch.int32, device="cuda") for k, p in (("w", pw), ("s", ps))}
+    sw = G.make_seeds(nw, 0x29C)
+    ss = G.make_seeds(ns, 0x29D)
+    outs = {k: torch.empty((3, csaw.edge_bound(p)), dtype=torch.int32, device="cuda") for k, p in (("w", pw), ("s", ps))}
+    last = {}
 
     def step(obj, batched=False):
-        a = obj.sample(pwb if batched else pw, sw, out=outs["w"])
-        b = obj.sample(psb if batched else ps, ss, out=outs["s"])
+        a = obj.sample(pwb if batched else pw, sw, out=outs["w"], with_depth=False)
+        b = obj.sample(psb if batched else ps, ss, out=outs["s"], with_depth=False)
+        last["h"] = edge_hash(outs["w"], a[0].numel()) + "|" + edge_hash(outs["s"], b[0].numel())
         return a[0].numel() + b[0].numel()
 
-    for name, obj, bt in (("stream", S, False), ("in_memory", G, False), ("in_memory_batched", G, True)):
-        for _ in range(args.warmup):
+    # above 2^31 edges the plain in-memory run (every hub step rebuilds a
+    # prefix of up to millions of edges) would take minutes: compare with
+    # the batched in-memory run only
+    big = g.n_edges > (1 << 31)
+    runs = [("stream", S, False, args.stream_warmup, args.steps)]
+    if not big:
+        runs.append(("in_memory", G, False, 0, 1))
+    runs.append(("in_memory_batched", G, True, args.stream_warmup, args.steps))
+    hashes = {}
+    for name, obj, bt, warm, steps in runs:
+        for _ in range(warm):
             step(obj, bt)
         torch.cuda.synchronize()
         i0 = S.info() if name == "stream" else None
         t0 = time.perf_counter()
-        e = sum(step(obj, bt) for _ in range(args.steps))
+        e = sum(step(obj, bt) for _ in range(steps))
         torch.cuda.synchronize()
-        dt = (time.perf_counter() - t0) / args.steps
-        r = {"ms_per_step": dt * 1e3, "edges_per_step": e / args.steps, "seps": e / args.steps / dt}
+        dt = (time.perf_counter() - t0) / steps
+        hashes[name] = last["h"]
+        r = {"ms_per_step": dt * 1e3, "steps": steps, "warmup": warm, "edges_per_step": e / steps,
+             "seps": e / steps / dt}
         if name == "stream":
             i1 = S.info()
-            r["h2d_bytes_per_step"] = (i1["bytes_h2d"] - i0["bytes_h2d"]) / args.steps
-            r["partition_loads_per_step"] = (i1["partition_loads"] - i0["partition_loads"]) / args.steps
+            r["h2d_bytes_per_step"] = (i1["bytes_h2d"] - i0["bytes_h2d"]) / steps
+            r["partition_loads_per_step"] = (i1["partition_loads"] - i0["partition_loads"]) / steps
             r["partitions"] = i1["n_partitions"]
             r["slots"] = i1["n_slots"]
             r["h2d_gbs"] = r["h2d_bytes_per_step"] / dt / 1e9
         res[name] = r
-    assert res["stream"]["edges_per_step"] == res["in_memory"]["edges_per_step"] == \
-        res["in_memory_batched"]["edges_per_step"]
-    res["stream_vs_in_memory"] = res["stream"]["seps"] / res["in_memory"]["seps"]
+    if len(set(hashes.values())) != 1:
+        raise SystemExit(f"streaming and in-memory runs emitted different edge multisets: {hashes}")
+    res["edge_multiset_hash"] = hashes
+    ref = "in_memory" if "in_memory" in res else "in_memory_batched"
+    res["stream_vs_in_memory"] = {"reference": ref, "ratio": res["stream"]["seps"] / res[ref]["seps"]}
     S.close()
     G.close()
     return res
-
 
 
 def profile_step(args):
@@ -1020,6 +1050,12 @@ def main():
                     help="time the degree rule vs the learned scheduler on a heavy-tailed R-MAT graph instead")
     ap.add_argument("--serve", action="store_true", help="run only the serving (request loop) workload")
     ap.add_argument("--stream", action="store_true", help="run only the streaming (out-of-budget) workload")
+    ap.add_argument("--stream-scale", type=int, default=26)
+    ap.add_argument("--stream-budget-gb", type=float, default=4.0)
+    ap.add_argument("--stream-pbits", type=int, default=17)
+    ap.add_argument("--stream-walks", type=int, default=1 << 17)
+    ap.add_argument("--stream-samples", type=int, default=1 << 15)
+    ap.add_argument("--stream-warmup", type=int, default=1, help="untimed streaming steps before timing")
     ap.add_argument("--serve-requests", type=int, default=4000, help="requests per serving stream")
     ap.add_argument("--forms", default="plain,batched,learned",
                     help="forms to time; the last one is reported as value (profiling runs use one form)")
