@@ -838,7 +838,9 @@ def streaming(args):
     page-locked host memory, the device partition budget capped at
     --stream-budget-gb with 2^--stream-pbits-vertex partitions; one step =
     --stream-walks edge-weight-biased walks of length 20 and --stream-samples
-    edge-weight-biased samples F1 N10 D2.  The defaults are 1/8 of the
+    edge-weight-biased samples F1 N10 D2; with --stream-cache 1 (default) the
+    streaming graph's weight-bias prefix cache is built first and streamed in
+    place of the weights.  The defaults are 1/8 of the
     scale-29 configuration (131,072 walks, 32,768 samples, 4 GiB, 2^17-vertex
     partitions: 512, as many as scale 29 has); the configuration's own shape
     is --stream-scale 28 --stream-budget-gb 32 --stream-pbits 20
@@ -872,6 +874,11 @@ def streaming(args):
     t0 = time.perf_counter()
     S = csaw.StreamGraph(g, partition_bits=pbits, slot_budget_bytes=budget, rowptr64=True)
     res["stream_setup_s"] = time.perf_counter() - t0
+    if args.stream_cache:   # the weight-bias prefix, streamed in place of the weights
+        t0 = time.perf_counter()
+        S.cache(2)
+        res["prefix_cache_build_s"] = time.perf_counter() - t0
+    res["prefix_cache"] = bool(args.stream_cache)
     G = csaw.Graph(g, rowptr64=True)
     sw = G.make_seeds(nw, 0x29C)
     ss = G.make_seeds(ns, 0x29D)
@@ -1056,6 +1063,8 @@ def main():
     ap.add_argument("--stream-walks", type=int, default=1 << 17)
     ap.add_argument("--stream-samples", type=int, default=1 << 15)
     ap.add_argument("--stream-warmup", type=int, default=1, help="untimed streaming steps before timing")
+    ap.add_argument("--stream-cache", type=int, default=1,
+                    help="1: build the streaming graph's weight-bias prefix cache (streamed in place of weights)")
     ap.add_argument("--serve-requests", type=int, default=4000, help="requests per serving stream")
     ap.add_argument("--forms", default="plain,batched,learned",
                     help="forms to time; the last one is reported as value (profiling runs use one form)")

@@ -25,7 +25,7 @@ EXPORTS = [
     "csaw_graph_stats", "csaw_graph_profile", "csaw_graph_kernel_stats", "csaw_make_seeds",
     "csaw_sample", "csaw_sample_host", "csaw_sample_batch", "csaw_sample_noalloc", "csaw_sampler_compat",
     "csaw_graph_set_option", "csaw_stream_graph_create", "csaw_stream_graph_destroy", "csaw_stream_sample",
-    "csaw_stream_stats", "csaw_sched_info", "csaw_sched_get_records", "csaw_sched_train", "csaw_sched_classes", "csaw_sched_get_model", "csaw_sched_set_model",
+    "csaw_stream_stats", "csaw_stream_graph_cache", "csaw_sched_info", "csaw_sched_get_records", "csaw_sched_train", "csaw_sched_classes", "csaw_sched_get_model", "csaw_sched_set_model",
     "csaw_mlp_grad_host", "csaw_server_create", "csaw_server_destroy", "csaw_server_submit", "csaw_server_wait",
     "csaw_server_get_stats", "csaw_graph_autotune",
 ]
@@ -138,6 +138,7 @@ def lib():
     L.csaw_stream_graph_destroy.argtypes = [p]
     L.csaw_stream_sample.argtypes = sig
     L.csaw_stream_stats.argtypes = [p, ctypes.POINTER(StreamInfo)]
+    L.csaw_stream_graph_cache.argtypes = [p, i32]
     PF = ctypes.POINTER(ctypes.c_float)
     L.csaw_sched_info.argtypes = [p, P64, ctypes.POINTER(ctypes.c_int), PF]
     L.csaw_sched_train.argtypes = [p, i32, ctypes.c_float, u64, PF]

@@ -284,6 +284,12 @@ class StreamGraph:
         except Exception:
             pass
 
+    def cache(self, bias):
+        """Builds the prefix cache of `bias` (csaw_stream_graph_cache): later
+        jobs with that bias stream each partition's prefix instead of its
+        weights and search it (the same edges)."""
+        check(lib().csaw_stream_graph_cache(self.h, BIAS_NAMES.get(bias, bias)))
+
     def info(self):
         s = _lib.StreamInfo()
         check(lib().csaw_stream_stats(self.h, ctypes.byref(s)))

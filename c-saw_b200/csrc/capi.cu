@@ -316,7 +316,7 @@ int ensure_cdf(csaw_graph_s *g, cudaStream_t st) {
     const DevGraph dg = dev_view(g);
     {
         LaunchScope ls(g, KK_INIT, st);
-        k_cdf_build<I, BIAS><<<g->sm_count * 8, 256, 0, st>>>(dg, cdf, CDF_BIG);
+        k_cdf_build<I, BIAS><<<g->sm_count * 8, 256, 0, st>>>(dg, cdf, CDF_BIG, 0, g->V);
     }
     if (g->n_big > 0) {
         const int64_t stride = ((g->maxdeg >> 5) + 1 + (g->maxdeg >> 10) + 1 + 8 + 63) & ~63ll;

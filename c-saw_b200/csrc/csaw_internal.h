@@ -117,6 +117,13 @@ struct LevelArgs {
     const int32_t *const *part_col;
     const float *const *part_w;
     int pbits;
+    // Streaming with a prefix cache: part_w holds each partition's canonical
+    // prefix (re-based like part_col), the two index levels are resident for
+    // the whole graph, and raw biases (a rebuild) are read from the
+    // page-locked host weights.
+    int part_cdf;
+    const float *cdf1_all, *cdf2_all;
+    const float *host_w;
 };
 
 // Level of input item `it`: depth, fanout, whether its children are pushed.

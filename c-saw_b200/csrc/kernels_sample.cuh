@@ -137,6 +137,20 @@ __device__ __forceinline__ int select_warp(const DevGraph &g, int64_t beg, int64
     return st.sel;
 }
 
+// Streaming: the bias bases of a resident partition -- its weights, or its
+// canonical prefix with the graph's resident index levels (raw weights, for
+// a rebuild, read from page-locked host memory).
+__device__ __forceinline__ void stream_bases(DevGraph &g, const LevelArgs &a, int part) {
+    if (a.part_cdf) {
+        g.cdf = a.part_w[part];
+        g.cdf1 = a.cdf1_all;
+        g.cdf2 = a.cdf2_all;
+        g.v.weight = a.host_w;
+    } else {
+        g.v.weight = a.part_w[part];
+    }
+}
+
 // ----------------------------------------------------- level expansion
 // One warp per queue item (grid-stride, persistent grid).  Biased items whose
 // degree exceeds WBUF are deferred to k_expand_heavy.  STREAM: each item
@@ -173,7 +187,7 @@ k_expand_warp(DevGraph g0, LevelArgs a) {
             const int part = v >> a.pbits;
             g.v.col = a.part_col[part];
             if (!g.v.col) continue;   // partition not resident this round
-            g.v.weight = a.part_w[part];
+            stream_bases(g, a, part);
         }
         int l, N;
         bool push;
@@ -234,7 +248,7 @@ k_expand_warp(DevGraph g0, LevelArgs a) {
                 nv = __shfl_sync(FULL, dst, 0);
                 if (a.part_col[nv >> a.pbits]) {
                     const int64_t nd = row_begin<I>(g, nv + 1) - row_begin<I>(g, nv);
-                    cont = !(BIASED && nd > 1 && nd > WBUF);   // the warp path can take it
+                    cont = !(BIASED && nd > 1 && nd > WBUF && !a.part_cdf);   // the warp path can take it
                 }
             }
             if (push && !cont) {
@@ -255,7 +269,7 @@ k_expand_warp(DevGraph g0, LevelArgs a) {
             N = 1;
             push = l + 1 < a.D;
             g.v.col = a.part_col[v >> a.pbits];
-            g.v.weight = a.part_w[v >> a.pbits];
+            stream_bases(g, a, v >> a.pbits);
         }
     }
     stg.flush(oa, lane);
@@ -297,7 +311,7 @@ __device__ __forceinline__ void heavy_body(const DevGraph &g0, const LevelArgs &
         if (STREAM) {   // deferred by the warp pass, so its partition is resident
             const int part = v >> a.pbits;
             g.v.col = a.part_col[part];
-            g.v.weight = a.part_w[part];
+            stream_bases(g, a, part);
         }
         const int32_t s = __ldcg(a.in_s + it);
         const uint32_t p = __ldcg(a.in_p + it);
@@ -633,11 +647,11 @@ __global__ void k_mdrw(DevGraph g, WalkArgs a) {
 // scanning on the fly).  One warp per vertex up to big_deg; vertices above go
 // to k_cdf_build_big, one CTA each.
 template <typename I, int BIAS>
-__global__ void k_cdf_build(DevGraph g, float *cdf, int64_t big_deg) {
+__global__ void k_cdf_build(DevGraph g, float *cdf, int64_t big_deg, int64_t v0, int64_t v1) {
     const int lane = threadIdx.x & 31;
     const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t v = gw; v < g.v.n_vertices; v += nw) {
+    for (int64_t v = v0 + gw; v < v1; v += nw) {
         const int64_t beg = row_begin<I>(g, v), d = row_begin<I>(g, v + 1) - beg;
         if (d <= 0 || d > big_deg) continue;
         auto wfn = [&](int64_t i) { return edge_bias<I, BIAS>(g, beg + i); };
@@ -734,6 +748,21 @@ static __global__ void k_dedup_filter(int32_t *qv, const int32_t *qs, const uint
 
 // Search index of a built prefix cache: c1[k] = cdf[32k + 31] and
 // c2[u] = cdf[1024u + 1023] where those edges exist (others are never read).
+// The index entries whose edge lies in [e0, e1): cdf1[k] = cdf[32k + 31],
+// cdf2[u] = cdf[1024u + 1023] (cdf indexed by global edge; entries past the
+// last edge are left as they are, zero).
+static __global__ void k_cdf_index_range(const float *cdf, int64_t e0, int64_t e1, float *c1, float *c2) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t k = (e0 >> 5) + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k <= (e1 - 1) >> 5; k += stride) {
+        const int64_t i = (k << 5) + 31;
+        if (i >= e0 && i < e1) c1[k] = cdf[i];
+    }
+    for (int64_t u = (e0 >> 10) + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u <= (e1 - 1) >> 10; u += stride) {
+        const int64_t j = (u << 10) + 1023;
+        if (j >= e0 && j < e1) c2[u] = cdf[j];
+    }
+}
+
 static __global__ void k_cdf_index(const float *cdf, int64_t E, float *c1, int64_t n1, float *c2, int64_t n2) {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n1; k += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = (k << 5) + 31;

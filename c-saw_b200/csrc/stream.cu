@@ -164,11 +164,16 @@ struct csaw_stream_graph_s {
     std::map<int64_t, int64_t> free_regions;   // offset -> bytes
     std::vector<int64_t> res_off;     // per partition: region offset, or -1
     std::vector<int64_t> res_bytes;
-    std::vector<char> res_w;          // region holds the partition's weights too
+    std::vector<char> res_w;          // what the region holds beside the columns (a Second)
     std::vector<int> resident;        // resident partitions, in load order
     std::vector<cudaEvent_t> ready, freed;   // per partition, created on first load
     cudaStream_t copy = nullptr;
     Buf q[3][4], counts, offsets, cursor, heavy, hscratch, ctr, skip, ptab;
+    // Prefix cache per bias kind (csaw_stream_graph_cache): the canonical
+    // prefix of every row in page-locked host memory, streamed in place of the
+    // weights, and its two index levels resident on the device.
+    float *h_cdf[4] = {};
+    float *d_idx[4] = {};             // cdf1 [(E + 31) / 32], then cdf2 [(E + 1023) / 1024]
     StreamCounters *hctr = nullptr;
     int64_t loads = 0, hits = 0, bytes_h2d = 0, launches = 0;
 };
@@ -190,10 +195,14 @@ namespace {
         if (rc_) return rc_; \
     } while (0)
 
-int64_t region_bytes(const csaw_stream_graph_s *g, int part, bool with_w) {
+// What a partition's region holds beside its columns: nothing, its weights,
+// or its rows' canonical prefix for bias kind b (SECOND_CDF + b).
+enum : int { SECOND_NONE = 0, SECOND_W = 1, SECOND_CDF = 2 };
+
+int64_t region_bytes(const csaw_stream_graph_s *g, int part, int second) {
     const int64_t ne = g->pbeg[part + 1] - g->pbeg[part];
     const int64_t colb = (4 * std::max<int64_t>(ne, 1) + 255) & ~255ll;
-    return with_w ? 2 * colb : colb;
+    return second != SECOND_NONE ? 2 * colb : colb;
 }
 
 // First-fit region of `bytes` in the arena, or -1.
@@ -234,22 +243,23 @@ int evict(csaw_stream_graph_s *g, int part) {
     return 0;
 }
 
-// Makes `part` resident (with its weights if need_w), evicting partitions
-// that are neither protected nor have pending items, oldest first; *ok is
-// false (nothing changed) when it does not fit without evicting those.
-int make_resident(csaw_stream_graph_s *g, int part, bool need_w, const std::vector<char> &protect,
+// Makes `part` resident (with the second array `second` the job needs),
+// evicting partitions that are neither protected nor have pending items,
+// oldest first; *ok is false (nothing changed) when it does not fit without
+// evicting those.
+int make_resident(csaw_stream_graph_s *g, int part, int second, const std::vector<char> &protect,
                   const std::vector<int64_t> &pend, bool *ok) {
     *ok = false;
-    const bool with_w = need_w && g->h_w;
+    const bool with_w = second != SECOND_NONE;
     if (g->res_off[part] >= 0) {
-        if (!with_w || g->res_w[part]) {
+        if (!with_w || g->res_w[part] == second) {
             g->hits++;
             *ok = true;
             return 0;
         }
-        STRY(evict(g, part));   // resident without the weights this job needs: reload
+        STRY(evict(g, part));   // resident without the array this job needs: reload
     }
-    const int64_t bytes = region_bytes(g, part, with_w);
+    const int64_t bytes = region_bytes(g, part, second);
     int64_t off = region_alloc(g, bytes);
     while (off < 0) {
         int victim = -1;
@@ -260,7 +270,7 @@ int make_resident(csaw_stream_graph_s *g, int part, bool need_w, const std::vect
             }
         if (victim < 0)
             for (int q : g->resident)   // or unusable by this job (weights missing)
-                if (!protect[q] && with_w && !g->res_w[q]) {
+                if (!protect[q] && with_w && g->res_w[q] != second) {
                     victim = q;
                     break;
                 }
@@ -277,7 +287,8 @@ int make_resident(csaw_stream_graph_s *g, int part, bool need_w, const std::vect
         SCK(cudaMemcpyAsync(g->arena + off, g->h_col + e0, sizeof(int32_t) * ne, cudaMemcpyHostToDevice, g->copy));
         g->bytes_h2d += 4 * ne;
         if (with_w) {
-            SCK(cudaMemcpyAsync(g->arena + off + bytes / 2, g->h_w + e0, sizeof(float) * ne, cudaMemcpyHostToDevice,
+            const float *src2 = second == SECOND_W ? g->h_w : g->h_cdf[second - SECOND_CDF];
+            SCK(cudaMemcpyAsync(g->arena + off + bytes / 2, src2 + e0, sizeof(float) * ne, cudaMemcpyHostToDevice,
                                 g->copy));
             g->bytes_h2d += 4 * ne;
         }
@@ -285,7 +296,7 @@ int make_resident(csaw_stream_graph_s *g, int part, bool need_w, const std::vect
     SCK(cudaEventRecord(g->ready[part], g->copy));
     g->res_off[part] = off;
     g->res_bytes[part] = bytes;
-    g->res_w[part] = with_w ? 1 : 0;
+    g->res_w[part] = (char)second;
     g->resident.push_back(part);
     g->loads++;
     *ok = true;
@@ -298,7 +309,12 @@ template <typename I, int BIAS>
 int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], const int32_t *seeds, int32_t *src,
                int32_t *dst, int32_t *smp, int32_t *dep, int64_t cap, cudaStream_t st) {
     constexpr bool BIASED = BIAS != CSAW_BIAS_UNBIASED;
-    const bool need_w = (BIAS == CSAW_BIAS_EDGE_WEIGHT || BIAS == CSAW_BIAS_HOOK) && g->h_w;
+    // the prefix cache of this bias (if built) is streamed in place of the
+    // weights; otherwise the weights, when the bias reads them
+    const bool cached = BIASED && g->h_cdf[BIAS];
+    const int second = cached ? SECOND_CDF + BIAS
+                              : (((BIAS == CSAW_BIAS_EDGE_WEIGHT || BIAS == CSAW_BIAS_HOOK) && g->h_w) ? SECOND_W
+                                                                                                     : SECOND_NONE);
     const int S = p->n_samples, F = p->mode == CSAW_MODE_WALK ? 1 : p->frontier_size, D = p->depth;
     // pending items at once: at most every item of every level
     double per = F, lvl = F;
@@ -384,7 +400,7 @@ int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], co
         // weights this job needs); if none, the next partitions of the sweep
         std::vector<int> round;
         for (int q : g->resident)
-            if (pend[q] > 0 && (!need_w || g->res_w[q])) round.push_back(q);
+            if (pend[q] > 0 && (second == SECOND_NONE || g->res_w[q] == second)) round.push_back(q);
         std::fill(in_round.begin(), in_round.end(), 0);
         if (round.empty()) {
             std::vector<int> cand;
@@ -397,12 +413,12 @@ int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], co
             }
             // most pending items per byte first
             std::stable_sort(cand.begin(), cand.end(), [&](int x, int y) {
-                return (double)pend[x] * (double)region_bytes(g, y, need_w) >
-                       (double)pend[y] * (double)region_bytes(g, x, need_w);
+                return (double)pend[x] * (double)region_bytes(g, y, second) >
+                       (double)pend[y] * (double)region_bytes(g, x, second);
             });
             for (int q : cand) {
                 bool ok = false;
-                STRY(make_resident(g, q, need_w, in_round, pend, &ok));
+                STRY(make_resident(g, q, second, in_round, pend, &ok));
                 if (!ok) break;
                 in_round[q] = 1;
                 visited[q] = 1;
@@ -428,6 +444,7 @@ int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], co
             dg.v.rowptr_is_64 = g->idx64;
             dg.v.n_vertices = g->V;
             dg.v.n_edges = g->E;
+            dg.cdf_bias = cached ? BIAS : -1;
             LevelArgs a{};
             a.in_v = qv(A, 0);
             a.in_s = qv(A, 1);
@@ -437,6 +454,12 @@ int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], co
             a.part_col = (const int32_t *const *)g->ptab.p;
             a.part_w = (const float *const *)((const void *const *)g->ptab.p + g->npart);
             a.pbits = g->pbits;
+            a.part_cdf = cached ? 1 : 0;
+            if (cached) {
+                a.cdf1_all = g->d_idx[BIAS];
+                a.cdf2_all = g->d_idx[BIAS] + ((g->E + 31) >> 5);
+                a.host_w = g->reg_w ? g->h_w : nullptr;   // page-locked in place: device-readable
+            }
             a.out_v = qv(U, 0);
             a.out_s = qv(U, 1);
             a.out_p = (uint32_t *)qv(U, 2);
@@ -595,9 +618,116 @@ extern "C" int csaw_stream_graph_destroy(csaw_stream_graph g) {
     if (g->hctr) cudaFreeHost(g->hctr);
     if (g->reg_col) cudaHostUnregister((void *)g->h_col);
     if (g->reg_w) cudaHostUnregister((void *)g->h_w);
+    for (int b = 0; b < 4; ++b) {
+        if (g->h_cdf[b]) cudaFreeHost(g->h_cdf[b]);
+        if (g->d_idx[b]) cudaFree(g->d_idx[b]);
+    }
     cudaGetLastError();
     delete g;
     return 0;
+}
+
+namespace {
+
+// Builds the prefix cache of bias kind BIAS: partition by partition, the
+// columns (and weights) go to device staging, every row's canonical prefix is
+// computed there (a warp per row, any degree: the same bits as the in-memory
+// cache, which builds large rows a CTA each), the index entries of the
+// partition's edges are written into the resident index levels, and the
+// prefix is copied to page-locked host memory.
+template <typename I, int BIAS>
+int build_stream_cdf(csaw_stream_graph_s *g) {
+    if (g->h_cdf[BIAS]) return 0;
+    const bool reads_w = BIAS == CSAW_BIAS_EDGE_WEIGHT || BIAS == CSAW_BIAS_HOOK;
+    if (reads_w && !(g->h_w && g->reg_w))
+        return csaw_host_fail(CSAW_ERR_INVALID,
+                              "the prefix cache of this bias needs page-locked weights (rebuilds read them)");
+    const int64_t E = g->E, n1 = (E + 31) >> 5, n2 = (E + 1023) >> 10, maxp = std::max<int64_t>(g->max_pedges, 1);
+    float *h = nullptr, *idx = nullptr, *stage_w = nullptr, *stage_cdf = nullptr;
+    int32_t *stage_col = nullptr;
+    auto cleanup = [&]() {
+        cudaFree(stage_col);
+        cudaFree(stage_w);
+        cudaFree(stage_cdf);
+        cudaGetLastError();
+    };
+    if (cudaHostAlloc((void **)&h, sizeof(float) * (size_t)std::max<int64_t>(E, 1), cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        return csaw_host_fail(CSAW_ERR_NOMEM, "page-locked prefix cache allocation failed");
+    }
+    if (cudaMalloc((void **)&idx, sizeof(float) * (size_t)(n1 + n2)) != cudaSuccess ||
+        cudaMalloc((void **)&stage_col, sizeof(int32_t) * (size_t)maxp) != cudaSuccess ||
+        (reads_w && cudaMalloc((void **)&stage_w, sizeof(float) * (size_t)maxp) != cudaSuccess) ||
+        cudaMalloc((void **)&stage_cdf, sizeof(float) * (size_t)maxp) != cudaSuccess) {
+        cudaGetLastError();
+        cleanup();
+        cudaFree(idx);
+        cudaFreeHost(h);
+        return csaw_host_fail(CSAW_ERR_NOMEM, "prefix cache staging allocation failed");
+    }
+    cudaStream_t st = g->copy;
+    int rc = 0;
+    auto ck = [&](cudaError_t e, const char *what) {
+        if (e != cudaSuccess && !rc) {
+            cudaGetLastError();
+            rc = csaw_host_fail(CSAW_ERR_CUDA, (std::string(what) + ": " + cudaGetErrorString(e)).c_str());
+        }
+    };
+    ck(cudaMemsetAsync(idx, 0, sizeof(float) * (size_t)(n1 + n2), st), "index clear");
+    for (int q = 0; q < g->npart && !rc; ++q) {
+        const int64_t e0 = g->pbeg[q], e1 = g->pbeg[q + 1], ne = e1 - e0;
+        if (ne == 0) continue;
+        ck(cudaMemcpyAsync(stage_col, g->h_col + e0, sizeof(int32_t) * ne, cudaMemcpyHostToDevice, st), "columns");
+        if (reads_w) ck(cudaMemcpyAsync(stage_w, g->h_w + e0, sizeof(float) * ne, cudaMemcpyHostToDevice, st), "weights");
+        DevGraph dg{};
+        dg.v.rowptr = g->d_rowptr;
+        dg.v.rowptr_is_64 = g->idx64;
+        dg.v.n_vertices = g->V;
+        dg.v.n_edges = g->E;
+        dg.v.col = stage_col - e0;   // re-based: col[e] is edge e of this partition
+        dg.v.weight = reads_w ? stage_w - e0 : nullptr;
+        dg.cdf_bias = -1;
+        const int64_t v0 = (int64_t)q << g->pbits, v1 = std::min<int64_t>(g->V, (int64_t)(q + 1) << g->pbits);
+        k_cdf_build<I, BIAS><<<g->sm_count * 8, 256, 0, st>>>(dg, stage_cdf - e0, INT64_MAX, v0, v1);
+        k_cdf_index_range<<<g->sm_count * 2, 256, 0, st>>>(stage_cdf - e0, e0, e1, idx, idx + n1);
+        g->launches += 2;
+        ck(cudaGetLastError(), "prefix build launch");
+        ck(cudaMemcpyAsync(h + e0, stage_cdf, sizeof(float) * ne, cudaMemcpyDeviceToHost, st), "prefix copy");
+        ck(cudaStreamSynchronize(st), "prefix build");   // the staging buffers are reused
+    }
+    cleanup();
+    if (rc) {
+        cudaFree(idx);
+        cudaFreeHost(h);
+        return rc;
+    }
+    g->h_cdf[BIAS] = h;
+    g->d_idx[BIAS] = idx;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" int csaw_stream_graph_cache(csaw_stream_graph g, int bias) {
+    if (!g) return csaw_host_fail(CSAW_ERR_INVALID, "graph is NULL");
+    if (bias < CSAW_BIAS_DEGREE || bias > CSAW_BIAS_HOOK) return csaw_host_fail(CSAW_ERR_INVALID, "bias must be biased");
+    if (bias == CSAW_BIAS_EDGE_WEIGHT && !g->h_w) return csaw_host_fail(CSAW_ERR_INVALID, "graph has no weights");
+    if (cudaSetDevice(g->device) != cudaSuccess) return csaw_host_fail(CSAW_ERR_CUDA, "cudaSetDevice failed");
+    if (cudaStreamSynchronize(g->copy) != cudaSuccess) {
+        cudaGetLastError();
+        return csaw_host_fail(CSAW_ERR_CUDA, "copy stream failed");
+    }
+#define CSAW_STREAM_CACHE(I)                                                  \
+    switch (bias) {                                                           \
+        case CSAW_BIAS_DEGREE: return build_stream_cdf<I, CSAW_BIAS_DEGREE>(g); \
+        case CSAW_BIAS_EDGE_WEIGHT: return build_stream_cdf<I, CSAW_BIAS_EDGE_WEIGHT>(g); \
+        default: return build_stream_cdf<I, CSAW_BIAS_HOOK>(g);               \
+    }
+    if (g->idx64) {
+        CSAW_STREAM_CACHE(int64_t)
+    }
+    CSAW_STREAM_CACHE(int32_t)
+#undef CSAW_STREAM_CACHE
 }
 
 extern "C" int csaw_stream_sample(csaw_stream_graph g, const csaw_params *p, const int32_t *seeds, int32_t *out_src,

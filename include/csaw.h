@@ -244,7 +244,8 @@ int csaw_graph_set_option(csaw_graph g, int option, int64_t value);
  * Autotuner of the launch shape for a recurring batch (the reference fixes
  * n_blocks x n_threads by hand, main.cu:219-224): times the batch under
  * each candidate
- * (grid 50/100/200 % x pairing on/off), device-timed, after one untimed run
+ * (per-level launches with grid 50/100/200 % x pairing on/off, and the
+ * persistent job kernel with pairing), device-timed, after one untimed run
  * each, and keeps the fastest in the graph's options.  The jobs' outputs are
  * overwritten by the runs (identical under every candidate).
  */
@@ -252,6 +253,7 @@ typedef struct {
     int32_t grid_pct, pair;         /* chosen shape */
     double best_ms, default_ms;     /* its time, and the default shape's */
     int32_t candidates;
+    int32_t persistent;             /* chosen: 1 = persistent job kernel */
 } csaw_tune_result;
 int csaw_graph_autotune(csaw_graph g, csaw_job *jobs, int n_jobs, void *stream, csaw_tune_result *out);
 
@@ -337,6 +339,17 @@ int csaw_stream_sample(csaw_stream_graph g, const csaw_params *p, const int32_t 
                        int32_t *out_src, int32_t *out_dst, int32_t *out_sample,
                        int32_t *out_depth, int64_t capacity, int64_t *n_out, void *stream);
 int csaw_stream_stats(csaw_stream_graph g, csaw_stream_info *out);
+/* Builds the per-vertex prefix cache of a bias kind (DEGREE, EDGE_WEIGHT or
+ * HOOK) for a streaming graph: every row's canonical prefix in page-locked
+ * host memory (4 E bytes) and its two index levels on the device (4.13 E/32
+ * bytes); later jobs with that bias stream each partition's prefix in place
+ * of its weights and search it instead of recomputing a row's prefix per
+ * expansion (raw weights, for the rare rebuild after repeated collisions,
+ * are read from the page-locked host array).  The in-memory cache's
+ * streamed-partition counterpart (SURVEY's Cp, functions.cuh:329-341);
+ * output unchanged.  Edge-weight and hook biases need the weights
+ * page-locked in place (csaw_stream_info.host_pinned_in_place bit 1). */
+int csaw_stream_graph_cache(csaw_stream_graph g, int bias);
 
 /*
  * Request loop (continuous batching).  The reference runs one synchronous

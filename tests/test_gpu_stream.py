@@ -86,3 +86,53 @@ def test_stream_weights_added_to_resident_partitions(csaw, powerlaw_small):
         a = [x.cpu().numpy() for x in sg.sample(p, sd)]
         b = oracle.run(g.rowptr, g.col, g.weight, seeds, 0, bias, 300, 1, 2, [10, 5], seed=3, n_threads=8)
         _same(a, b)
+
+
+@pytest.mark.parametrize("rowptr64", [False, True])
+@pytest.mark.parametrize("bias", [1, 2, 3])
+def test_stream_prefix_cache_equals_oracle(csaw, rmat12_pareto, rowptr64, bias):
+    """With the streaming prefix cache (csaw_stream_graph_cache) each
+    partition's canonical prefix is streamed instead of its weights and
+    searched: the edges stay the in-memory run's (and the oracle's), for
+    neighbor sampling with rebuilds and for walks, through a budget of a few
+    partitions."""
+    import torch
+    g = rmat12_pareto
+    pbits = 8
+    edges = np.diff(g.rowptr[np.minimum(np.arange(0, g.n_vertices + (1 << pbits), 1 << pbits), g.n_vertices)])
+    sg = csaw.StreamGraph(g, partition_bits=pbits, slot_budget_bytes=3 * int(edges.max()) * 8, rowptr64=rowptr64)
+    sg.cache(bias)
+    G = csaw.Graph(g, rowptr64=rowptr64)
+    deg = np.diff(g.rowptr)
+    hubs = np.argsort(deg)[-8:].astype(np.int32)
+    seeds = np.concatenate([hubs, oracle.make_seeds(g.rowptr, 2 * 200 - 8, 31 + bias)]).astype(np.int32)
+    for mode, fan, depth, n, F in ((0, [12, 6, 3], 3, 200, 2), (0, [30, 4], 2, 200, 2), (1, None, 30, 400, 1)):
+        sd = seeds[:n * F]
+        p = csaw.make_params(mode, bias, n, F, (fan or [1])[0], depth, fan, seed=0x51 + bias)
+        a = [x.cpu().numpy() for x in sg.sample(p, torch.from_numpy(sd).cuda())]
+        b = [x.cpu().numpy() for x in G.sample(p, torch.from_numpy(sd).cuda())]
+        _same(a, b)
+        if bias in (1, 2):
+            _same(a, oracle.run(g.rowptr, g.col, g.weight, sd, mode, bias, n, F, depth, fan, seed=0x51 + bias,
+                                n_threads=8))
+    info = sg.info()
+    assert info["partition_loads"] > info["n_slots"] and info["bytes_h2d"] > 0
+    sg.close()
+
+
+def test_stream_cached_and_uncached_biases_mix(csaw, rmat12_pareto):
+    """A streaming graph with a weight-bias prefix cache runs degree-biased
+    (uncached: weights not needed), weight-biased (cached) and unbiased jobs
+    in turn; resident partitions are reloaded with the array each job needs."""
+    import torch
+    g = rmat12_pareto
+    sg = csaw.StreamGraph(g, partition_bits=9, slot_budget_bytes=1 << 20)
+    sg.cache(2)
+    seeds = oracle.make_seeds(g.rowptr, 300, 5)
+    sd = torch.from_numpy(seeds).cuda()
+    for bias in (2, 1, 0, 2, 1):
+        p = csaw.make_params(0, bias, 300, 1, 10, 2, [10, 5], seed=7 + bias)
+        a = [x.cpu().numpy() for x in sg.sample(p, sd)]
+        _same(a, oracle.run(g.rowptr, g.col, g.weight, seeds, 0, bias, 300, 1, 2, [10, 5], seed=7 + bias,
+                            n_threads=8))
+    sg.close()
