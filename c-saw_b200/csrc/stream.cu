@@ -52,6 +52,8 @@ using namespace csaw;
 
 namespace {
 
+constexpr int STREAM_GROUPS = 4;   // launches a loading round is split into (copy/compute overlap)
+
 struct StreamCounters {
     unsigned long long out_count;
     unsigned long long bytes[8];
@@ -333,7 +335,7 @@ int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], co
     STRY(grow(g->offsets, sizeof(uint32_t) * (size_t)(nbins + 1)));
     STRY(grow(g->ctr, sizeof(StreamCounters)));
     STRY(grow(g->skip, (size_t)g->npart));
-    STRY(grow(g->ptab, sizeof(void *) * 2 * (size_t)g->npart));
+    STRY(grow(g->ptab, sizeof(void *) * 2 * (size_t)g->npart * STREAM_GROUPS));
     int hblocks = 0;
     int64_t hstride = 0;
     if (BIASED && g->maxdeg > WBUF) {
@@ -399,6 +401,7 @@ int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], co
         // this round: the resident partitions with pending items (with the
         // weights this job needs); if none, the next partitions of the sweep
         std::vector<int> round;
+        bool loading = false;   // this round copies partitions in
         for (int q : g->resident)
             if (pend[q] > 0 && (second == SECOND_NONE || g->res_w[q] == second)) round.push_back(q);
         std::fill(in_round.begin(), in_round.end(), 0);
@@ -425,20 +428,31 @@ int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], co
                 round.push_back(q);
             }
             if (round.empty()) return csaw_host_fail(CSAW_ERR_INVALID, "no partition fits the device budget");
+            loading = true;
         }
-        // one launch over all pending items: the round's partitions in the
-        // table, every other partition's items skipped (they stay pending)
+        // Launches over all pending items, each with a table of some of the
+        // round's partitions (every other partition's items are skipped and
+        // stay pending).  A loading round is split, in load order, into up
+        // to STREAM_GROUPS groups, each launched as soon as its own
+        // partitions have arrived, so the copies of later groups overlap the
+        // sampling of earlier ones; a round of resident partitions is one
+        // launch.
         std::fill(h_skip.begin(), h_skip.end(), 0);
-        std::fill(h_tab.begin(), h_tab.end(), nullptr);
-        for (int part : round) {
-            SCK(cudaStreamWaitEvent(st, g->ready[part], 0));
-            h_skip[part] = 1;
-            unsigned char *base = g->arena + g->res_off[part];
-            h_tab[part] = (const int32_t *)base - g->pbeg[part];
-            if (g->res_w[part]) h_tab[g->npart + part] = (const float *)(base + g->res_bytes[part] / 2) - g->pbeg[part];
-        }
-        SCK(cudaMemcpyAsync(g->ptab.p, h_tab.data(), sizeof(void *) * h_tab.size(), cudaMemcpyHostToDevice, st));
-        {
+        for (int part : round) h_skip[part] = 1;
+        const int ngroups = loading ? std::min<int>(STREAM_GROUPS, (int)round.size()) : 1;
+        for (int k = 0; k < ngroups; ++k) {
+            const size_t lo = round.size() * k / ngroups, hi = round.size() * (k + 1) / ngroups;
+            std::fill(h_tab.begin(), h_tab.end(), nullptr);
+            for (size_t r = lo; r < hi; ++r) {
+                const int part = round[r];
+                SCK(cudaStreamWaitEvent(st, g->ready[part], 0));
+                unsigned char *base = g->arena + g->res_off[part];
+                h_tab[part] = (const int32_t *)base - g->pbeg[part];
+                if (g->res_w[part])
+                    h_tab[g->npart + part] = (const float *)(base + g->res_bytes[part] / 2) - g->pbeg[part];
+            }
+            const void **tab = (const void **)g->ptab.p + (size_t)k * 2 * g->npart;
+            SCK(cudaMemcpyAsync(tab, h_tab.data(), sizeof(void *) * h_tab.size(), cudaMemcpyHostToDevice, st));
             DevGraph dg{};
             dg.v.rowptr = g->d_rowptr;
             dg.v.rowptr_is_64 = g->idx64;
@@ -451,8 +465,8 @@ int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], co
             a.in_p = (const uint32_t *)qv(A, 2);
             a.in_dep = qv(A, 3);
             a.n_in = &c->n_pend;
-            a.part_col = (const int32_t *const *)g->ptab.p;
-            a.part_w = (const float *const *)((const void *const *)g->ptab.p + g->npart);
+            a.part_col = (const int32_t *const *)tab;
+            a.part_w = (const float *const *)(tab + g->npart);
             a.pbits = g->pbits;
             a.part_cdf = cached ? 1 : 0;
             if (cached) {
@@ -489,8 +503,8 @@ int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], co
                 k_expand_heavy<I, BIAS, true><<<hblocks, HEAVY_THREADS, 0, st>>>(dg, a);
                 g->launches++;
             }
+            for (size_t r = lo; r < hi; ++r) SCK(cudaEventRecord(g->freed[round[r]], st));
         }
-        for (int part : round) SCK(cudaEventRecord(g->freed[part], st));
         SCK(cudaMemcpyAsync(d_skip, h_skip.data(), (size_t)g->npart, cudaMemcpyHostToDevice, st));
         STRY(rebin(true));
     }
