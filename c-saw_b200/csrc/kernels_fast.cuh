@@ -29,10 +29,7 @@ constexpr int WF = 512;  // per-warp shared prefix capacity of the fast kernels
 #ifndef CSAW_PAIR_MIN_BLOCKS
 #define CSAW_PAIR_MIN_BLOCKS 4
 #endif
-// 1: the pair pass defers each item's emission by one item (see pair_body).
-#ifndef CSAW_PAIR_PIPELINE
-#define CSAW_PAIR_PIPELINE 0
-#endif
+
 constexpr int FAST_THREADS = 256;
 
 // Canonical prefix of a single tile held one element per lane (w = 0 for
@@ -370,7 +367,9 @@ __global__ void k_init_queue_fast(DevGraph g, const int32_t *seeds, uint32_t n, 
     qd[i] = (int32_t)(row_begin<I>(g, v + 1) - b);
 }
 
-// Writes one output edge and, on inner levels, the child queue item.
+// Emitting an edge: emit_load reads the selected neighbor (its record on
+// inner levels), emit_finish writes the output edge and, on inner levels,
+// the child queue item; emit_edge does both.
 template <typename I>
 __device__ __forceinline__ NbrRec emit_load(const DevGraph &g, const LevelArgs &a, int64_t e) {
     NbrRec r;
@@ -799,16 +798,6 @@ __device__ __forceinline__ void pair_body(const DevGraph &g, const LevelArgs &a,
     int off = 0;
     uint32_t i = gh;
     if (i < n) off = request(__ldcg(&a.pair_list[i].beg), __ldcg(&a.pair_list[i].d));
-#if CSAW_PAIR_PIPELINE
-    // The previous item's emission, deferred by one item: its neighbor
-    // gathers are issued right after its draws and consumed after this
-    // item's staging and draws, so their latency overlaps them.
-    bool pend = false;
-    NbrRec prec{};
-    int32_t pv = 0, ps = 0;
-    uint32_t pp = 0, pq = 0;
-    unsigned long long pob = 0;
-#endif
     for (; i < n; i += nh) {
         const uint32_t inext = i + nh;
         long long nbeg = 0;
@@ -845,11 +834,6 @@ __device__ __forceinline__ void pair_body(const DevGraph &g, const LevelArgs &a,
         }
         __syncwarp(h.mask);   // every read of the buffer is done: it is free
         if (inext < n) off = request(nbeg, nd);
-#if CSAW_PAIR_PIPELINE
-        if (pend && h.sl < N)
-            emit_finish<I>(g, a, prec, pv, ps, pp * (uint32_t)N + (uint32_t)h.sl, (int64_t)pob + h.sl, pq + (uint32_t)h.sl);
-        pend = false;
-#endif
         if (!ok) {   // rebuild needed: a whole warp redoes the item (in shared memory up to WF)
             if (h.sl == 0) {
                 if (d <= WF) a.refill_list[atomicAdd(a.n_refill, 1u)] = en;
@@ -857,19 +841,9 @@ __device__ __forceinline__ void pair_body(const DevGraph &g, const LevelArgs &a,
             }
             continue;
         }
-#if CSAW_PAIR_PIPELINE
-        if (h.sl < N) prec = emit_load<I>(g, a, beg + sel);
-        pv = en.v;
-        ps = en.s;
-        pp = en.p;
-        pq = en.q;
-        pob = en.ob;
-        pend = true;
-#else
         if (h.sl < N)
             emit_edge<I>(g, a, beg + sel, en.v, en.s, en.p * (uint32_t)N + (uint32_t)h.sl, (int64_t)en.ob + h.sl,
                          en.q + (uint32_t)h.sl);
-#endif
         if (rec) {
             __syncwarp(h.mask);
             if (h.sl == 0)
@@ -882,10 +856,6 @@ __device__ __forceinline__ void pair_body(const DevGraph &g, const LevelArgs &a,
                                                             (a.push ? 12ull + 2 * (sizeof(I) + 4) : 0ull));
         }
     }
-#if CSAW_PAIR_PIPELINE
-    if (pend && h.sl < N)
-        emit_finish<I>(g, a, prec, pv, ps, pp * (uint32_t)N + (uint32_t)h.sl, (int64_t)pob + h.sl, pq + (uint32_t)h.sl);
-#endif
 #pragma unroll
     for (int o = 16; o; o >>= 1) {
         my_bytes += __shfl_xor_sync(FULL, my_bytes, o);
