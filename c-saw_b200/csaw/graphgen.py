@@ -167,7 +167,10 @@ def rmat_device_bucketed(scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=0, wei
     assert buckets & (buckets - 1) == 0 and shift > 0
     ab, abc = a + b, a + b + c
     rowptr = np.zeros(V + 1, dtype=np.int64)
-    cols, ws = [], []
+    # filled in place (the generated edge count bounds the deduplicated one),
+    # so host memory peaks near the final graph size
+    col_all = np.empty(E, dtype=np.int32)
+    w_all = None if weight == "none" else np.empty(E, dtype=np.float32)
     total = 0
     for bk in range(buckets):
         gen = torch.Generator(device=device)
@@ -195,8 +198,7 @@ def rmat_device_bucketed(scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=0, wei
         del src
         rowptr[lo + 1:lo + 1 + (1 << shift)] = total + torch.cumsum(counts, 0).cpu().numpy()
         m = col.numel()
-        total += m
-        cols.append(col.cpu().numpy())
+        col_all[total:total + m] = col.cpu().numpy()
         del col
         wgen = torch.Generator(device=device)
         wgen.manual_seed(seed + 1 + bk)
@@ -209,14 +211,13 @@ def rmat_device_bucketed(scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=0, wei
             w = None
         else:
             raise ValueError(weight)
-        ws.append(None if w is None else w.float().cpu().numpy())
+        if w is not None:
+            w_all[total:total + m] = w.float().cpu().numpy()
+        total += m
         del w
         torch.cuda.empty_cache()
-    col = np.concatenate(cols)
-    del cols
-    w = None if ws[0] is None else np.concatenate(ws)
-    del ws
-    return CSR(rowptr, col, w, name=f"rmat{scale}_ef{edge_factor}_dev")
+    return CSR(rowptr, col_all[:total], None if w_all is None else w_all[:total],
+               name=f"rmat{scale}_ef{edge_factor}_dev")
 
 
 def powerlaw_directed(n_vertices=875_713, n_edges=5_105_039, gamma=2.1, max_degree=460, zipf=0.6,
