@@ -78,12 +78,13 @@ WORKLOADS = {
         text="(a) degree-biased neighbor sampling {na} samples F4 N20 D3 + (b) degree-biased random walks {nb} x 64"),
 }
 FLUSH_BYTES = 256 << 20
-KINDS = ("expand", "select", "hub", "pair", "heavy", "walk", "walk_thread", "setup")
+KINDS = ("expand", "select", "select_thread", "hub", "pair", "heavy", "walk", "walk_thread", "setup")
 TRAFFIC_TABLE = os.path.join(ROOT, "profiles", "dram_traffic_rmat22.md")
 
 
 def kernel_name(kind, batched):
     return {"expand": "k_coop_fast" if batched else "k_expand_warp", "select": "k_select_fast",
+            "select_thread": "k_select_thread",
             "hub": "k_select_hub", "pair": "k_select_pair", "heavy": "k_expand_heavy",
             "walk": "k_walk_fast" if batched else "k_walk_warp",
             "walk_thread": "k_walk_thread_fast" if batched else "k_walk_thread", "setup": "setup"}[kind]
@@ -855,8 +856,7 @@ def streaming(args):
     sc = args.stream_scale
     t0 = time.perf_counter()
     if sc >= 27:
-        g = graphgen.rmat_device_bucketed(scale=sc, buckets=16 if sc <= 28 else 32,
-                                          **{k: v for k, v in STREAM_GRAPH.items()})
+        g = graphgen.rmat_device_bucketed(scale=sc, **{k: v for k, v in STREAM_GRAPH.items()})
     else:
         g = graphgen.rmat_device(scale=sc, symmetrize=False, **STREAM_GRAPH)
     gen_s = time.perf_counter() - t0

@@ -17,7 +17,7 @@ GRAPH_DEGREE_BIAS, GRAPH_CDF_CACHE, GRAPH_NO_CDF_CACHE = 1, 2, 4
 PARAM_DEDUP = 1
 MAX_DEPTH = 64
 KERNEL_KINDS = {"expand": 0, "heavy": 1, "walk": 2, "mdrw": 3, "setup": 4, "select": 5, "hub": 6, "pair": 7,
-                "walk_thread": 8, "persist": 9}
+                "walk_thread": 8, "persist": 9, "select_thread": 10}
 
 # Every symbol include/csaw.h declares (tests check the library exports them).
 EXPORTS = [
@@ -36,7 +36,8 @@ OPT_PAIR = 4
 OPT_HOST_PARTS = 5
 OPT_RETRY_SMEM = 6
 OPT_PERSISTENT = 7
-MLP_NPARAM, MLP_NORM = 1542, 18
+OPT_THREAD_SELECT = 8
+MLP_NPARAM, MLP_NORM = 1575, 18
 
 
 class CsawError(RuntimeError):

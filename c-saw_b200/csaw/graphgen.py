@@ -150,32 +150,25 @@ def rmat_device(scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=0, symmetrize=T
     return out
 
 
-def rmat_device_bucketed(scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=0, weight="uniform", buckets=16,
-                         device="cuda", chunk=1 << 26):
+def rmat_device_bucketed(scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=0, weight="uniform",
+                         max_bucket_edges=1 << 30, device="cuda", chunk=1 << 26):
     """Directed R-MAT as rmat_device() for graphs whose edge keys do not fit
     one on-device sort (scales 27-29): the edge stream (same quadrant rule,
-    one torch Philox generator seeded with `seed`) is generated once per
-    source range of V / buckets vertices, keeping only that range's edges,
-    which are deduplicated and turned into that range's CSR rows, then
-    moved to host memory.  Every pass replays the same stream, so the
-    buckets partition one graph; self-loops and duplicates are removed.
+    one torch Philox generator seeded with `seed`) is replayed once to count
+    edges per coarse source range, the ranges are merged into buckets of at
+    most max_bucket_edges generated edges (R-MAT puts most edges on low
+    source ids, so equal ranges would not do), then replayed once per bucket,
+    keeping that bucket's edges, which are deduplicated and turned into its
+    CSR rows in host memory.  Self-loops and duplicates are removed.
     Weights come from a generator seeded with seed + 1 + bucket."""
     import torch
     V = 1 << scale
     E = edge_factor * V
-    shift = scale - int(np.log2(buckets))
-    assert buckets & (buckets - 1) == 0 and shift > 0
     ab, abc = a + b, a + b + c
-    rowptr = np.zeros(V + 1, dtype=np.int64)
-    # filled in place (the generated edge count bounds the deduplicated one),
-    # so host memory peaks near the final graph size
-    col_all = np.empty(E, dtype=np.int32)
-    w_all = None if weight == "none" else np.empty(E, dtype=np.float32)
-    total = 0
-    for bk in range(buckets):
+
+    def stream():
         gen = torch.Generator(device=device)
         gen.manual_seed(seed)
-        keys = []
         for off in range(0, E, chunk):
             n = min(chunk, E - off)
             s = torch.zeros(n, dtype=torch.int64, device=device)
@@ -185,18 +178,44 @@ def rmat_device_bucketed(scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=0, wei
                 s |= (r >= ab).to(torch.int64) << bit
                 d |= (((r >= a) & (r < ab)) | (r >= abc)).to(torch.int64) << bit
                 del r
-            keep = ((s >> shift) == bk) & (s != d)
+            yield s, d
+            del s, d
+
+    cbits = min(16, scale - 1)
+    cshift = scale - cbits
+    counts = torch.zeros(1 << cbits, dtype=torch.int64, device=device)
+    for s, d in stream():
+        counts += torch.bincount(s >> cshift, minlength=1 << cbits)
+    counts = counts.cpu().numpy()
+    bounds = [0]   # coarse range boundaries of the buckets
+    acc = 0
+    for k, n in enumerate(counts):
+        if acc and acc + n > max_bucket_edges:
+            bounds.append(k)
+            acc = 0
+        acc += int(n)
+    bounds.append(1 << cbits)
+    rowptr = np.zeros(V + 1, dtype=np.int64)
+    # filled in place (the generated edge count bounds the deduplicated one),
+    # so host memory peaks near the final graph size
+    col_all = np.empty(E, dtype=np.int32)
+    w_all = None if weight == "none" else np.empty(E, dtype=np.float32)
+    total = 0
+    for bk in range(len(bounds) - 1):
+        lo, hi = bounds[bk] << cshift, bounds[bk + 1] << cshift
+        keys = []
+        for s, d in stream():
+            keep = (s >= lo) & (s < hi) & (s != d)
             keys.append(torch.unique(s[keep] * V + d[keep]))
-            del s, d, keep
+            del keep
         key = torch.unique(torch.cat(keys))
         del keys
         src = key // V
         col = (key % V).to(torch.int32)
         del key
-        lo = bk << shift
-        counts = torch.bincount(src - lo, minlength=1 << shift)
+        cnt = torch.bincount(src - lo, minlength=hi - lo)
         del src
-        rowptr[lo + 1:lo + 1 + (1 << shift)] = total + torch.cumsum(counts, 0).cpu().numpy()
+        rowptr[lo + 1:hi + 1] = total + torch.cumsum(cnt, 0).cpu().numpy()
         m = col.numel()
         col_all[total:total + m] = col.cpu().numpy()
         del col
@@ -215,7 +234,8 @@ def rmat_device_bucketed(scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=0, wei
             w_all[total:total + m] = w.float().cpu().numpy()
         total += m
         del w
-        torch.cuda.empty_cache()
+        if device != "cpu":
+            torch.cuda.empty_cache()
     return CSR(rowptr, col_all[:total], None if w_all is None else w_all[:total],
                name=f"rmat{scale}_ef{edge_factor}_dev")
 

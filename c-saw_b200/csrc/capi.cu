@@ -54,7 +54,7 @@ int fail(int code, const std::string &msg) {
     } while (0)
 
 enum { KK_EXPAND = 0, KK_HEAVY = 1, KK_WALK = 2, KK_MDRW = 3, KK_INIT = 4, KK_SELECT = 5, KK_HUB = 6, KK_PAIR = 7,
-       KK_WALK_THREAD = 8, KK_PERSIST = 9, KK_COUNT = 10 };
+       KK_WALK_THREAD = 8, KK_PERSIST = 9, KK_SELECT_THREAD = 10, KK_COUNT = 11 };
 
 struct Counters {
     unsigned long long out_count;
@@ -68,6 +68,7 @@ struct Counters {
     uint32_t n_hub;
     uint32_t n_pair;
     uint32_t n_refill;
+    uint32_t n_thread;
     int err;
 };
 
@@ -120,7 +121,8 @@ constexpr size_t MAX_WARM = 1024;                   // batch keys remembered for
 // on its own stream, so independent jobs overlap on the device.
 struct JobCtx {
     DevBuf q[2][5], heavy, sel, hlist, hscratch, wscratch, seeds_in, out_dev, cta[4], retry, stab, hubsel, pairsel, dedup,
-        pctr;   // per-level counters and barrier words of a persistent job
+        pctr,   // per-level counters and barrier words of a persistent job
+        tsel;   // thread-per-item list
     Counters *ctr = nullptr, *hctr = nullptr;
     cudaStream_t stream = nullptr;   // owned (batch jobs); job 0 uses the caller's
     cudaEvent_t done = nullptr;
@@ -159,7 +161,8 @@ struct csaw_graph_s {
     int host_parts = 0;           // CSAW_OPT_HOST_PARTS (0: by output size; -1: copy after the job)
     int retry_smem = 0;           // CSAW_OPT_RETRY_SMEM (bytes)
     bool persistent = false;      // CSAW_OPT_PERSISTENT
-    uint32_t class_mask = 0x3f;   // classes the trained model picks (bit c)
+    int thread_sel = 1;           // CSAW_OPT_THREAD_SELECT: 0 off, 1 degree rule, 2 every d <= 32 item
+    uint32_t class_mask = 0x7f;   // classes the trained model picks (bit c)
     int32_t *big_verts = nullptr; // vertices above CDF_BIG (the cache builds them one CTA each)
     int64_t n_big = 0;
     NbrRec *nrec = nullptr;       // per-edge neighbor records (batched schedules)
@@ -361,9 +364,9 @@ int sched_for(csaw_graph_s *g, int schedule, int bias, int warp_slots, cudaStrea
     *out = nullptr;
     if (schedule != CSAW_SCHED_LEARNED || bias == CSAW_BIAS_UNBIASED) return 0;
     SchedArgs h{};
-    // a trained model that picks no CTA class routes exactly as the degree
-    // rule; one that lost its timed trial is not used
-    bool routes = g->trained && (g->class_mask & 0x3cu) && !g->mlp_lost;
+    // a trained model that picks neither a CTA class nor the thread class
+    // leaves the degree rule in place; one that lost its timed trial is not used
+    bool routes = g->trained && (g->class_mask & 0x7cu) && !g->mlp_lost;
     if (routes && g->trial) routes = g->trial_arm == 1;
     h.mode = g->recording ? SCHED_RECORD : (routes ? SCHED_MLP : SCHED_THRESHOLD);
     h.wq = g->mlp_wq;
@@ -511,6 +514,7 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
     const int sgrid = plain ? 0
                       : shaped(cached ? grid_for(k_select_fast<I, BIAS, true>, FAST_THREADS, 0, g->sm_count)
                                       : grid_for(k_select_fast<I, BIAS, false>, FAST_THREADS, 0, g->sm_count));
+    const int tgrid = plain ? 0 : shaped(grid_for(k_select_thread<I, BIAS>, FAST_THREADS, 0, g->sm_count));
     if (!plain) {
         TRY(ensure_nbr(g, st));
         TRY(ensure(c->sel, sizeof(SelEntry) * qcap, st));
@@ -524,6 +528,7 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
         for (int k = 0; k < 4; ++k)
             if (sched || k == 1) TRY(ensure(c->cta[k], sizeof(SelEntry) * qcap, st));
         if (sched && g->sched_host.mode == SCHED_MLP) TRY(ensure(c->stab, 2 * TAB_N, st));
+        if (BIASED && g->thread_sel) TRY(ensure(c->tsel, sizeof(SelEntry) * qcap, st));
     }
     const bool tabled = sched && g->sched_host.mode == SCHED_MLP;
     // CTA classes launched: those the model may pick, and CTA-256 wherever the
@@ -626,6 +631,13 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
         a.n_refill = &c->ctr->n_refill;
         a.retry_list = (SelEntry *)c->retry.p;
         a.n_retry = &c->ctr->n_retry;
+        // a thread list where some item of the level may take the thread class
+        // (the degree rule sends none when N > 16)
+        const bool thr_level = !plain && BIASED && g->thread_sel &&
+                               (g->thread_sel == 2 || sched != nullptr || fan[l] <= THREAD_RULE_MAX_N);
+        a.thread_list = thr_level ? (SelEntry *)c->tsel.p : nullptr;
+        a.n_thread = &c->ctr->n_thread;
+        a.thread_force = g->thread_sel == 2;
         a.heavy_scratch = (float *)c->hscratch.p;
         a.heavy_stride = hstride;
         a.heavy_smem = 0;   // only the retry launch below has dynamic shared memory
@@ -676,6 +688,8 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
                 a.n_hub = &pc[l].n_hub;
                 a.n_pair = &pc[l].n_pair;
                 a.n_refill = &pc[l].n_refill;
+                a.thread_list = nullptr;   // the thread pass's registers do not fit the persistent kernel
+                a.n_thread = &pc[l].n_thread;
                 a.refill_list = (SelEntry *)c->cta[1].p;   // the warp list is still being read beside the pair pass
                 pa.lv[l] = a;
                 LevelArgs ar = a;
@@ -717,11 +731,12 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
         for (int l = 0; l < D; ++l) {
             const int cur = l & 1, nxt = cur ^ 1;
             CK(cudaMemsetAsync(&c->ctr->nq[nxt], 0, sizeof(uint32_t), st));
-            CK(cudaMemsetAsync(&c->ctr->n_heavy, 0, 10 * sizeof(uint32_t), st));  // n_heavy .. n_refill
+            CK(cudaMemsetAsync(&c->ctr->n_heavy, 0, 11 * sizeof(uint32_t), st));  // n_heavy .. n_thread
             LevelArgs a = make_level(l);
             if (tabled) {
                 LaunchScope ls(g, KK_INIT, st);
-                k_sched_table<<<TAB_N * 32 / 256, 256, 0, st>>>(sched, a.n_in, a.N, l, (uint8_t *)c->stab.p);
+                k_sched_table<<<TAB_N * 32 / 256, 256, 0, st>>>(sched, a.n_in, a.N, l, a.thread_list != nullptr,
+                                                                 (uint8_t *)c->stab.p);
             }
             {
                 LaunchScope ls(g, KK_EXPAND, st);
@@ -750,6 +765,10 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
                 LaunchScope ls(g, KK_SELECT, st);
                 if (cached) k_select_fast<I, BIAS, true><<<sgrid, FAST_THREADS, 0, st>>>(dg, a);
                 else k_select_fast<I, BIAS, false><<<sgrid, FAST_THREADS, 0, st>>>(dg, a);
+            }
+            if (a.thread_list) {
+                LaunchScope ls(g, KK_SELECT_THREAD, st);
+                k_select_thread<I, BIAS><<<tgrid, FAST_THREADS, 0, st>>>(dg, a);
             }
             // with the pair list, every cached hub (d > WF >= 4N) is paired:
             // the hub list stays empty
@@ -1009,10 +1028,10 @@ int enqueue_job(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int32_t 
 constexpr int TRIAL_RUNS = 3;
 
 // Starts the timed trial of a freshly trained or loaded model (only when it
-// would route some items to CTA classes; otherwise it equals the degree rule).
+// picks some CTA class or the thread class; otherwise the degree rule stays).
 void start_trial(csaw_graph_s *g) {
     g->mlp_lost = false;
-    g->trial = g->trained && (g->class_mask & 0x3cu);
+    g->trial = g->trained && (g->class_mask & 0x7cu);
     g->trial_arm = 1;
     g->trial_n[0] = g->trial_n[1] = 0;
     g->trial_ms[0] = g->trial_ms[1] = 0.0;
@@ -1700,6 +1719,11 @@ extern "C" int csaw_graph_set_option(csaw_graph g, int option, int64_t value) {
             if (value < -1 || value > MAX_HOST_PARTS) return fail(CSAW_ERR_INVALID, "host parts must be in [-1, 8]");
             g->host_parts = (int)value;
             return 0;
+        case CSAW_OPT_THREAD_SELECT:
+            if (value < 0 || value > 2) return fail(CSAW_ERR_INVALID, "thread select: 0, 1 or 2");
+            g->thread_sel = (int)value;
+            ++g_alloc_epoch;   // launch structure is baked into cached graphs
+            return 0;
         case CSAW_OPT_PERSISTENT:
             g->persistent = value != 0;
             ++g_alloc_epoch;   // launch structure is baked into cached graphs
@@ -1787,9 +1811,10 @@ extern "C" int csaw_sched_info(csaw_graph g, int64_t *n_records, int *trained, f
 }
 
 // Class mask of a trained model: classes 0 and 1 always (the warp pass),
-// CTA classes only where the model picks them on its training records.
+// CTA classes and the thread class only where the model picks them on its
+// training records.
 static int pick_classes(csaw_graph_s *g, int n) {
-    g->class_mask = 0x3f;
+    g->class_mask = 0x7f;
     if (n <= 0) return 0;
     uint32_t *m = nullptr;
     CK(cudaMalloc((void **)&m, sizeof(uint32_t)));
@@ -1808,7 +1833,7 @@ static int pick_classes(csaw_graph_s *g, int n) {
 
 extern "C" int csaw_sched_classes(csaw_graph g, uint32_t *mask) {
     if (!g || !mask) return fail(CSAW_ERR_INVALID, "NULL argument");
-    *mask = !g->trained ? 0x3fu : (g->mlp_lost ? 0x3u : g->class_mask);
+    *mask = !g->trained ? 0x7fu : (g->mlp_lost ? 0x3u : g->class_mask);
     return 0;
 }
 
@@ -1886,7 +1911,7 @@ extern "C" int csaw_sched_set_model(csaw_graph g, const float *params, const flo
     k_mlp_to_bf16<<<(MLP_NPARAM + 255) / 256, 256>>>(g->mlp_w, g->mlp_wq);
     CK(cudaGetLastError());
     CK(cudaDeviceSynchronize());
-    g->class_mask = 0x3f;   // no training records to prune by
+    g->class_mask = 0x7f;   // no training records to prune by
     g->trained = true;
     start_trial(g);
     g->recording = false;

@@ -91,6 +91,9 @@ struct LevelArgs {
     uint32_t *n_refill;
     SelEntry *retry_list;     // batched: cached hubs the warp pass handed back
     uint32_t *n_retry;
+    SelEntry *thread_list;    // batched: thread-class items (N < d <= 32), a thread each, or null
+    uint32_t *n_thread;
+    int thread_force;         // the degree rule sends every N < d <= 32 item to the thread list
     const SchedArgs *sched;   // learned scheduler, or null (degree rule)
     float *heavy_scratch;     // per-CTA scratch for the heavy kernel
     int64_t heavy_stride;     // floats per CTA

@@ -425,6 +425,7 @@ __device__ __forceinline__ void coop_body(const DevGraph &g, const LevelArgs &a)
     const int N = a.N;
     const bool cached = BIASED && g.cdf && g.cdf_bias == BIAS;
     const bool routed = BIASED && a.sched && a.sched->mode != SCHED_THRESHOLD;
+    const bool thr_ok = BIASED && a.thread_list != nullptr;
     const int nout = 2 + (a.o_smp != nullptr) + (a.o_dep != nullptr);
     const unsigned long long per_edge = 4ull + 4ull * nout + (a.push ? 12ull + 2 * (sizeof(I) + 4) : 0ull);
     uint32_t bs = (n + nw - 1) / nw;
@@ -447,10 +448,9 @@ __device__ __forceinline__ void coop_body(const DevGraph &g, const LevelArgs &a)
         const bool drawn = k > 0 && d > N;
         // execution class of items that need draws: degree rule, or learned
         int cls = 1;
-        if (drawn && BIASED) cls = threshold_class(d, WF, cached);
+        if (drawn && BIASED) cls = rule_class(d, N, n, WF, cached, thr_ok, a.thread_force);
         if (routed && a.sched_tab) {   // trained model: one table load per item
-            if (drawn && d > 32) cls = table_class(a.sched_tab, d, a.sched->vstats[v], N, WF, cached);
-            else if (drawn) cls = 0;
+            if (drawn) cls = table_class(a.sched_tab, d, a.sched->vstats[v], N, WF, cached);
         } else if (routed) {
             float2 st = make_float2(0.f, 0.f);
             if (drawn) st = a.sched->vstats[v];
@@ -465,15 +465,17 @@ __device__ __forceinline__ void coop_body(const DevGraph &g, const LevelArgs &a)
                 hb ^= hb >> 15;
                 hb *= 0x2C1B3C6Du;
                 hb ^= hb >> 13;
-                const int c = choose_class(a.sched, a.sched->wq, db, N, sb, n, a.depth, hb, WF, cached, lane);
+                const int c = choose_class(a.sched, a.sched->wq, db, N, sb, n, a.depth, hb, WF, cached, thr_ok, lane);
                 if (lane == b) cls = c;
             }
         }
-        const bool heavy = drawn && cls >= 2;
+        // thread class: one item per thread (valid only with a thread list)
+        const bool thr = drawn && cls == CLS_THREAD;
+        const bool heavy = drawn && cls >= 2 && !thr;
         // cached items with few slots and a rare rebuild run two per warp;
         // other warp-class items above WF search the cached prefix in their own list
-        const bool pair = drawn && !heavy && cached && N <= 16 && d >= 4 * N && a.pair_list;
-        const bool hub = drawn && !heavy && cached && d > WF && !pair;
+        const bool pair = drawn && !heavy && !thr && cached && N <= 16 && d >= 4 * N && a.pair_list;
+        const bool hub = drawn && !heavy && !thr && cached && d > WF && !pair;
         const int incl = warp_incl_scan(k, lane);
         const int excl = incl - k;
         const int K = __shfl_sync(FULL, incl, 31);
@@ -488,13 +490,22 @@ __device__ __forceinline__ void coop_body(const DevGraph &g, const LevelArgs &a)
             qb = __shfl_sync(FULL, qb, 0);
         }
         // hand off items that need draws, with their reserved slots
-        const unsigned sm = __ballot_sync(FULL, drawn && !heavy && !hub && !pair);
+        const unsigned sm = __ballot_sync(FULL, drawn && !heavy && !hub && !pair && !thr);
         if (sm) {
             uint32_t pos = 0;
             if (lane == 0) pos = atomicAdd(a.n_sel, (uint32_t)__popc(sm));
             pos = __shfl_sync(FULL, pos, 0);
-            if (drawn && !heavy && !hub && !pair)
+            if (drawn && !heavy && !hub && !pair && !thr)
                 a.sel_list[pos + __popc(sm & ((1u << lane) - 1u))] =
+                    SelEntry{it, qb + (uint32_t)excl, ob + excl, v, s, p, (int32_t)d, (long long)beg, cls, 0};
+        }
+        const unsigned tm = __ballot_sync(FULL, thr);
+        if (tm) {
+            uint32_t pos = 0;
+            if (lane == 0) pos = atomicAdd(a.n_thread, (uint32_t)__popc(tm));
+            pos = __shfl_sync(FULL, pos, 0);
+            if (thr)
+                a.thread_list[pos + __popc(tm & ((1u << lane) - 1u))] =
                     SelEntry{it, qb + (uint32_t)excl, ob + excl, v, s, p, (int32_t)d, (long long)beg, cls, 0};
         }
         const unsigned pbm = __ballot_sync(FULL, pair);
@@ -646,6 +657,135 @@ template <typename I, int BIAS, bool CACHED>
 __global__ void __launch_bounds__(FAST_THREADS, 4)
 k_select_fast(DevGraph g, LevelArgs a) {
     select_fast_body<I, BIAS, CACHED>(g, a);
+}
+
+// ------------------------------------------------ thread-per-item selection
+// One thread runs one item with N < d <= 32 (biased) through the whole
+// selection, serially in slot order, exactly as the semantics define it:
+// the row's canonical prefix lives in 32 registers (the same Kogge-Stone
+// additions and running max as the warp's tile scan, so the same bits), a
+// draw's index is the number of prefix values <= t (the prefix is monotone),
+// selected indices are a 32-bit mask, a slot that has drawn REJECT_ATTEMPTS
+// times in a phase rebuilds the prefix with the selected neighbors zeroed,
+// and zero mass or MAX_SLOT_DRAWS takes the smallest unselected index.  The
+// slots' indices go to shared memory and the edges are emitted afterwards,
+// four slots at a time, so an item's neighbor gathers are in flight together
+// instead of one per slot.  A warp thus carries 32 items instead of one.
+
+constexpr int THREAD_SEL_SLOTS = 32;   // N < d <= 32
+
+// Canonical prefix of the (at most 32) biases of row [beg, beg + d), the
+// neighbors in zmask counted as zero; returns T.
+template <typename I, int BIAS>
+__device__ __forceinline__ float thread_tile_prefix(const DevGraph &g, int64_t beg, int d, uint32_t zmask,
+                                                    float (&P)[32]) {
+#pragma unroll
+    for (int i = 0; i < 32; ++i) P[i] = (i < d && !((zmask >> i) & 1u)) ? edge_bias<I, BIAS>(g, beg + i) : 0.f;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+#pragma unroll
+        for (int i = 31; i >= off; --i) P[i] = __fadd_rn(P[i], P[i - off]);
+    }
+    float m = 0.f;
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+        const float pi = i < d ? __fadd_rn(0.f, __fadd_rn(0.f, P[i])) : 0.f;
+        m = fmaxf(m, pi);
+        P[i] = m;
+    }
+    return P[31];
+}
+
+// Selects the item's N slots; slot j's neighbor index goes to sidx[j * stride].
+template <typename I, int BIAS>
+__device__ __forceinline__ void select_thread_item(const DevGraph &g, const LevelArgs &a, const SelEntry &en, int N,
+                                                   uint8_t *sidx, int stride) {
+    const int64_t beg = en.beg;
+    const int d = en.d;
+    const DrawCtx dc{a.k0, a.k1, en.p, (uint32_t)en.s, (uint32_t)a.depth};
+    float P[32];
+    float T = thread_tile_prefix<I, BIAS>(g, beg, d, 0u, P);
+    uint32_t selmask = 0;
+    for (int j = 0; j < N; ++j) {
+        SlotRng rng;
+        int A = 0, ph = 0, idx = 0;
+        for (;;) {
+            if (!(T > 0.f) || A == MAX_SLOT_DRAWS) {   // no mass left, or the slot's draw guard
+                idx = __ffs(~selmask) - 1;
+                break;
+            }
+            if (ph == REJECT_ATTEMPTS) {   // new phase: the selected neighbors zeroed out of the prefix
+                T = thread_tile_prefix<I, BIAS>(g, beg, d, selmask, P);
+                ph = 0;
+                continue;
+            }
+            const float t = its_target(rng.word(dc, j, A), T);
+            ++A;
+            ++ph;
+            idx = 0;
+#pragma unroll
+            for (int i = 0; i < 32; ++i) idx += P[i] <= t ? 1 : 0;
+            if (!((selmask >> idx) & 1u)) break;
+        }
+        selmask |= 1u << idx;
+        sidx[j * stride] = (uint8_t)idx;
+    }
+}
+
+#ifndef CSAW_THREAD_SEL_MIN_BLOCKS
+#define CSAW_THREAD_SEL_MIN_BLOCKS 3
+#endif
+
+template <typename I, int BIAS>
+__device__ __forceinline__ void select_thread_body(const DevGraph &g, const LevelArgs &a) {
+    __shared__ uint8_t s_idx[THREAD_SEL_SLOTS * FAST_THREADS];   // [slot][thread]
+    const int lane = threadIdx.x & 31;
+    const uint32_t n = __ldcg(a.n_thread);
+    const uint32_t n_level = __ldcg(a.n_in);
+    const int N = a.N;
+    const int nout = 2 + (a.o_smp != nullptr) + (a.o_dep != nullptr);
+    const bool rec = a.sched && a.sched->mode == SCHED_RECORD;
+    uint8_t *sidx = s_idx + threadIdx.x;
+    unsigned long long my_bytes = 0, my_items = 0;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        long long t0 = 0;
+        if (rec) t0 = clock64();
+        select_thread_item<I, BIAS>(g, a, load_sel(a.thread_list + i), N, sidx, FAST_THREADS);
+        // the entry again (an L1/L2 hit): its emission fields stay out of the
+        // selection loop's registers
+        const SelEntry en = load_sel(a.thread_list + i);
+        for (int j0 = 0; j0 < N; j0 += 4) {
+            NbrRec r[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (j0 + u < N) r[u] = emit_load<I>(g, a, en.beg + sidx[(j0 + u) * FAST_THREADS]);
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (j0 + u < N)
+                    emit_finish<I>(g, a, r[u], en.v, en.s, en.p * (uint32_t)N + (uint32_t)(j0 + u),
+                                   (int64_t)en.ob + j0 + u, en.q + (uint32_t)(j0 + u));
+        }
+        if (rec) record_profile(a.sched, en.d, N, a.sched->vstats[en.v], n_level, a.depth, en.cls, clock64() - t0);
+        my_items++;
+        my_bytes += 16 + 4ull * en.d +
+                    (unsigned long long)N * (4ull + 4ull * nout + (a.push ? 12ull + 2 * (sizeof(I) + 4) : 0ull));
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        my_bytes += __shfl_xor_sync(FULL, my_bytes, o);
+        my_items += __shfl_xor_sync(FULL, my_items, o);
+    }
+    if (lane == 0 && my_items) {
+        atomicAdd(&a.bytes[10], my_bytes);
+        atomicAdd(&a.items[10], my_items);
+    }
+}
+
+template <typename I, int BIAS>
+__global__ void __launch_bounds__(FAST_THREADS, CSAW_THREAD_SEL_MIN_BLOCKS)
+k_select_thread(DevGraph g, LevelArgs a) {
+    select_thread_body<I, BIAS>(g, a);
 }
 
 // Half-warp primitives: a warp runs two independent items, lanes 0-15 and

@@ -41,7 +41,7 @@ struct PersistLevelCtr {
     uint32_t n_hub;
     uint32_t n_pair;
     uint32_t n_refill;
-    uint32_t pad;
+    uint32_t n_thread;   // unused: a persistent job has no thread list
 };
 
 struct PersistArgs {

@@ -1,17 +1,20 @@
 // sched_mlp.cuh -- learned execution-granularity scheduler (sm_100a).
 //
 // For every frontier item that needs draws (d > N, biased), the batched
-// expansion can run it at one of six granularities:
+// expansion can run it at one of seven granularities:
 //   0 warp, registers (d <= 32)      1 warp, shared memory (d <= WF)
 //   2 CTA of 128 threads            3 CTA of 256     4 CTA of 512     5 CTA of 1024
+//   6 one thread (d <= 32, the row's prefix in its registers; 32 items a warp)
 // The choice never changes the output (every draw is keyed by the work item),
-// only the time.  The plain rule picks by degree (0 / 1 / 3).  The learned rule
-// runs a small MLP (8 -> 32 -> 32 -> 6, ReLU, 1542 parameters) on per-item
-// features and predicts each class's latency (normalised log2 cycles); the
-// class chosen minimises predicted latency x (1 + u (warps - 1)), where
-// u in [0, 1] grows with the level's size relative to the warp slots: a small
-// frontier leaves warps idle, so wide CTAs cost little; a large one is
-// throughput-bound, so warps are weighed in.
+// only the time.  The degree rule picks 0 / 1 / 3, and 6 for d <= 32 when
+// N <= 16 and the level is large (rule_class).  The learned rule runs a small
+// MLP (8 -> 32 -> 32 -> 7, ReLU, 1575 parameters) on per-item features and
+// predicts each class's latency (normalised log2 cycles); the class chosen
+// minimises predicted latency x (1 + u (width - 1)), width in warps (1/32 for
+// a thread), where u in [0, 1] grows with the level's size relative to the
+// warp slots: a small frontier leaves warps idle, so wide CTAs cost little and
+// narrow threads gain little; a large one is throughput-bound, so width is
+// weighed in.
 //
 // Features (all cheap per item): log2 d, log2 N, log2(d/N), coefficient of
 // variation of the neighbor biases, collision estimate N * sum p_i^2 (both
@@ -32,16 +35,23 @@
 
 namespace csaw {
 
-constexpr int MLP_IN = 8, MLP_H = 32, MLP_OUT = 6;
+constexpr int MLP_IN = 8, MLP_H = 32, MLP_OUT = 7;
 constexpr int MLP_W1 = 0;                              // [32][8]
 constexpr int MLP_B1 = MLP_W1 + MLP_H * MLP_IN;        // [32]
 constexpr int MLP_W2 = MLP_B1 + MLP_H;                 // [32][32]
 constexpr int MLP_B2 = MLP_W2 + MLP_H * MLP_H;         // [32]
-constexpr int MLP_W3 = MLP_B2 + MLP_H;                 // [6][32]
-constexpr int MLP_B3 = MLP_W3 + MLP_OUT * MLP_H;       // [6]
-constexpr int MLP_NPARAM = MLP_B3 + MLP_OUT;           // 1542
+constexpr int MLP_W3 = MLP_B2 + MLP_H;                 // [7][32]
+constexpr int MLP_B3 = MLP_W3 + MLP_OUT * MLP_H;       // [7]
+constexpr int MLP_NPARAM = MLP_B3 + MLP_OUT;           // 1575
 constexpr int MLP_NORM = 2 * MLP_IN + 2;               // x mean/std, y mean/std
-constexpr int N_CLASSES = 6;
+constexpr int N_CLASSES = 7;
+constexpr int CLS_THREAD = 6;
+constexpr uint32_t CLS_CTA_MASK = 0x3cu;   // classes 2..5
+// The degree rule's thread class: levels of at least this many items (fewer
+// leave most warps idle when 32 items share one), at most this many draws
+// per item (a thread runs its slots one after another).
+constexpr uint32_t THREAD_RULE_MIN_ITEMS = 1u << 16;
+constexpr int THREAD_RULE_MAX_N = 16;
 
 enum : int { SCHED_THRESHOLD = 0, SCHED_MLP = 1, SCHED_RECORD = 2 };
 
@@ -64,7 +74,10 @@ struct SchedArgs {
     uint32_t class_mask;           // SCHED_MLP: classes the model may pick (bit c)
 };
 
-__device__ __forceinline__ int class_warps(int c) { return c <= 1 ? 1 : (4 << (c - 2)); }
+// Width of a class in warps.
+__device__ __forceinline__ float class_width(int c) {
+    return c == CLS_THREAD ? 1.f / 32.f : (c <= 1 ? 1.f : (float)(4 << (c - 2)));
+}
 
 // Item features (shared by the router and the profile recorders).
 __device__ __forceinline__ void item_features(float x[MLP_IN], int64_t d, int N, float2 st, uint32_t n_level,
@@ -82,10 +95,11 @@ __device__ __forceinline__ void item_features(float x[MLP_IN], int64_t d, int N,
 // Valid classes for degree d (bit c set if class c can run the item).
 // With the per-vertex prefix cache, class 1 (one warp) also takes items above
 // wf: it searches the cached prefix instead of building one in shared memory.
-__device__ __forceinline__ unsigned valid_classes(int64_t d, int wf, bool cached) {
-    unsigned m = 0x3cu;              // CTAs always
+// thr: the job has a thread list (batched, biased, not disabled).
+__device__ __forceinline__ unsigned valid_classes(int64_t d, int wf, bool cached, bool thr) {
+    unsigned m = CLS_CTA_MASK;       // CTAs always
     if (d <= wf || cached) m |= 0x2u;
-    if (d <= 32) m |= 0x1u;
+    if (d <= 32) m |= thr ? 0x41u : 0x1u;
     return m;
 }
 
@@ -93,8 +107,16 @@ __device__ __forceinline__ int threshold_class(int64_t d, int wf, bool cached) {
     return d <= 32 ? 0 : ((d <= wf || cached) ? 1 : 3);
 }
 
+// The degree rule with the thread class: one-tile rows with few draws, on
+// large levels, run a thread each (every one-tile row when forced).
+__device__ __forceinline__ int rule_class(int64_t d, int N, uint32_t n_level, int wf, bool cached, bool thr,
+                                          bool force = false) {
+    if (thr && d <= 32 && (force || (N <= THREAD_RULE_MAX_N && n_level >= THREAD_RULE_MIN_ITEMS))) return CLS_THREAD;
+    return threshold_class(d, wf, cached);
+}
+
 // Warp-cooperative MLP inference for one item (warp-uniform x); returns the
-// predicted normalised log2 latency of class `lane` on lanes 0..5.
+// predicted normalised log2 latency of class `lane` on lanes 0..6.
 // W: the bf16 weights (3 KB, read through the read-only cache).
 __device__ __forceinline__ float mlp_infer(const __nv_bfloat16 *W, const float *norm, const float x[MLP_IN], int lane) {
     float h = __bfloat162float(__ldg(W + MLP_B1 + lane));
@@ -118,13 +140,13 @@ __device__ __forceinline__ float mlp_infer(const __nv_bfloat16 *W, const float *
 }
 
 // Cheapest class among `valid` from the predicted normalised log2 latency y
-// of class `lane` (lanes 0..5), or -1 when `valid` is empty.
+// of class `lane` (lanes 0..6), or -1 when `valid` is empty.
 __device__ __forceinline__ int class_argmin(float y, const float *norm, uint32_t n_level, int warp_slots,
                                             unsigned valid, int lane) {
     const float u = fminf(1.f, (float)n_level / (16.f * (float)warp_slots));
-    // predicted latency in cycles (up to the common scale), weighted by warps
+    // predicted latency in cycles (up to the common scale), weighted by width
     float cost = exp2f(y * norm[2 * MLP_IN + 1] + norm[2 * MLP_IN]) *
-                 (1.f + u * (float)(class_warps(lane < MLP_OUT ? lane : 0) - 1));
+                 (1.f + u * (class_width(lane < MLP_OUT ? lane : 0) - 1.f));
     if (lane >= MLP_OUT || !((valid >> lane) & 1u)) cost = __int_as_float(0x7f800000);   // +inf
     // argmin over lanes 0..7 (ties: lowest class)
     int best = lane;
@@ -144,10 +166,9 @@ __device__ __forceinline__ int class_argmin(float y, const float *norm, uint32_t
 // Class for one drawn biased item (warp-uniform inputs; all lanes call).
 __device__ __forceinline__ int choose_class(const SchedArgs *sa, const __nv_bfloat16 *W, int64_t d, int N, float2 st,
                                             uint32_t n_level, int depth, uint32_t hash, int wf, bool cached,
-                                            int lane) {
-    const unsigned valid = valid_classes(d, wf, cached);
-    if (!sa || sa->mode == SCHED_THRESHOLD) return threshold_class(d, wf, cached);
-    if (sa->mode == SCHED_MLP && d <= 32) return 0;   // one tile in registers: nothing cheaper
+                                            bool thr, int lane) {
+    const unsigned valid = valid_classes(d, wf, cached, thr);
+    if (!sa || sa->mode == SCHED_THRESHOLD) return rule_class(d, N, n_level, wf, cached, thr);
     if (sa->mode == SCHED_RECORD) {
         const int nv = __popc(valid);
         int pick = (int)(hash % (uint32_t)nv);
@@ -159,26 +180,34 @@ __device__ __forceinline__ int choose_class(const SchedArgs *sa, const __nv_bflo
     item_features(x, d, N, st, n_level, depth, sa->bias_kind, sa->warp_slots);
     const float y = mlp_infer(W, sa->norm, x, lane);
     const int best = class_argmin(y, sa->norm, n_level, sa->warp_slots, valid & sa->class_mask, lane);
-    return best >= 0 ? best : threshold_class(d, wf, cached);
+    return best >= 0 ? best : rule_class(d, N, n_level, wf, cached, thr);
 }
 
 // ------------------------------------------------------- decision table
 // Per level, the model is evaluated once per cell of a grid over the three
-// per-item features that vary within a level (log2 d in half steps from 5,
-// CoV in half steps, N sum p^2 in unit steps; the level's N, size, depth and
-// bias fixed), and the expansion kernel routes each item by one table load.
-// Each cell holds two picks: over classes 1..5 (the item fits a warp: d <= WF
-// or a cached prefix) and over the CTA classes 2..5 (255: none allowed).
+// per-item features that vary within a level (degree: steps of 4 up to 32,
+// then log2 d in half steps from 5; CoV in half steps; N sum p^2 in unit
+// steps; the level's N, size, depth and bias fixed), and the expansion kernel
+// routes each item by one table load.  Each cell holds two picks: over the
+// classes valid for a warp-sized item (0, 1, the CTAs and the thread for
+// d <= 32; 1 and the CTAs above) and over the CTA classes 2..5 (255: none
+// allowed).
+constexpr int TAB_SMALL = 8;   // degree bins of d <= 32
 constexpr int TAB_D = 40, TAB_C = 8, TAB_P = 8, TAB_N = TAB_D * TAB_C * TAB_P;
 
+__device__ __forceinline__ int tab_degree_bin(int64_t d) {
+    if (d <= 32) return (int)((d - 1) >> 2);
+    return min(TAB_D - 1, TAB_SMALL + max(0, (int)((__log2f((float)d) - 5.f) * 2.f)));
+}
+
 __device__ __forceinline__ int tab_index(int64_t d, float2 st, int N) {
-    const int bd = min(TAB_D - 1, max(0, (int)((__log2f((float)d) - 5.f) * 2.f)));
+    const int bd = tab_degree_bin(d);
     const int bc = min(TAB_C - 1, max(0, (int)(st.x * 2.f)));
     const int bp = min(TAB_P - 1, max(0, (int)fminf(8.f, (float)N * st.y)));
     return (bd * TAB_C + bc) * TAB_P + bp;
 }
 
-// Class of a drawn item with d > 32 from the level's table.
+// Class of a drawn item from the level's table (built with the same thr).
 __device__ __forceinline__ int table_class(const uint8_t *tab, int64_t d, float2 st, int N, int wf, bool cached) {
     const bool warp_ok = cached || d <= wf;
     const int c = tab[2 * tab_index(d, st, N) + (warp_ok ? 0 : 1)];
@@ -186,13 +215,17 @@ __device__ __forceinline__ int table_class(const uint8_t *tab, int64_t d, float2
 }
 
 // One warp per cell; n_level read on the device (the level's item count).
-static __global__ void k_sched_table(const SchedArgs *sa, const uint32_t *n_in, int N, int depth, uint8_t *tab) {
+// thr: the level has a thread list.
+static __global__ void k_sched_table(const SchedArgs *sa, const uint32_t *n_in, int N, int depth, int thr,
+                                     uint8_t *tab) {
     const int lane = threadIdx.x & 31;
     const int cell = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (cell >= TAB_N) return;
     const int bp = cell % TAB_P, bc = (cell / TAB_P) % TAB_C, bd = cell / (TAB_P * TAB_C);
     const uint32_t n_level = *n_in;
-    const float ld = 5.f + ((float)bd + 0.5f) * 0.5f, lN = __log2f((float)N);
+    const bool small = bd < TAB_SMALL;
+    const float ld = small ? __log2f(4.f * (float)bd + 2.5f) : 5.f + ((float)(bd - TAB_SMALL) + 0.5f) * 0.5f;
+    const float lN = __log2f((float)N);
     float x[MLP_IN];
     x[0] = ld;
     x[1] = lN;
@@ -203,8 +236,11 @@ static __global__ void k_sched_table(const SchedArgs *sa, const uint32_t *n_in, 
     x[6] = (float)depth;
     x[7] = (float)sa->bias_kind;
     const float y = mlp_infer(sa->wq, sa->norm, x, lane);
-    const int a = class_argmin(y, sa->norm, n_level, sa->warp_slots, sa->class_mask & 0x3eu, lane);
-    const int b = class_argmin(y, sa->norm, n_level, sa->warp_slots, sa->class_mask & 0x3cu, lane);
+    // a small cell's degree d may be below N: such items take all their
+    // neighbors and are never routed, so the cell's pick does not matter
+    const unsigned va = small ? (0x3fu | (thr ? 0x40u : 0u)) : 0x3eu;
+    const int a = class_argmin(y, sa->norm, n_level, sa->warp_slots, sa->class_mask & va, lane);
+    const int b = class_argmin(y, sa->norm, n_level, sa->warp_slots, sa->class_mask & CLS_CTA_MASK, lane);
     if (lane == 0) {
         tab[2 * cell] = (uint8_t)(a < 0 ? 255 : a);
         tab[2 * cell + 1] = (uint8_t)(b < 0 ? 255 : b);
@@ -220,11 +256,10 @@ static __global__ void k_sched_pick(const ProfRec *rec, int n, const __nv_bfloat
     for (int i = gw; i < n; i += nw) {
         const float *x = rec[i].x;
         const int64_t d = (int64_t)(exp2f(x[0]) + 0.5f);
-        if (d <= 32) continue;
         const uint32_t n_level = (uint32_t)((exp2f(x[5]) - 1.f) * (float)warp_slots + 0.5f);
         const float y = mlp_infer(W, norm, x, lane);
-        const int a = class_argmin(y, norm, n_level, warp_slots, valid_classes(d, wf, false) & 0x3eu, lane);
-        const int b = class_argmin(y, norm, n_level, warp_slots, valid_classes(d, wf, true) & 0x3eu, lane);
+        const int a = class_argmin(y, norm, n_level, warp_slots, valid_classes(d, wf, false, true), lane);
+        const int b = class_argmin(y, norm, n_level, warp_slots, valid_classes(d, wf, true, true), lane);
         if (lane == 0) {
             if (a >= 0) atomicOr(mask, 1u << a);
             if (b >= 0) atomicOr(mask, 1u << b);

@@ -143,7 +143,7 @@ int csaw_graph_stats(csaw_graph g, csaw_stats *out);
  * with one thread per walk (unbiased walks; many biased walks over a cached
  * prefix), 9 persistent job kernel (every level of a batched neighbor job in
  * one launch; its bytes and items are counted under the kinds of the passes
- * it runs).
+ * it runs), 10 batched thread-per-item selection (N < d <= 32).
  */
 int csaw_graph_profile(csaw_graph g, int enable);
 int csaw_graph_kernel_stats(csaw_graph g, int kind, double *ms, int64_t *launches,
@@ -236,7 +236,14 @@ enum {
      * 0 (default): one launch per pass and level.  Applies to degree-rule
      * jobs over a cached prefix (or unbiased) without dedup, up to 4 levels;
      * others use the per-level launches.  Never changes the output. */
-    CSAW_OPT_PERSISTENT = 7
+    CSAW_OPT_PERSISTENT = 7,
+    /* Thread class of batched biased items with N < d <= 32 (one thread
+     * each, the row's prefix in registers, 32 items per warp, instead of a
+     * warp each).  1 (default): the degree rule uses it when N <= 16 on
+     * levels of at least 65,536 items, and the learned scheduler may pick
+     * it; 2: the degree rule uses it for every such item; 0: never.  Never
+     * changes the output. */
+    CSAW_OPT_THREAD_SELECT = 8
 };
 int csaw_graph_set_option(csaw_graph g, int option, int64_t value);
 
@@ -260,24 +267,28 @@ int csaw_graph_autotune(csaw_graph g, csaw_job *jobs, int n_jobs, void *stream, 
 /*
  * Learned execution-granularity scheduler (CSAW_SCHED_LEARNED).  Replaces
  * the reference's fixed warp-per-vertex schedule (main.cu:60-91); it never
- * changes the output.  An MLP 8 -> 32 -> 32 -> 6 predicts, per item that
- * needs draws, the latency of six granularities (warp in registers, warp in
- * shared memory, CTA of 128/256/512/1024 threads); without a trained model
- * the degree rule is used.  csaw_sched_train fits it on the GPU (FP32 forward
- * and backward kernels, full-batch Adam) to the recorded profiles;
- * csaw_mlp_grad_host exposes the mean loss and gradient for checking.
- * Parameter layout: W1[32][8] b1[32] W2[32][32] b2[32] W3[6][32] b3[6]
- * (1542 floats); norm: x mean[8], x std[8], y mean, y std (18 floats).
+ * changes the output.  An MLP 8 -> 32 -> 32 -> 7 predicts, per item that
+ * needs draws, the latency of seven granularities (class 0 warp in
+ * registers, 1 warp in shared memory, 2-5 CTA of 128/256/512/1024 threads,
+ * 6 one thread, for d <= 32 in batched jobs with CSAW_OPT_THREAD_SELECT on);
+ * without a trained model the degree rule is used (0 / 1 / CTA-256 by degree,
+ * 6 for d <= 32 with N <= 16 on levels of at least 65,536 items).
+ * csaw_sched_train fits it on the GPU (FP32 forward and backward kernels,
+ * full-batch Adam) to the recorded profiles; csaw_mlp_grad_host exposes the
+ * mean loss and gradient for checking.
+ * Parameter layout: W1[32][8] b1[32] W2[32][32] b2[32] W3[7][32] b3[7]
+ * (1575 floats); norm: x mean[8], x std[8], y mean, y std (18 floats).
  * Profile record: float x[8], int32 class, float cycles (40 bytes).
  */
 int csaw_sched_info(csaw_graph g, int64_t *n_records, int *trained, float *last_loss);
 int csaw_sched_get_records(csaw_graph g, void *out, int64_t max_n, int64_t *n);
 int csaw_sched_train(csaw_graph g, int epochs, float lr, uint64_t seed, float *final_loss);
 /* Classes a trained model may pick (bit c for class c).  Training keeps the
- * warp classes 0 and 1 and the CTA classes the model picks on its own
- * training records; only those CTA widths are launched (plus CTA-256 for hubs
- * above 512 edges without a cached prefix).  0x3f when untrained.  A trained
- * (or loaded) model that routes items to CTA classes is then on trial: the
+ * warp classes 0 and 1 and the CTA classes and thread class the model picks
+ * on its own training records; only those CTA widths are launched (plus
+ * CTA-256 for hubs above 512 edges without a cached prefix).  0x7f when
+ * untrained.  A trained (or loaded) model that routes items to CTA classes or
+ * the thread class is then on trial: the
  * next learned biased neighbor jobs alternate between its routing and the
  * degree rule, timed on the device, three runs each; if its mean time is not
  * lower it is not used and the mask reads 0x3 (the degree rule).  Output is

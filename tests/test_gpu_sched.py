@@ -25,7 +25,7 @@ def np_loss_grad(w, norm, rec):
     w = w.astype(np.float64)
     W1 = w[0:256].reshape(32, 8); b1 = w[256:288]
     W2 = w[288:1312].reshape(32, 32); b2 = w[1312:1344]
-    W3 = w[1344:1536].reshape(6, 32); b3 = w[1536:1542]
+    W3 = w[1344:1568].reshape(7, 32); b3 = w[1568:1575]
     x = (rec["x"].astype(np.float64) - norm[:8]) / norm[8:16]
     a1 = x @ W1.T + b1; h1 = np.maximum(a1, 0)
     a2 = h1 @ W2.T + b2; h2 = np.maximum(a2, 0)
@@ -47,11 +47,11 @@ def np_loss_grad(w, norm, rec):
 def test_mlp_gradient_matches_numpy(csaw):
     from csaw.sampler import PROF_DTYPE, mlp_grad
     rng = np.random.default_rng(0)
-    w = (rng.standard_normal(1542) * 0.3).astype(np.float32)
+    w = (rng.standard_normal(1575) * 0.3).astype(np.float32)
     norm = np.concatenate([rng.standard_normal(8), 0.5 + rng.random(8), [10.0, 2.0]]).astype(np.float32)
     rec = np.zeros(777, dtype=PROF_DTYPE)
     rec["x"] = rng.standard_normal((777, 8)) * 2
-    rec["cls"] = rng.integers(0, 6, 777)
+    rec["cls"] = rng.integers(0, 7, 777)
     rec["cycles"] = 2.0 ** rng.uniform(8, 14, 777)
     loss, g = mlp_grad(w, norm, rec)
     rl, rg = np_loss_grad(w, norm, rec)
