@@ -47,6 +47,24 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
                  : "memory");
 }
 
+// Three copies completing one phase together (sizes multiples of 16, 0 for
+// none; addresses 16-byte aligned): one arrival expecting all their bytes.
+__device__ __forceinline__ void bulk_copy_tx(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_load3(void *d0, const void *s0, uint32_t b0, void *d1, const void *s1, uint32_t b1,
+                                           void *d2, const void *s2, uint32_t b2, uint64_t *bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(b0 + b1 + b2)
+                 : "memory");
+    if (b0) bulk_copy_tx(d0, s0, b0, bar);
+    if (b1) bulk_copy_tx(d1, s1, b1, bar);
+    if (b2) bulk_copy_tx(d2, s2, b2, bar);
+}
+
 __device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(

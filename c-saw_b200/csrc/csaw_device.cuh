@@ -128,6 +128,20 @@ __device__ __forceinline__ int search_upper32(const float *P, int d, float t) {
     return lo;
 }
 
+// The same index by binary lifting in a fixed LOG steps, for d <= 2^LOG: no
+// data-dependent loop (lanes and half-warps searching rows of different
+// lengths stay converged); the last element is never read.
+template <int LOG>
+__device__ __forceinline__ int search_upper_lift(const float *P, int d, float t) {
+    int lo = 0;
+#pragma unroll
+    for (int step = 1 << (LOG - 1); step >= 1; step >>= 1) {
+        const int idx = lo + step - 1;
+        if (idx < d - 1 && !(P[idx] > t)) lo += step;
+    }
+    return lo;
+}
+
 // The same index for one warp-uniform target, found by the whole warp with a
 // 32-way search: each round probes the last element of 32 equal chunks of the
 // remaining range and keeps the first chunk whose probe exceeds t, so a

@@ -867,26 +867,43 @@ __device__ __forceinline__ StagePlan stage_plan(const DevGraph &g, int64_t beg, 
     return StagePlan{STAGE_NONE, nullptr, 0};
 }
 
-// cdf_search with the plan's index level staged in S (shared): the same
-// index (the first i with P[i] > t is unique), the staged level searched in
-// shared memory, the rest in global memory one 128-byte line per level.
-// As in cdf_search, no level probes its last candidate.
-__device__ __forceinline__ int64_t staged_cdf_search(const DevGraph &g, const StagePlan &sp, const float *S,
-                                                     int64_t beg, int64_t d, float t) {
+// cdf_search for an item whose index level is staged (STAGE_CDF1 /
+// STAGE_CDF2), once the staged entries' search has given r: the remaining
+// levels in global memory, one 32-entry line each, by fixed-step lifting.
+// The same index as cdf_search (the first i with P[i] > t is unique); as
+// there, no level reads its last candidate.
+__device__ __forceinline__ int64_t staged_refine(const DevGraph &g, int mode, int r, int64_t beg, int64_t d, float t) {
     const int64_t end = beg + d;
-    if (sp.mode == STAGE_NONE) return cdf_search(g, beg, d, t);
     int64_t k;
-    if (sp.mode == STAGE_CDF1) {
-        k = (beg >> 5) + search_upper32(S, sp.count, t);
+    if (mode == STAGE_CDF1) {
+        k = (beg >> 5) + r;
     } else {
-        const int64_t u = (beg >> 10) + search_upper32(S, sp.count, t);
+        const int64_t u = (beg >> 10) + r;
         const int64_t ka = (u << 5) > (beg >> 5) ? (u << 5) : (beg >> 5);
         const int64_t kb = (u << 5) + 31 < ((end - 1) >> 5) ? (u << 5) + 31 : ((end - 1) >> 5);
-        k = ka + search_upper(g.cdf1 + ka, kb - ka + 1, t);
+        k = ka + search_upper_lift<5>(g.cdf1 + ka, (int)(kb - ka + 1), t);
     }
     const int64_t ia = (k << 5) > beg ? (k << 5) : beg;
     const int64_t ib = (k << 5) + 31 < end - 1 ? (k << 5) + 31 : end - 1;
-    return ia + search_upper(g.cdf + ia, ib - ia + 1, t) - beg;
+    return ia + search_upper_lift<5>(g.cdf + ia, (int)(ib - ia + 1), t) - beg;
+}
+
+// Shared-memory copy of a work entry (three 16-byte loads).
+__device__ __forceinline__ SelEntry load_sel_smem(const SelEntry *e) {
+    const int4 *q = reinterpret_cast<const int4 *>(e);
+    const int4 x = q[0], y = q[1], z = q[2];
+    SelEntry r;
+    r.it = (uint32_t)x.x;
+    r.q = (uint32_t)x.y;
+    r.ob = ((unsigned long long)(uint32_t)x.w << 32) | (uint32_t)x.z;
+    r.v = y.x;
+    r.s = y.y;
+    r.p = (uint32_t)y.z;
+    r.d = y.w;
+    r.beg = (long long)(((unsigned long long)(uint32_t)z.y << 32) | (uint32_t)z.x);
+    r.cls = z.z;
+    r.pad = z.w;
+    return r;
 }
 
 // Counted bytes of the prefix reads of one item (4 bytes per element staged
@@ -903,17 +920,24 @@ __device__ __forceinline__ unsigned long long staged_bytes(const StagePlan &sp, 
 
 // Level expansion, part 2 for items over a cached prefix with N <= 16 and
 // d >= 4N (a rebuild is rare): two items per warp, one per half-warp, lanes
-// N..15 of a half idle instead of N..31 of a warp.  Rows up to WF edges are
-// staged in shared memory by the bulk copy engine and searched there; the
-// next item's row is requested as soon as the current item's draws are
-// resolved, so its transfer overlaps the current item's edge emission
-// (dependent neighbor-record gathers and stores).  Larger rows are searched
-// in global memory through the prefix index.  Items that need a rebuild are
-// redone from scratch: rows up to WF by k_select_fast on the refill list
-// (written over the consumed warp list), larger ones by the CTA pass.
+// N..15 of a half idle instead of N..31 of a warp.  For each item the bulk
+// copy engine stages, on one barrier: its work entry, the 16 bytes holding
+// its prefix total T, and what its draws search (stage_plan: the prefix row
+// up to WF edges, else the row's entries of the first or second prefix index
+// level).  The next item's copies are requested as soon as the current
+// item's draws are resolved, so they overlap the current item's edge
+// emission (dependent neighbor-record gathers and stores).  Every draw
+// searches the staged array in shared memory by fixed-step lifting; index
+// entries then lead to one 32-entry line per remaining level in global
+// memory, so rows and hubs share one resolver loop.  Items that need a
+// rebuild are redone from scratch: rows up to WF edges by k_select_fast on
+// the refill list (written over the consumed warp list), larger ones by the
+// CTA pass.
+constexpr int PAIR_ENT = 16;   // floats of a half's entry slot: the 48-byte entry and the 16-byte T window
+
 template <typename I, int BIAS>
-__device__ __forceinline__ void pair_body(const DevGraph &g, const LevelArgs &a, float *buf, uint64_t *bar,
-                                          uint32_t &parity) {
+__device__ __forceinline__ void pair_body(const DevGraph &g, const LevelArgs &a, float *buf, float *ebuf,
+                                          uint64_t *bar, uint32_t &parity) {
     const int lane = threadIdx.x & 31;
     const Half h(lane);
     const uint32_t gh = (blockIdx.x * blockDim.x + threadIdx.x) >> 4;
@@ -923,57 +947,55 @@ __device__ __forceinline__ void pair_body(const DevGraph &g, const LevelArgs &a,
     const int N = a.N;
     const int nout = 2 + (a.o_smp != nullptr) + (a.o_dep != nullptr);
     unsigned long long my_bytes = 0, my_items = 0;
-    // requests the staged copy of what an item searches (stage_plan); returns
-    // the copy's offset in the buffer
-    auto request = [&](long long rbeg, int rd) -> int {
+    // requests the staged copies of item idx (row range rbeg, rd); returns the
+    // offset of its staged array in the buffer
+    auto request = [&](uint32_t idx, long long rbeg, int rd) -> int {
         const StagePlan sp = stage_plan(g, rbeg, rd);
-        if (sp.mode == STAGE_NONE) return 0;
-        const RowWindow w = row_window(sp.src, sp.count);
+        RowWindow w{nullptr, 0, 0u};
+        if (sp.mode != STAGE_NONE) w = row_window(sp.src, sp.count);
         if (h.sl == 0) {
-            fence_async_smem();   // this half's reads of buf precede the copy's writes
-            bulk_load(buf, w.start, w.bytes, bar);
+            const int64_t e = rbeg + rd - 1;   // T's element; the cache is padded past its last row
+            fence_async_smem();                // this half's reads of buf precede the copies' writes
+            bulk_load3(ebuf, a.pair_list + idx, (uint32_t)sizeof(SelEntry), ebuf + 12, g.cdf + (e & ~(int64_t)3), 16u,
+                       buf, w.start, w.bytes, bar);
         }
         return w.off;
     };
     int off = 0;
     uint32_t i = gh;
-    if (i < n) off = request(__ldcg(&a.pair_list[i].beg), __ldcg(&a.pair_list[i].d));
+    if (i < n) off = request(i, __ldcg(&a.pair_list[i].beg), __ldcg(&a.pair_list[i].d));
     for (; i < n; i += nh) {
         const uint32_t inext = i + nh;
         long long nbeg = 0;
         int nd = 0;
-        if (inext < n) {   // the next row's range: its load overlaps this item
+        if (inext < n) {   // the next item's range: its load overlaps this item
             nbeg = __ldcg(&a.pair_list[inext].beg);
             nd = __ldcg(&a.pair_list[inext].d);
         }
-        const SelEntry en = load_sel(a.pair_list + i);
+        if (!mbar_wait(bar, parity)) {   // bounded: report instead of spinning on
+            if (h.sl == 0) atomicOr(a.err, ERR_COPY_WAIT);
+            mbar_wait(bar, parity);        // let the copies in flight land first
+            break;
+        }
+        parity ^= 1u;
+        const SelEntry en = load_sel_smem(reinterpret_cast<const SelEntry *>(ebuf));
         const int64_t beg = en.beg, d = en.d;
+        const float T = ebuf[12 + ((beg + d - 1) & 3)];
         const DrawCtx dc{a.k0, a.k1, en.p, (uint32_t)en.s, (uint32_t)a.depth};
         const bool rec = a.sched && a.sched->mode == SCHED_RECORD;
         long long t0 = 0;
         if (rec) t0 = clock64();
         const StagePlan sp = stage_plan(g, beg, (int)d);
-        if (sp.mode != STAGE_NONE && !mbar_wait(bar, parity)) {   // bounded: report instead of spinning on
-            if (h.sl == 0) atomicOr(a.err, ERR_COPY_WAIT);
-            mbar_wait(bar, parity);                                 // let the copy in flight land first
-            break;
-        }
-        if (sp.mode != STAGE_NONE) parity ^= 1u;
         const float *S = buf + off;   // the staged row or index entries
         int sel;
-        bool ok;
-        if (sp.mode == STAGE_ROW) {
-            const int dd = (int)d;
-            const float T = S[dd - 1];
-            ok = half_select(h, N, dc, T, [&](uint32_t x) { return search_upper32(S, dd, its_target(x, T)); }, sel);
-        } else {
-            const float T = __ldg(g.cdf + beg + d - 1);
-            ok = half_select(h, N, dc, T, [&](uint32_t x) { return (int)staged_cdf_search(g, sp, S, beg, d,
-                                                                                          its_target(x, T)); },
-                             sel);
-        }
-        __syncwarp(h.mask);   // every read of the buffer is done: it is free
-        if (inext < n) off = request(nbeg, nd);
+        const bool ok = half_select(h, N, dc, T, [&](uint32_t x) -> int {
+            const float t = its_target(x, T);
+            if (sp.mode == STAGE_NONE) return (int)cdf_search(g, beg, d, t);
+            const int r = search_upper_lift<9>(S, sp.count, t);
+            return sp.mode == STAGE_ROW ? r : (int)staged_refine(g, sp.mode, r, beg, d, t);
+        }, sel);
+        __syncwarp(h.mask);   // every read of the buffers is done: they are free
+        if (inext < n) off = request(inext, nbeg, nd);
         if (!ok) {   // rebuild needed: a whole warp redoes the item (in shared memory up to WF)
             if (h.sl == 0) {
                 if (d <= WF) a.refill_list[atomicAdd(a.n_refill, 1u)] = en;
@@ -1007,8 +1029,8 @@ __device__ __forceinline__ void pair_body(const DevGraph &g, const LevelArgs &a,
     }
 }
 
-// Shared staging buffers of the pair pass: one row window per half-warp,
-// each with its bulk-copy barrier.
+// Shared staging buffers of the pair pass: one row window and one entry slot
+// per half-warp, each half with its bulk-copy barrier.
 constexpr int PAIR_HALVES = FAST_THREADS / 16;
 constexpr int PAIR_ROW = WF + 4;   // floats: a row of up to WF plus its 16-byte alignment window
 
@@ -1016,13 +1038,14 @@ template <typename I, int BIAS>
 __global__ void __launch_bounds__(FAST_THREADS, CSAW_PAIR_MIN_BLOCKS)
 k_select_pair(DevGraph g, LevelArgs a) {
     __shared__ __align__(16) float s_P[PAIR_HALVES * PAIR_ROW];
+    __shared__ __align__(16) float s_E[PAIR_HALVES * PAIR_ENT];
     __shared__ __align__(8) uint64_t s_bar[PAIR_HALVES];
     const int hid = threadIdx.x >> 4;
     if ((threadIdx.x & 15) == 0) mbar_init(s_bar + hid);
     mbar_init_fence();
     __syncthreads();
     uint32_t parity = 0;
-    pair_body<I, BIAS>(g, a, s_P + hid * PAIR_ROW, s_bar + hid, parity);
+    pair_body<I, BIAS>(g, a, s_P + hid * PAIR_ROW, s_E + hid * PAIR_ENT, s_bar + hid, parity);
 }
 
 // Level expansion, part 2 for hub items (d > WF) over a cached prefix: one

@@ -82,9 +82,10 @@ __device__ __forceinline__ void grid_barrier(unsigned *arrive, unsigned nblocks,
     __syncthreads();
 }
 
-// Bytes of dynamic shared memory of k_persist: the pair pass's row windows
-// and their barriers.
-constexpr size_t PERSIST_SMEM = sizeof(float) * PAIR_HALVES * PAIR_ROW + sizeof(uint64_t) * PAIR_HALVES;
+// Bytes of dynamic shared memory of k_persist: the pair pass's row windows,
+// entry slots and barriers.
+constexpr size_t PERSIST_SMEM =
+    sizeof(float) * PAIR_HALVES * (PAIR_ROW + PAIR_ENT) + sizeof(uint64_t) * PAIR_HALVES;
 
 // The passes: the frequent ones inlined into the one kernel, the hub and
 // CTA-retry passes (rare, with large state of their own) as calls, so their
@@ -102,9 +103,9 @@ __device__ __noinline__ void call_hub(const DevGraph &g, const LevelArgs &a) {
     hub_body<I, BIAS>(g, a);
 }
 template <typename I, int BIAS>
-__device__ __forceinline__ void call_pair(const DevGraph &g, const LevelArgs &a, float *buf, uint64_t *bar,
-                                       uint32_t &parity) {
-    pair_body<I, BIAS>(g, a, buf, bar, parity);
+__device__ __forceinline__ void call_pair(const DevGraph &g, const LevelArgs &a, float *buf, float *ebuf,
+                                       uint64_t *bar, uint32_t &parity) {
+    pair_body<I, BIAS>(g, a, buf, ebuf, bar, parity);
 }
 template <typename I, int BIAS>
 __device__ __noinline__ void call_heavy(const DevGraph &g, const LevelArgs &a) {
@@ -121,7 +122,8 @@ k_persist(const __grid_constant__ DevGraph g, const __grid_constant__ PersistArg
     constexpr bool BIASED = BIAS != CSAW_BIAS_UNBIASED;
     extern __shared__ float s_heavy[];   // the same dynamic region heavy_body names (unused by it here)
     float *pairP = s_heavy;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(s_heavy + PAIR_HALVES * PAIR_ROW);
+    float *pairE = s_heavy + PAIR_HALVES * PAIR_ROW;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(pairE + PAIR_HALVES * PAIR_ENT);
     const int hid = threadIdx.x >> 4;
     if (BIASED) {
         if ((threadIdx.x & 15) == 0) mbar_init(bars + hid);
@@ -137,7 +139,8 @@ k_persist(const __grid_constant__ DevGraph g, const __grid_constant__ PersistArg
         grid_barrier(pa.arrive + k++, nblocks, pa.err);
         call_select<I, BIAS, BIASED>(g, pa.lv[l]);
         if (fl & PF_HUB) call_hub<I, BIAS>(g, pa.lv[l]);
-        if (BIASED && (fl & PF_PAIR)) call_pair<I, BIAS>(g, pa.lv[l], pairP + hid * PAIR_ROW, bars + hid, parity);
+        if (BIASED && (fl & PF_PAIR))
+            call_pair<I, BIAS>(g, pa.lv[l], pairP + hid * PAIR_ROW, pairE + hid * PAIR_ENT, bars + hid, parity);
         grid_barrier(pa.arrive + k++, nblocks, pa.err);
         if (BIASED && (fl & PF_PAIR)) call_select<I, BIAS, true>(g, pa.refill[l]);
         if (fl & PF_RETRY) {
