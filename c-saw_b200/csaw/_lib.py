@@ -37,6 +37,7 @@ OPT_HOST_PARTS = 5
 OPT_RETRY_SMEM = 6
 OPT_PERSISTENT = 7
 OPT_THREAD_SELECT = 8
+OPT_INCR_REBUILD = 9
 MLP_NPARAM, MLP_NORM = 1575, 18
 
 

@@ -154,6 +154,10 @@ struct csaw_graph_s {
     float *ebias = nullptr;
     bool ebias_flag = false;   // materialised at creation (visible to every schedule)
     float *cdf[4] = {};           // per bias kind: canonical per-vertex prefix, or null
+    float2 *tsc[4] = {};          // per bias kind, with cdf: tile summaries of the rows above TSC_MIN_DEG
+    int32_t *tsc_verts = nullptr; // those rows
+    int64_t n_tsc = 0;
+    bool incr_rebuild = true;     // CSAW_OPT_INCR_REBUILD
     bool cdf_flag = false;        // CSAW_GRAPH_CDF_CACHE: visible to the plain schedule too
     bool cdf_off = false;         // CSAW_GRAPH_NO_CDF_CACHE
     int grid_pct = 100;           // CSAW_OPT_GRID_PCT
@@ -228,6 +232,7 @@ DevGraph dev_view(const csaw_graph_s *g, int schedule = CSAW_SCHED_BATCHED, int 
     d.cdf2 = d.cdf ? d.cdf + g->E + ((g->E + 31) >> 5) : nullptr;
     d.cdf_bias = bias;
     d.nrec = fast ? g->nrec : nullptr;
+    d.tsc = (d.cdf && g->incr_rebuild) ? g->tsc[bias] : nullptr;
     return d;
 }
 
@@ -334,9 +339,19 @@ int ensure_cdf(csaw_graph_s *g, cudaStream_t st) {
         LaunchScope ls(g, KK_INIT, st);
         k_cdf_index<<<g->sm_count * 4, 256, 0, st>>>(cdf, g->E, cdf + g->E, n1, cdf + g->E + n1, n2);
     }
+    float2 *tsc = nullptr;   // tile summaries of the hub rows (incremental rebuilds)
+    if (g->n_tsc > 0) {
+        const size_t n = (size_t)((g->E >> 5) + g->V + 1);
+        CK(cudaMalloc((void **)&tsc, sizeof(float2) * n));
+        LaunchScope ls(g, KK_INIT, st);
+        k_tile_summary<I, BIAS><<<(int)std::min<int64_t>(g->n_tsc, g->sm_count * 8), 256, 0, st>>>(
+            dg, tsc, g->tsc_verts, (int)g->n_tsc);
+        g->dev_bytes += 8 * (int64_t)n;
+    }
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));
     g->cdf[BIAS] = cdf;
+    g->tsc[BIAS] = tsc;
     g->dev_bytes += 4 * (g->E + n1 + n2);
     ++g_alloc_epoch;
     return 0;
@@ -1183,9 +1198,11 @@ extern "C" int csaw_graph_create(const void *rowptr, int rowptr_is_64, const int
         if (d > 0) non.push_back((int32_t)v);
     }
     n_non = (int64_t)non.size();
-    std::vector<int32_t> big;
-    for (int64_t v = 0; v < n_vertices; ++v)
+    std::vector<int32_t> big, hubs;
+    for (int64_t v = 0; v < n_vertices; ++v) {
         if (rp(v + 1) - rp(v) > CDF_BIG) big.push_back((int32_t)v);
+        if (rp(v + 1) - rp(v) > TSC_MIN_DEG) hubs.push_back((int32_t)v);
+    }
     for (int64_t e = 0; e < n_edges; ++e)
         if (col[e] < 0 || col[e] >= n_vertices) return fail(CSAW_ERR_INVALID, "col entry out of range");
     if (weights)
@@ -1241,6 +1258,11 @@ extern "C" int csaw_graph_create(const void *rowptr, int rowptr_is_64, const int
         CKG(cudaMalloc((void **)&g->big_verts, sizeof(int32_t) * big.size()));
         CKG(cudaMemcpy(g->big_verts, big.data(), sizeof(int32_t) * big.size(), cudaMemcpyHostToDevice));
     }
+    g->n_tsc = (int64_t)hubs.size();
+    if (!hubs.empty()) {
+        CKG(cudaMalloc((void **)&g->tsc_verts, sizeof(int32_t) * hubs.size()));
+        CKG(cudaMemcpy(g->tsc_verts, hubs.data(), sizeof(int32_t) * hubs.size(), cudaMemcpyHostToDevice));
+    }
     CKG(cudaMalloc((void **)&g->nonisolated, sizeof(int32_t) * (size_t)(n_non > 0 ? n_non : 1)));
     if (n_non > 0)
         CKG(cudaMemcpy(g->nonisolated, non.data(), sizeof(int32_t) * (size_t)n_non, cudaMemcpyHostToDevice));
@@ -1276,7 +1298,9 @@ extern "C" int csaw_graph_destroy(csaw_graph g) {
     cudaFree(g->weight);
     cudaFree(g->ebias);
     for (float *c : g->cdf) cudaFree(c);
+    for (float2 *c : g->tsc) cudaFree(c);
     cudaFree(g->big_verts);
+    cudaFree(g->tsc_verts);
     cudaFree(g->nrec);
     cudaFree(g->nonisolated);
     for (auto &kv : g->graphs) cudaGraphExecDestroy(kv.second);
@@ -1718,6 +1742,10 @@ extern "C" int csaw_graph_set_option(csaw_graph g, int option, int64_t value) {
         case CSAW_OPT_HOST_PARTS:
             if (value < -1 || value > MAX_HOST_PARTS) return fail(CSAW_ERR_INVALID, "host parts must be in [-1, 8]");
             g->host_parts = (int)value;
+            return 0;
+        case CSAW_OPT_INCR_REBUILD:
+            g->incr_rebuild = value != 0;
+            ++g_alloc_epoch;   // the device view is baked into cached graphs
             return 0;
         case CSAW_OPT_THREAD_SELECT:
             if (value < 0 || value > 2) return fail(CSAW_ERR_INVALID, "thread select: 0, 1 or 2");

@@ -50,7 +50,22 @@ struct DevGraph {
     // carries its own adjacency range, so the next expansion or walk step
     // skips the dependent rowptr loads.
     const NbrRec *nrec;    // [E] or null
+    // Tile summaries of rows above TSC_MIN_DEG edges, with cdf (same bias):
+    // for each 32-edge tile t of the row (row-aligned, as the canonical
+    // prefix tiles it), x = the tile's Kogge-Stone total and y = the maximum
+    // of its in-tile scan over the row's edges, at tsc_slot(beg, v) + t.
+    const float2 *tsc;     // or null
 };
+
+// Rows with more edges than this have tile summaries (the rows a CTA retry
+// can get: above the warp passes' shared-memory prefix of 512).
+constexpr int64_t TSC_MIN_DEG = 512;
+
+// First summary slot of row (v, beg).  Slots of different rows never meet:
+// row v's last tile sits at or below (beg_next >> 5) + v, the next row's
+// first at (beg_next >> 5) + v + 1 or above, so E / 32 + V + 1 slots cover
+// every row.
+__device__ __forceinline__ int64_t tsc_slot(int64_t beg, int32_t v) { return (beg >> 5) + (int64_t)v; }
 
 template <typename I>
 __device__ __forceinline__ int64_t row_begin(const DevGraph &g, int64_t v) {
@@ -140,6 +155,24 @@ __device__ __forceinline__ int search_upper_lift(const float *P, int d, float t)
         if (idx < d - 1 && !(P[idx] > t)) lo += step;
     }
     return lo;
+}
+
+// warp_search_upper over an array this CTA wrote earlier in the launch
+// (shared or global memory): plain loads instead of the read-only path.
+__device__ __forceinline__ int64_t warp_search_upper_rw(const float *P, int64_t d, float t, int lane) {
+    int64_t lo = 0, hi = d;   // the answer lies in [lo, hi)
+    while (hi - lo > 32) {
+        const int64_t step = (hi - lo + 31) >> 5;
+        const int64_t idx = lo + (int64_t)(lane + 1) * step - 1;
+        const bool up = idx >= hi - 1 || P[idx] > t;
+        const int k = __ffs(__ballot_sync(FULL, up)) - 1;
+        const int64_t nlo = lo + (int64_t)k * step;
+        hi = nlo + step < hi ? nlo + step : hi;
+        lo = nlo;
+    }
+    const int64_t idx = lo + lane;
+    const bool up = idx >= hi - 1 || P[idx] > t;
+    return lo + __ffs(__ballot_sync(FULL, up)) - 1;
 }
 
 // The same index for one warp-uniform target, found by the whole warp with a

@@ -286,13 +286,166 @@ __host__ __device__ __forceinline__ int64_t heavy_need(int64_t d) {
     return d + (d >> 5) + (d >> 10) + (d >> 5) + 8;
 }
 
+// ------------------------------------------- incremental rebuild of a hub
+// The canonical prefix of a row with the selected neighbors Z zeroed is, per
+// edge i in tile t (32 edges, row-aligned) of group u (32 tiles):
+//   P'[i] = C_u + (qex_t + a_t[i])      (then a running max)
+// with a_t the tile's Kogge-Stone scan, qex_t the exclusive Kogge-Stone scan
+// of the group's tile totals and C_u the in-order sum of the earlier groups'
+// totals.  Only the tiles holding a zeroed neighbor change their scan; the
+// others keep the totals and in-tile maxima of the tile-summary cache.  So a
+// rebuild recomputes those tiles, rescans the tile totals of every group,
+// carries across groups in order and keeps, per tile, the running max of
+// M_t = C_u + (qex_t + max a_t), the tile's largest P' (rounding is monotone,
+// so the largest a_t gives it).  The first i with P'[i] > x lies in the
+// first tile whose running max exceeds x; that tile's P' values are
+// recomputed from its 32 biases with the same additions.  Every value is
+// the one the full rescan computes, and the search returns the same index,
+// but a rebuild touches d/32 summaries instead of d biases and d prefix
+// values.  Scratch (floats): RM, QEX, QA per tile, GC per group.
+struct IncrView {
+    float *RM, *QEX, *QA, *GC;
+    int64_t ntiles, ngroups;
+};
+
+__device__ __forceinline__ IncrView incr_view(float *P, int64_t d) {
+    IncrView iv;
+    iv.ntiles = (d + 31) >> 5;
+    iv.ngroups = (iv.ntiles + 31) >> 5;
+    iv.RM = P;
+    iv.QEX = P + iv.ntiles;
+    iv.QA = P + 2 * iv.ntiles;
+    iv.GC = P + 3 * iv.ntiles;
+    return iv;
+}
+
+// The rebuild, by the whole CTA (all threads call it; zs[0..nz) in shared
+// memory are the zeroed edge offsets).  Returns the new total T.
+template <typename WFn>
+__device__ float incr_rebuild(const DevGraph &g, WFn wfn, int64_t beg, int32_t v, int64_t d, const int32_t *zs,
+                              int nz, const IncrView &iv) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const float2 *ts = g.tsc + tsc_slot(beg, v);
+    // per group: tile totals (recomputed where a neighbor is zeroed), their
+    // exclusive scan, qex + max a per tile, the group total
+    for (int64_t gg = warp; gg < iv.ngroups; gg += nw) {
+        const int64_t t = (gg << 5) + lane;
+        float tot = 0.f, amax = 0.f;
+        if (t < iv.ntiles) {
+            const float2 x = __ldg(ts + t);
+            tot = x.x;
+            amax = x.y;
+        }
+        bool touched = false;
+        for (int k = 0; k < nz; ++k) touched |= (int64_t)(zs[k] >> 5) == t;
+        unsigned tm = __ballot_sync(FULL, touched);
+        while (tm) {
+            const int b = __ffs(tm) - 1;
+            tm &= tm - 1;
+            const int64_t i = ((((gg << 5) + b)) << 5) + lane;
+            float w = 0.f;
+            if (i < d) {
+                w = wfn(i);
+                for (int k = 0; k < nz; ++k)
+                    if ((int64_t)zs[k] == i) w = 0.f;
+            }
+            const float a = warp_ks_sum(w, lane);
+            const float at = __shfl_sync(FULL, a, 31);
+            float m = i < d ? a : 0.f;
+#pragma unroll
+            for (int off = 16; off; off >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, off));
+            if (lane == b) {
+                tot = at;
+                amax = m;
+            }
+        }
+        const float q = warp_ks_sum(tot, lane);
+        float qex = __shfl_up_sync(FULL, q, 1);
+        if (lane == 0) qex = 0.f;
+        if (t < iv.ntiles) {
+            iv.QEX[t] = qex;
+            iv.QA[t] = __fadd_rn(qex, amax);
+        }
+        if (lane == 31) iv.GC[gg] = q;
+    }
+    __syncthreads();
+    if (warp == 0) {   // carry into each group, in group order (as cta_canon_prefix)
+        float C = 0.f;
+        for (int64_t g0 = 0; g0 < iv.ngroups; g0 += 32) {
+            const int64_t gg = g0 + lane;
+            const float tot = gg < iv.ngroups ? iv.GC[gg] : 0.f;
+            const int m = iv.ngroups - g0 < 32 ? (int)(iv.ngroups - g0) : 32;
+            float mine = 0.f;
+            for (int k = 0; k < m; ++k) {
+                if (lane == k) mine = C;
+                C = __fadd_rn(C, __shfl_sync(FULL, tot, k));
+            }
+            if (gg < iv.ngroups) iv.GC[gg] = mine;
+        }
+    }
+    __syncthreads();
+    for (int64_t t = threadIdx.x; t < iv.ntiles; t += blockDim.x) iv.RM[t] = __fadd_rn(iv.GC[t >> 5], iv.QA[t]);
+    __syncthreads();
+    {   // running max of the tile maxima (max is exact: ranges scanned in parallel)
+        __shared__ float s_rm[32];
+        const int64_t per = (iv.ntiles + nw - 1) / nw;
+        const int64_t t0 = (int64_t)warp * per, t1 = t0 + per < iv.ntiles ? t0 + per : iv.ntiles;
+        float rmax = 0.f;
+        for (int64_t t = t0 + lane; t < t1; t += 32) rmax = fmaxf(rmax, iv.RM[t]);
+#pragma unroll
+        for (int off = 16; off; off >>= 1) rmax = fmaxf(rmax, __shfl_xor_sync(FULL, rmax, off));
+        if (lane == 0) s_rm[warp] = rmax;
+        __syncthreads();
+        float carry = 0.f;
+        for (int w = 0; w < warp; ++w) carry = fmaxf(carry, s_rm[w]);
+        for (int64_t base = t0; base < t1; base += 32) {
+            const int64_t t = base + lane;
+            const float ms = fmaxf(warp_max_scan(t < t1 ? iv.RM[t] : 0.f, lane), carry);
+            if (t < t1) iv.RM[t] = ms;
+            carry = __shfl_sync(FULL, ms, 31);
+        }
+    }
+    __syncthreads();
+    return iv.RM[iv.ntiles - 1];
+}
+
+// Draw searches after an incremental rebuild, by one warp (all lanes call):
+// each lane with act set gets the first i with P'[i] > t.
+template <typename WFn>
+__device__ __forceinline__ int incr_search(WFn wfn, int64_t d, const int32_t *zs, int nz, const IncrView &iv, float t,
+                                           bool act, int lane) {
+    int res = -1;
+    unsigned am = __ballot_sync(FULL, act);
+    while (am) {
+        const int b = __ffs(am) - 1;
+        am &= am - 1;
+        const float tb = __shfl_sync(FULL, t, b);
+        const int64_t k = warp_search_upper_rw(iv.RM, iv.ntiles, tb, lane);   // the tile holding the answer
+        const int64_t i = (k << 5) + lane;
+        float w = 0.f;
+        if (i < d) {
+            w = wfn(i);
+            for (int z = 0; z < nz; ++z)
+                if ((int64_t)zs[z] == i) w = 0.f;
+        }
+        const float a = warp_ks_sum(w, lane);
+        const float p = __fadd_rn(iv.GC[k >> 5], __fadd_rn(iv.QEX[k], a));
+        const unsigned hit = __ballot_sync(FULL, i < d && p > tb);
+        // hit is never empty: the tile's largest P' is its running max entry
+        if (lane == b) res = (int)((k << 5) + (hit ? __ffs(hit) - 1 : 0));
+    }
+    return res;
+}
+
 // One CTA per deferred item: the canonical prefix is built by the whole CTA in
 // shared memory when the launch has room for the row (a.heavy_smem), else in
 // global scratch (same canonical order, so bit-identical to the warp path);
-// warp 0 runs the slot resolver; every rebuild is a CTA-wide rescan.
+// warp 0 runs the slot resolver; a rebuild is incremental over the tile
+// summaries for a cached hub (incr_rebuild), else a CTA-wide rescan.
 template <typename I, int BIAS, bool STREAM = false>
 __device__ __forceinline__ void heavy_body(const DevGraph &g0, const LevelArgs &a) {
-    __shared__ int s_flag, s_j;
+    __shared__ int s_flag, s_j, s_nz;
+    __shared__ int32_t s_z[32];   // zeroed neighbors of an incremental rebuild
     extern __shared__ float s_heavy[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float *const P_global = a.heavy_scratch + (int64_t)blockIdx.x * a.heavy_stride;
@@ -328,13 +481,18 @@ __device__ __forceinline__ void heavy_body(const DevGraph &g0, const LevelArgs &
         uint32_t *zb = (uint32_t *)(gcar + (d >> 10) + 1);
         auto wfn = [&](int64_t i) { return edge_bias<I, BIAS>(g, beg + i); };
         bool indexed = g.cdf && g.cdf_bias == BIAS;   // cached prefix, searched through its index
+        // cached hub with tile summaries: rebuilds are incremental
+        const bool incr = !STREAM && indexed && g.tsc && d > TSC_MIN_DEG;
+        bool rebuilt = false;
+        const IncrView iv = incr_view(P, d);
         float T = indexed ? g.cdf[beg + d - 1] : cta_canon_prefix(wfn, d, P, tsum, gcar, nullptr);
         const DrawCtx dc{a.k0, a.k1, p, (uint32_t)s, (uint32_t)l};
         SlotRng rng;
         SelState st;
         auto cand_of = [&](uint32_t x, bool act) -> int {
+            const float t = act ? its_target(x, T) : 0.f;
+            if (rebuilt) return incr_search(wfn, d, s_z, s_nz, iv, t, act, lane);   // all lanes take part
             if (!act) return -1;
-            const float t = its_target(x, T);
             return indexed ? (int)cdf_search(g, beg, d, t) : (int)search_upper(P, d, t);
         };
         bool zero = !(T > 0.f);
@@ -352,12 +510,22 @@ __device__ __forceinline__ void heavy_body(const DevGraph &g0, const LevelArgs &
             __syncthreads();
             const int need = s_flag, j = s_j;
             if (!need) break;
-            const int64_t nwords = (d + 31) >> 5;
-            for (int64_t w = threadIdx.x; w < nwords; w += blockDim.x) zb[w] = 0u;
-            __syncthreads();
-            if (warp == 0 && lane < j) atomicOr(&zb[st.sel >> 5], 1u << (st.sel & 31));
-            __syncthreads();
-            T = cta_canon_prefix(wfn, d, P, tsum, gcar, zb);
+            if (incr) {
+                if (warp == 0) {
+                    if (lane < j) s_z[lane] = st.sel;
+                    if (lane == 0) s_nz = j;
+                }
+                __syncthreads();
+                T = incr_rebuild(g, wfn, beg, v, d, s_z, j, iv);
+                rebuilt = true;
+            } else {
+                const int64_t nwords = (d + 31) >> 5;
+                for (int64_t w = threadIdx.x; w < nwords; w += blockDim.x) zb[w] = 0u;
+                __syncthreads();
+                if (warp == 0 && lane < j) atomicOr(&zb[st.sel >> 5], 1u << (st.sel & 31));
+                __syncthreads();
+                T = cta_canon_prefix(wfn, d, P, tsum, gcar, zb);
+            }
             indexed = false;
             if (warp == 0) {
                 if (!(T > 0.f)) zero = true;
@@ -669,6 +837,27 @@ __global__ void k_cdf_build_big(DevGraph g, float *cdf, const int32_t *verts, in
         float *gcar = tsum + (d >> 5) + 1;
         auto wfn = [&](int64_t i) { return edge_bias<I, BIAS>(g, beg + i); };
         cta_canon_prefix(wfn, d, cdf + beg, tsum, gcar, nullptr);
+    }
+}
+
+// Tile summaries (DevGraph::tsc) of the rows in verts: one CTA per row,
+// a warp per tile, the same Kogge-Stone scan as the canonical prefix.
+template <typename I, int BIAS>
+__global__ void k_tile_summary(DevGraph g, float2 *out, const int32_t *verts, int n) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+        const int32_t v = verts[k];
+        const int64_t beg = row_begin<I>(g, v), d = row_begin<I>(g, v + 1) - beg;
+        const int64_t ntiles = (d + 31) >> 5, base = tsc_slot(beg, v);
+        for (int64_t t = warp; t < ntiles; t += nw) {
+            const int64_t i = (t << 5) + lane;
+            const float a = warp_ks_sum(i < d ? edge_bias<I, BIAS>(g, beg + i) : 0.f, lane);
+            const float tot = __shfl_sync(FULL, a, 31);
+            float m = i < d ? a : 0.f;
+#pragma unroll
+            for (int off = 16; off; off >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, off));
+            if (lane == 0) out[base + t] = make_float2(tot, m);
+        }
     }
 }
 

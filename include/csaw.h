@@ -243,7 +243,12 @@ enum {
      * levels of at least 65,536 items, and the learned scheduler may pick
      * it; 2: the degree rule uses it for every such item; 0: never.  Never
      * changes the output. */
-    CSAW_OPT_THREAD_SELECT = 8
+    CSAW_OPT_THREAD_SELECT = 8,
+    /* 1 (default): a CTA retry of a cached hub (more than 512 edges) rebuilds
+     * its prefix incrementally from per-tile summaries built with the cache
+     * (8 bytes per 32 edges of the hub rows, E/32 + V + 1 slots); 0: every
+     * rebuild rescans the whole row.  Never changes the output. */
+    CSAW_OPT_INCR_REBUILD = 9
 };
 int csaw_graph_set_option(csaw_graph g, int option, int64_t value);
 

@@ -103,9 +103,10 @@ def test_hub_walk_parity(csaw, skewed_hubs, cache, schedule, bias):
 
 
 def test_cache_residency_policy(csaw, skewed_hubs):
-    """The batched schedule builds the cache (4.13E bytes) on first biased use of a
-    graph with hubs; the plain schedule does not unless asked; the opt-out
-    flag keeps it off; an unbiased job never builds it."""
+    """The batched schedule builds the cache (4.13E bytes, plus the hub rows'
+    tile summaries, 8 (E/32 + V + 1) bytes) on first biased use of a graph
+    with hubs; the plain schedule does not unless asked; the opt-out flag
+    keeps it off; an unbiased job never builds it."""
     g = skewed_hubs
     E = g.n_edges
     seeds = oracle.make_seeds(g.rowptr, 64, 1)
@@ -119,6 +120,8 @@ def test_cache_residency_policy(csaw, skewed_hubs):
         return after - before
 
     cache = 4 * (E + (E + 31) // 32 + (E + 1023) // 1024)   # prefix and its two search-index levels
+    assert np.diff(g.rowptr).max() > 512
+    cache += 8 * ((E >> 5) + g.n_vertices + 1)                 # tile summaries (rows above 512 edges)
     assert grows(None, 1, 2) - grows(False, 1, 2) == cache   # batched also adds neighbor records
     assert grows(None, 0, 2) == 0
     assert grows(True, 0, 2) == cache
