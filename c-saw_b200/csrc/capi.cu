@@ -785,7 +785,7 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
                 LaunchScope ls(g, KK_SELECT_THREAD, st);
                 k_select_thread<I, BIAS><<<tgrid, FAST_THREADS, 0, st>>>(dg, a);
             }
-            // with the pair list, every cached hub (d > WF >= 4N) is paired:
+            // with the pair list, every cached hub (d > WF >= 3N) is paired:
             // the hub list stays empty
             if (!plain && cached && g->maxdeg > WF && !a.pair_list) {
                 LaunchScope ls(g, KK_HUB, st);

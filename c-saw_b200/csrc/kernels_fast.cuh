@@ -29,6 +29,11 @@ constexpr int WF = 512;  // per-warp shared prefix capacity of the fast kernels
 #ifndef CSAW_PAIR_MIN_BLOCKS
 #define CSAW_PAIR_MIN_BLOCKS 4
 #endif
+// Cached items with N <= 16 and d >= this many times N go to the pair pass
+// (3: a phase-1 rejection is rare enough that its refill stays cheap).
+#ifndef CSAW_PAIR_MIN_RATIO
+#define CSAW_PAIR_MIN_RATIO 3
+#endif
 
 constexpr int FAST_THREADS = 256;
 
@@ -474,7 +479,7 @@ __device__ __forceinline__ void coop_body(const DevGraph &g, const LevelArgs &a)
         const bool heavy = drawn && cls >= 2 && !thr;
         // cached items with few slots and a rare rebuild run two per warp;
         // other warp-class items above WF search the cached prefix in their own list
-        const bool pair = drawn && !heavy && !thr && cached && N <= 16 && d >= 4 * N && a.pair_list;
+        const bool pair = drawn && !heavy && !thr && cached && N <= 16 && d >= CSAW_PAIR_MIN_RATIO * N && a.pair_list;
         const bool hub = drawn && !heavy && !thr && cached && d > WF && !pair;
         const int incl = warp_incl_scan(k, lane);
         const int excl = incl - k;
@@ -919,7 +924,7 @@ __device__ __forceinline__ unsigned long long staged_bytes(const StagePlan &sp, 
 }
 
 // Level expansion, part 2 for items over a cached prefix with N <= 16 and
-// d >= 4N (a rebuild is rare): two items per warp, one per half-warp, lanes
+// d >= 3N (a rebuild is rare): two items per warp, one per half-warp, lanes
 // N..15 of a half idle instead of N..31 of a warp.  For each item the bulk
 // copy engine stages, on one barrier: its work entry, the 16 bytes holding
 // its prefix total T, and what its draws search (stage_plan: the prefix row
