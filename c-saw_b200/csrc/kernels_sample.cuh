@@ -308,6 +308,10 @@ struct IncrView {
     int64_t ntiles, ngroups;
 };
 
+// Rows of up to this many groups (2 M edges) keep their group maxima in
+// shared memory for the draws' first search level.
+constexpr int INCR_SGROUPS = 2048;
+
 __device__ __forceinline__ IncrView incr_view(float *P, int64_t d) {
     IncrView iv;
     iv.ntiles = (d + 31) >> 5;
@@ -323,7 +327,7 @@ __device__ __forceinline__ IncrView incr_view(float *P, int64_t d) {
 // memory are the zeroed edge offsets).  Returns the new total T.
 template <typename WFn>
 __device__ float incr_rebuild(const DevGraph &g, WFn wfn, int64_t beg, int32_t v, int64_t d, const int32_t *zs,
-                              int nz, const IncrView &iv) {
+                              int nz, const IncrView &iv, float *sgm) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const float2 *ts = g.tsc + tsc_slot(beg, v);
     // per group: tile totals (recomputed where a neighbor is zeroed), their
@@ -406,34 +410,68 @@ __device__ float incr_rebuild(const DevGraph &g, WFn wfn, int64_t beg, int32_t v
         }
     }
     __syncthreads();
+    if (iv.ngroups <= INCR_SGROUPS) {   // the running max at each group's last tile
+        for (int64_t u = threadIdx.x; u < iv.ngroups; u += blockDim.x)
+            sgm[u] = iv.RM[(u << 5) + 31 < iv.ntiles - 1 ? (u << 5) + 31 : iv.ntiles - 1];
+        __syncthreads();
+    }
     return iv.RM[iv.ntiles - 1];
 }
 
 // Draw searches after an incremental rebuild, by one warp (all lanes call):
-// each lane with act set gets the first i with P'[i] > t.
+// each lane with act set gets the first i with P'[i] > t.  Each lane finds
+// its own tile, in parallel: its group among the running maxima at the
+// groups' last tiles (sgm, shared memory, when the row has at most
+// INCR_SGROUPS groups; else in RM), then the tile among the group's 32
+// entries of RM; it stages the tile's biases (zeroed ones as 0) in its row of
+// srow ([32][33] floats, shared) with the tile's carry and scan offset.  The
+// warp then scans each staged tile in turn, with no memory access on that
+// serial path.
 template <typename WFn>
-__device__ __forceinline__ int incr_search(WFn wfn, int64_t d, const int32_t *zs, int nz, const IncrView &iv, float t,
-                                           bool act, int lane) {
+__device__ __forceinline__ int incr_search(WFn wfn, int64_t d, const int32_t *zs, int nz, const IncrView &iv,
+                                           const float *sgm, float *srow, float t, bool act, int lane) {
+    int64_t k = 0;
+    float gc = 0.f, qx = 0.f;
+    if (act) {
+        int64_t u;
+        if (iv.ngroups <= INCR_SGROUPS) {
+            u = search_upper(sgm, iv.ngroups, t);
+        } else {
+            int64_t lo = 0, hi = iv.ngroups - 1;
+            while (lo < hi) {
+                const int64_t mid = (lo + hi) >> 1;
+                const int64_t te = (mid << 5) + 31 < iv.ntiles - 1 ? (mid << 5) + 31 : iv.ntiles - 1;
+                if (iv.RM[te] > t) hi = mid; else lo = mid + 1;
+            }
+            u = lo;
+        }
+        const int64_t k0 = u << 5;
+        k = k0 + search_upper_lift<5>(iv.RM + k0, iv.ntiles - k0 < 32 ? (int)(iv.ntiles - k0) : 32, t);
+        gc = iv.GC[u];
+        qx = iv.QEX[k];
+        uint32_t zm = 0;
+        for (int z = 0; z < nz; ++z)
+            if ((int64_t)(zs[z] >> 5) == k) zm |= 1u << (zs[z] & 31);
+        float *row = srow + lane * 33;
+        const int64_t i0 = k << 5;
+#pragma unroll
+        for (int m = 0; m < 32; ++m) row[m] = (i0 + m < d && !((zm >> m) & 1u)) ? wfn(i0 + m) : 0.f;
+    }
+    __syncwarp();
     int res = -1;
     unsigned am = __ballot_sync(FULL, act);
     while (am) {
         const int b = __ffs(am) - 1;
         am &= am - 1;
-        const float tb = __shfl_sync(FULL, t, b);
-        const int64_t k = warp_search_upper_rw(iv.RM, iv.ntiles, tb, lane);   // the tile holding the answer
-        const int64_t i = (k << 5) + lane;
-        float w = 0.f;
-        if (i < d) {
-            w = wfn(i);
-            for (int z = 0; z < nz; ++z)
-                if ((int64_t)zs[z] == i) w = 0.f;
-        }
-        const float a = warp_ks_sum(w, lane);
-        const float p = __fadd_rn(iv.GC[k >> 5], __fadd_rn(iv.QEX[k], a));
-        const unsigned hit = __ballot_sync(FULL, i < d && p > tb);
+        const long long kb = __shfl_sync(FULL, (long long)k, b);
+        const float tb = __shfl_sync(FULL, t, b), gb = __shfl_sync(FULL, gc, b), qb = __shfl_sync(FULL, qx, b);
+        const float a = warp_ks_sum(srow[b * 33 + lane], lane);
+        const float pv = __fadd_rn(gb, __fadd_rn(qb, a));
+        const unsigned hit = __ballot_sync(FULL, ((int64_t)kb << 5) + lane < d && pv > tb);
         // hit is never empty: the tile's largest P' is its running max entry
-        if (lane == b) res = (int)((k << 5) + (hit ? __ffs(hit) - 1 : 0));
+        if (lane == b) res = (int)(((int64_t)kb << 5) + (hit ? __ffs(hit) - 1 : 0));
     }
+    __syncwarp();   // the rows are free for the next call
     return res;
 }
 
@@ -445,7 +483,9 @@ __device__ __forceinline__ int incr_search(WFn wfn, int64_t d, const int32_t *zs
 template <typename I, int BIAS, bool STREAM = false>
 __device__ __forceinline__ void heavy_body(const DevGraph &g0, const LevelArgs &a) {
     __shared__ int s_flag, s_j, s_nz;
-    __shared__ int32_t s_z[32];   // zeroed neighbors of an incremental rebuild
+    __shared__ int32_t s_z[32];                 // zeroed neighbors of an incremental rebuild
+    __shared__ float s_gm[INCR_SGROUPS];        // its group maxima
+    __shared__ float s_row[32 * 33];            // its draws' staged tiles
     extern __shared__ float s_heavy[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float *const P_global = a.heavy_scratch + (int64_t)blockIdx.x * a.heavy_stride;
@@ -491,7 +531,7 @@ __device__ __forceinline__ void heavy_body(const DevGraph &g0, const LevelArgs &
         SelState st;
         auto cand_of = [&](uint32_t x, bool act) -> int {
             const float t = act ? its_target(x, T) : 0.f;
-            if (rebuilt) return incr_search(wfn, d, s_z, s_nz, iv, t, act, lane);   // all lanes take part
+            if (rebuilt) return incr_search(wfn, d, s_z, s_nz, iv, s_gm, s_row, t, act, lane);   // all lanes take part
             if (!act) return -1;
             return indexed ? (int)cdf_search(g, beg, d, t) : (int)search_upper(P, d, t);
         };
@@ -516,7 +556,7 @@ __device__ __forceinline__ void heavy_body(const DevGraph &g0, const LevelArgs &
                     if (lane == 0) s_nz = j;
                 }
                 __syncthreads();
-                T = incr_rebuild(g, wfn, beg, v, d, s_z, j, iv);
+                T = incr_rebuild(g, wfn, beg, v, d, s_z, j, iv, s_gm);
                 rebuilt = true;
             } else {
                 const int64_t nwords = (d + 31) >> 5;

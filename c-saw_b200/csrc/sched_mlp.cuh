@@ -93,13 +93,15 @@ __device__ __forceinline__ void item_features(float x[MLP_IN], int64_t d, int N,
 }
 
 // Valid classes for degree d (bit c set if class c can run the item).
-// With the per-vertex prefix cache, class 1 (one warp) also takes items above
-// wf: it searches the cached prefix instead of building one in shared memory.
-// thr: the job has a thread list (batched, biased, not disabled).
+// One-tile rows (d <= 32) run in a warp's registers or in one thread (thr:
+// the job has a thread list; batched, biased, not disabled): wider classes
+// only idle more lanes on them.  Longer rows run at warp or CTA width; with
+// the per-vertex prefix cache, class 1 (one warp) also takes items above wf:
+// it searches the cached prefix instead of building one in shared memory.
 __device__ __forceinline__ unsigned valid_classes(int64_t d, int wf, bool cached, bool thr) {
+    if (d <= 32) return thr ? 0x41u : 0x1u;
     unsigned m = CLS_CTA_MASK;       // CTAs always
     if (d <= wf || cached) m |= 0x2u;
-    if (d <= 32) m |= thr ? 0x41u : 0x1u;
     return m;
 }
 
@@ -189,9 +191,8 @@ __device__ __forceinline__ int choose_class(const SchedArgs *sa, const __nv_bflo
 // then log2 d in half steps from 5; CoV in half steps; N sum p^2 in unit
 // steps; the level's N, size, depth and bias fixed), and the expansion kernel
 // routes each item by one table load.  Each cell holds two picks: over the
-// classes valid for a warp-sized item (0, 1, the CTAs and the thread for
-// d <= 32; 1 and the CTAs above) and over the CTA classes 2..5 (255: none
-// allowed).
+// classes valid for an item a warp can run (0 and the thread for d <= 32; 1
+// and the CTAs above) and over the CTA classes 2..5 (255: none allowed).
 constexpr int TAB_SMALL = 8;   // degree bins of d <= 32
 constexpr int TAB_D = 40, TAB_C = 8, TAB_P = 8, TAB_N = TAB_D * TAB_C * TAB_P;
 
@@ -238,7 +239,7 @@ static __global__ void k_sched_table(const SchedArgs *sa, const uint32_t *n_in, 
     const float y = mlp_infer(sa->wq, sa->norm, x, lane);
     // a small cell's degree d may be below N: such items take all their
     // neighbors and are never routed, so the cell's pick does not matter
-    const unsigned va = small ? (0x3fu | (thr ? 0x40u : 0u)) : 0x3eu;
+    const unsigned va = small ? (thr ? 0x41u : 0x1u) : 0x3eu;
     const int a = class_argmin(y, sa->norm, n_level, sa->warp_slots, sa->class_mask & va, lane);
     const int b = class_argmin(y, sa->norm, n_level, sa->warp_slots, sa->class_mask & CLS_CTA_MASK, lane);
     if (lane == 0) {
