@@ -647,9 +647,13 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
         a.retry_list = (SelEntry *)c->retry.p;
         a.n_retry = &c->ctr->n_retry;
         // a thread list where some item of the level may take the thread class
-        // (the degree rule sends none when N > 16)
-        const bool thr_level = !plain && BIASED && g->thread_sel &&
-                               (g->thread_sel == 2 || sched != nullptr || fan[l] <= THREAD_RULE_MAX_N);
+        // (the degree rule sends none when N > 16 or when the level cannot
+        // reach THREAD_RULE_MIN_ITEMS items; a model that routes or records may)
+        double level_items = (double)B * F;
+        for (int i = 0; i < l; ++i) level_items *= fan[i];
+        const bool model = sched && g->sched_host.mode != SCHED_THRESHOLD;
+        const bool rule_thr = fan[l] <= THREAD_RULE_MAX_N && level_items >= (double)THREAD_RULE_MIN_ITEMS;
+        const bool thr_level = !plain && BIASED && g->thread_sel && (g->thread_sel == 2 || model || rule_thr);
         a.thread_list = thr_level ? (SelEntry *)c->tsel.p : nullptr;
         a.n_thread = &c->ctr->n_thread;
         a.thread_force = g->thread_sel == 2;

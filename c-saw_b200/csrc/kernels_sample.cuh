@@ -521,6 +521,8 @@ __device__ __forceinline__ void heavy_body(const DevGraph &g0, const LevelArgs &
         uint32_t *zb = (uint32_t *)(gcar + (d >> 10) + 1);
         auto wfn = [&](int64_t i) { return edge_bias<I, BIAS>(g, beg + i); };
         bool indexed = g.cdf && g.cdf_bias == BIAS;   // cached prefix, searched through its index
+        const bool indexed0 = indexed;
+        unsigned long long rebuild_bytes = 0;         // counted prefix reads of the rebuilds
         // cached hub with tile summaries: rebuilds are incremental
         const bool incr = !STREAM && indexed && g.tsc && d > TSC_MIN_DEG;
         bool rebuilt = false;
@@ -558,6 +560,10 @@ __device__ __forceinline__ void heavy_body(const DevGraph &g0, const LevelArgs &
                 __syncthreads();
                 T = incr_rebuild(g, wfn, beg, v, d, s_z, j, iv, s_gm);
                 rebuilt = true;
+                // the row's tile summaries, the touched tiles' biases, and per
+                // later draw one line of running maxima and one tile of biases
+                rebuild_bytes += 8ull * (unsigned long long)iv.ntiles + 128ull * (unsigned long long)j +
+                                 256ull * (unsigned long long)N;
             } else {
                 const int64_t nwords = (d + 31) >> 5;
                 for (int64_t w = threadIdx.x; w < nwords; w += blockDim.x) zb[w] = 0u;
@@ -565,6 +571,7 @@ __device__ __forceinline__ void heavy_body(const DevGraph &g0, const LevelArgs &
                 if (warp == 0 && lane < j) atomicOr(&zb[st.sel >> 5], 1u << (st.sel & 31));
                 __syncthreads();
                 T = cta_canon_prefix(wfn, d, P, tsum, gcar, zb);
+                rebuild_bytes += 4ull * (unsigned long long)d;   // every bias of the row again
             }
             indexed = false;
             if (warp == 0) {
@@ -617,7 +624,10 @@ __device__ __forceinline__ void heavy_body(const DevGraph &g0, const LevelArgs &
             }
         }
         my_items++;
-        my_bytes += expansion_bytes<I, BIAS>(g, d, N, true, a, push);
+        // a prefix built here reads every bias; a cached one is searched
+        // through its index (about log2 d probes a draw)
+        my_bytes += expansion_bytes<I, BIAS>(g, d, N, !indexed0, a, push) + rebuild_bytes +
+                    (indexed0 ? (unsigned long long)N * 4ull * (64 - __clzll((unsigned long long)d)) : 0ull);
         __syncthreads();
         if (rec && threadIdx.x == 0)
             record_profile(a.sched, d, N, a.sched->vstats[v], __ldcg(a.n_in), l, 2 + a.cta_class, clock64() - t0);
