@@ -839,7 +839,10 @@ def streaming(args):
     page-locked host memory, the device partition budget capped at
     --stream-budget-gb with 2^--stream-pbits-vertex partitions; one step =
     --stream-walks edge-weight-biased walks of length 20 and --stream-samples
-    edge-weight-biased samples F1 N10 D2; with --stream-cache 1 (default) the
+    edge-weight-biased samples F1 N10 D2; with --stream-read-in-place 1
+    (default) partitions outside the device arena are read in place from
+    page-locked host memory (0: copied in and evicted by sweeps); with
+    --stream-cache 1 (default) the
     streaming graph's weight-bias prefix cache is built first and streamed in
     place of the weights.  The defaults are 1/8 of the
     scale-29 configuration (131,072 walks, 32,768 samples, 4 GiB, 2^17-vertex
@@ -874,7 +877,9 @@ def streaming(args):
     psb = csaw.make_params(0, 2, ns, 1, 10, 2, seed=0x29B, schedule=csaw.SCHED_BATCHED)
     t0 = time.perf_counter()
     S = csaw.StreamGraph(g, partition_bits=pbits, slot_budget_bytes=budget, rowptr64=True)
+    S.set_option(csaw._lib.STREAM_OPT_READ_IN_PLACE, args.stream_read_in_place)
     res["stream_setup_s"] = time.perf_counter() - t0
+    res["read_in_place"] = bool(args.stream_read_in_place)
     if args.stream_cache:   # the weight-bias prefix, streamed in place of the weights
         t0 = time.perf_counter()
         S.cache(2)
@@ -930,6 +935,7 @@ def streaming(args):
             i1 = S.info()
             r["h2d_bytes_per_step"] = (i1["bytes_h2d"] - i0["bytes_h2d"]) / steps
             r["partition_loads_per_step"] = (i1["partition_loads"] - i0["partition_loads"]) / steps
+            r["items_read_in_place_per_step"] = (i1["items_read_in_place"] - i0["items_read_in_place"]) / steps
             r["partitions"] = i1["n_partitions"]
             r["slots"] = i1["n_slots"]
             r["h2d_gbs"] = r["h2d_bytes_per_step"] / dt / 1e9
@@ -1080,6 +1086,9 @@ def main():
     ap.add_argument("--stream-warmup", type=int, default=1, help="untimed streaming steps before timing")
     ap.add_argument("--stream-cache", type=int, default=1,
                     help="1: build the streaming graph's weight-bias prefix cache (streamed in place of weights)")
+    ap.add_argument("--stream-read-in-place", type=int, default=1,
+                    help="1: partitions outside the device arena are read in place from page-locked host memory; "
+                         "0: copied in and evicted by sweeps")
     ap.add_argument("--serve-requests", type=int, default=4000, help="requests per serving stream")
     ap.add_argument("--forms", default="plain,batched,learned",
                     help="forms to time; the last one is reported as value (profiling runs use one form)")

@@ -25,7 +25,7 @@ EXPORTS = [
     "csaw_graph_stats", "csaw_graph_profile", "csaw_graph_kernel_stats", "csaw_make_seeds",
     "csaw_sample", "csaw_sample_host", "csaw_sample_batch", "csaw_sample_noalloc", "csaw_sampler_compat",
     "csaw_graph_set_option", "csaw_stream_graph_create", "csaw_stream_graph_destroy", "csaw_stream_sample",
-    "csaw_stream_stats", "csaw_stream_graph_cache", "csaw_sched_info", "csaw_sched_get_records", "csaw_sched_train", "csaw_sched_classes", "csaw_sched_get_model", "csaw_sched_set_model",
+    "csaw_stream_stats", "csaw_stream_graph_cache", "csaw_stream_graph_set_option", "csaw_sched_info", "csaw_sched_get_records", "csaw_sched_train", "csaw_sched_classes", "csaw_sched_get_model", "csaw_sched_set_model",
     "csaw_mlp_grad_host", "csaw_server_create", "csaw_server_destroy", "csaw_server_submit", "csaw_server_wait",
     "csaw_server_get_stats", "csaw_graph_autotune",
 ]
@@ -38,6 +38,7 @@ OPT_RETRY_SMEM = 6
 OPT_PERSISTENT = 7
 OPT_THREAD_SELECT = 8
 OPT_INCR_REBUILD = 9
+STREAM_OPT_READ_IN_PLACE = 1
 MLP_NPARAM, MLP_NORM = 1575, 18
 
 
@@ -100,7 +101,7 @@ class Job(ctypes.Structure):
 class StreamInfo(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int64) for n in (
         "n_partitions", "n_slots", "partition_loads", "partition_hits", "bytes_h2d", "kernel_launches",
-        "host_pinned_in_place")]
+        "host_pinned_in_place", "items_read_in_place")]
 
 
 class Stats(ctypes.Structure):
@@ -141,6 +142,7 @@ def lib():
     L.csaw_stream_sample.argtypes = sig
     L.csaw_stream_stats.argtypes = [p, ctypes.POINTER(StreamInfo)]
     L.csaw_stream_graph_cache.argtypes = [p, i32]
+    L.csaw_stream_graph_set_option.argtypes = [p, i32, ctypes.c_int64]
     PF = ctypes.POINTER(ctypes.c_float)
     L.csaw_sched_info.argtypes = [p, P64, ctypes.POINTER(ctypes.c_int), PF]
     L.csaw_sched_train.argtypes = [p, i32, ctypes.c_float, u64, PF]

@@ -290,6 +290,10 @@ class StreamGraph:
         weights and search it (the same edges)."""
         check(lib().csaw_stream_graph_cache(self.h, BIAS_NAMES.get(bias, bias)))
 
+    def set_option(self, option, value):
+        """csaw_stream_graph_set_option (e.g. _lib.STREAM_OPT_READ_IN_PLACE)."""
+        check(lib().csaw_stream_graph_set_option(self.h, option, int(value)))
+
     def info(self):
         s = _lib.StreamInfo()
         check(lib().csaw_stream_stats(self.h, ctypes.byref(s)))

@@ -178,6 +178,12 @@ struct csaw_stream_graph_s {
     float *d_idx[4] = {};             // cdf1 [(E + 31) / 32], then cdf2 [(E + 1023) / 1024]
     StreamCounters *hctr = nullptr;
     int64_t loads = 0, hits = 0, bytes_h2d = 0, launches = 0;
+    // Read in place (CSAW_STREAM_OPT_READ_IN_PLACE): device addresses of the
+    // page-locked host arrays, null where not mapped
+    bool read_in_place = true;
+    const int32_t *dv_col = nullptr;
+    const float *dv_w = nullptr, *dv_cdf[4] = {};
+    int64_t host_items = 0;           // pending items served from host memory
 };
 
 namespace {
@@ -388,6 +394,18 @@ int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], co
     std::vector<uint8_t> h_skip((size_t)g->npart);
     std::vector<const void *> h_tab(2 * (size_t)g->npart);
     std::vector<char> visited((size_t)g->npart, 0), in_round((size_t)g->npart, 0);
+    // Read in place: every round processes every pending item; partitions in
+    // the arena are read from HBM, the others from their page-locked host
+    // arrays through the device's mapping (a hop then moves one prefix line
+    // and one column over the link instead of its whole partition).  Free
+    // arena space still takes the partitions of most pending items per byte,
+    // which serve the rounds and jobs after their copies land; nothing is
+    // evicted for them.
+    const float *dv_second =
+        second == SECOND_NONE ? nullptr : (second == SECOND_W ? g->dv_w : g->dv_cdf[second - SECOND_CDF]);
+    const bool rip = g->read_in_place && g->dv_col && (second == SECOND_NONE || dv_second);
+    const std::vector<char> protect_all((size_t)g->npart, 1);
+    std::vector<int> served;
     for (;;) {
         SCK(cudaMemcpyAsync(h_counts.data(), d_counts, sizeof(uint32_t) * (size_t)nbins, cudaMemcpyDeviceToHost, st));
         SCK(cudaStreamSynchronize(st));
@@ -399,11 +417,28 @@ int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], co
             for (int l = 0; l < D; ++l) pend[q] += h_counts[(size_t)q * D + l];
         }
         // this round: the resident partitions with pending items (with the
-        // weights this job needs); if none, the next partitions of the sweep
+        // weights this job needs); if none, the next partitions of the sweep.
+        // Read in place: every partition with pending items.
         std::vector<int> round;
         bool loading = false;   // this round copies partitions in
-        for (int q : g->resident)
-            if (pend[q] > 0 && (second == SECOND_NONE || g->res_w[q] == second)) round.push_back(q);
+        if (rip) {
+            std::vector<int> cand;
+            for (int q = 0; q < g->npart; ++q) {
+                if (pend[q] > 0) round.push_back(q);
+                if (pend[q] > 0 && g->res_off[q] < 0) cand.push_back(q);
+            }
+            std::stable_sort(cand.begin(), cand.end(), [&](int x, int y) {
+                return (double)pend[x] * (double)region_bytes(g, y, second) >
+                       (double)pend[y] * (double)region_bytes(g, x, second);
+            });
+            for (int q : cand) {   // into free space only
+                bool ok = false;
+                STRY(make_resident(g, q, second, protect_all, pend, &ok));
+            }
+        } else {
+            for (int q : g->resident)
+                if (pend[q] > 0 && (second == SECOND_NONE || g->res_w[q] == second)) round.push_back(q);
+        }
         std::fill(in_round.begin(), in_round.end(), 0);
         if (round.empty()) {
             std::vector<int> cand;
@@ -443,13 +478,36 @@ int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], co
         for (int k = 0; k < ngroups; ++k) {
             const size_t lo = round.size() * k / ngroups, hi = round.size() * (k + 1) / ngroups;
             std::fill(h_tab.begin(), h_tab.end(), nullptr);
-            for (size_t r = lo; r < hi; ++r) {
+            served.clear();
+            if (rip) {   // every partition: its copy in the arena once landed, else the host array
+                bool pending_copy = false;
+                for (int q = 0; q < g->npart; ++q) {
+                    bool dev = g->res_off[q] >= 0 && (second == SECOND_NONE || g->res_w[q] == second);
+                    if (dev && cudaEventQuery(g->ready[q]) != cudaSuccess) {
+                        dev = false;
+                        pending_copy = true;
+                    }
+                    if (dev) {
+                        unsigned char *base = g->arena + g->res_off[q];
+                        h_tab[q] = (const int32_t *)base - g->pbeg[q];
+                        if (g->res_w[q]) h_tab[g->npart + q] = (const float *)(base + g->res_bytes[q] / 2) - g->pbeg[q];
+                        served.push_back(q);
+                    } else {
+                        h_tab[q] = g->dv_col;
+                        h_tab[g->npart + q] = dv_second;
+                        g->host_items += pend[q];
+                    }
+                }
+                if (pending_copy) cudaGetLastError();   // "not ready" is no error
+            }
+            for (size_t r = lo; r < hi && !rip; ++r) {
                 const int part = round[r];
                 SCK(cudaStreamWaitEvent(st, g->ready[part], 0));
                 unsigned char *base = g->arena + g->res_off[part];
                 h_tab[part] = (const int32_t *)base - g->pbeg[part];
                 if (g->res_w[part])
                     h_tab[g->npart + part] = (const float *)(base + g->res_bytes[part] / 2) - g->pbeg[part];
+                served.push_back(part);
             }
             const void **tab = (const void **)g->ptab.p + (size_t)k * 2 * g->npart;
             SCK(cudaMemcpyAsync(tab, h_tab.data(), sizeof(void *) * h_tab.size(), cudaMemcpyHostToDevice, st));
@@ -503,7 +561,7 @@ int run_stream(csaw_stream_graph_s *g, const csaw_params *p, const int fan[], co
                 k_expand_heavy<I, BIAS, true><<<hblocks, HEAVY_THREADS, 0, st>>>(dg, a);
                 g->launches++;
             }
-            for (size_t r = lo; r < hi; ++r) SCK(cudaEventRecord(g->freed[round[r]], st));
+            for (int part : served) SCK(cudaEventRecord(g->freed[part], st));
         }
         SCK(cudaMemcpyAsync(d_skip, h_skip.data(), (size_t)g->npart, cudaMemcpyHostToDevice, st));
         STRY(rebin(true));
@@ -584,6 +642,11 @@ extern "C" int csaw_stream_graph_create(const void *rowptr, int rowptr_is_64, co
         g->reg_col = cudaHostRegister((void *)col, sizeof(int32_t) * n_edges, cudaHostRegisterDefault) == cudaSuccess;
         if (weights)
             g->reg_w = cudaHostRegister((void *)weights, sizeof(float) * n_edges, cudaHostRegisterDefault) == cudaSuccess;
+        cudaGetLastError();
+        // device addresses of the registered arrays, for reads in place
+        void *dp = nullptr;
+        if (g->reg_col && cudaHostGetDevicePointer(&dp, (void *)col, 0) == cudaSuccess) g->dv_col = (const int32_t *)dp;
+        if (g->reg_w && cudaHostGetDevicePointer(&dp, (void *)weights, 0) == cudaSuccess) g->dv_w = (const float *)dp;
         cudaGetLastError();
     }
     const int64_t per_max = std::max<int64_t>(g->max_pedges, 1) * (weights ? 8 : 4);
@@ -717,6 +780,9 @@ int build_stream_cdf(csaw_stream_graph_s *g) {
     }
     g->h_cdf[BIAS] = h;
     g->d_idx[BIAS] = idx;
+    void *dp = nullptr;
+    if (cudaHostGetDevicePointer(&dp, h, 0) == cudaSuccess) g->dv_cdf[BIAS] = (const float *)dp;
+    cudaGetLastError();
     return 0;
 }
 
@@ -794,5 +860,17 @@ extern "C" int csaw_stream_stats(csaw_stream_graph g, csaw_stream_info *out) {
     out->bytes_h2d = g->bytes_h2d;
     out->kernel_launches = g->launches;
     out->host_pinned_in_place = (g->reg_col ? 1 : 0) | (g->reg_w ? 2 : 0);
+    out->items_read_in_place = g->host_items;
     return 0;
+}
+
+extern "C" int csaw_stream_graph_set_option(csaw_stream_graph g, int option, int64_t value) {
+    if (!g) return csaw_host_fail(CSAW_ERR_INVALID, "stream graph is NULL");
+    switch (option) {
+        case CSAW_STREAM_OPT_READ_IN_PLACE:
+            g->read_in_place = value != 0;
+            return 0;
+        default:
+            return csaw_host_fail(CSAW_ERR_INVALID, "unknown stream graph option");
+    }
 }

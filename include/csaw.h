@@ -345,6 +345,7 @@ typedef struct {
     int64_t bytes_h2d;         /* adjacency bytes copied */
     int64_t kernel_launches;
     int64_t host_pinned_in_place; /* bit 0: col, bit 1: weights registered */
+    int64_t items_read_in_place;  /* pending items served from host memory (CSAW_STREAM_OPT_READ_IN_PLACE) */
 } csaw_stream_info;
 int csaw_stream_graph_create(const void *rowptr, int rowptr_is_64, const int32_t *col,
                              const float *weights, int64_t n_vertices, int64_t n_edges,
@@ -355,6 +356,17 @@ int csaw_stream_sample(csaw_stream_graph g, const csaw_params *p, const int32_t 
                        int32_t *out_src, int32_t *out_dst, int32_t *out_sample,
                        int32_t *out_depth, int64_t capacity, int64_t *n_out, void *stream);
 int csaw_stream_stats(csaw_stream_graph g, csaw_stream_info *out);
+/* Options of a streaming graph.  CSAW_STREAM_OPT_READ_IN_PLACE, 1 (default):
+ * when the host arrays a job reads are page-locked and mapped, partitions
+ * that are not in the device arena are read in place from host memory by
+ * the kernels (only the prefix lines and columns a hop touches cross the
+ * link), every round processes every pending item, and free arena space
+ * takes the partitions with the most pending items per byte without
+ * evicting any; 0: partitions are copied in before use and evicted when
+ * the budget is full (sweeps).  Output unchanged.  No counterpart in the
+ * reference, which copies fixed partitions (streaming_sampling.cu:597-714). */
+enum { CSAW_STREAM_OPT_READ_IN_PLACE = 1 };
+int csaw_stream_graph_set_option(csaw_stream_graph g, int option, int64_t value);
 /* Builds the per-vertex prefix cache of a bias kind (DEGREE, EDGE_WEIGHT or
  * HOOK) for a streaming graph: every row's canonical prefix in page-locked
  * host memory (4 E bytes) and its two index levels on the device (4.13 E/32
