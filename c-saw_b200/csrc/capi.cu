@@ -110,12 +110,12 @@ int ensure(DevBuf &b, size_t bytes, cudaStream_t st = nullptr) {
 
 constexpr int64_t QUEUE_ITEM_BUDGET = 32ll << 20;   // items per ping-pong queue
 constexpr int64_t SCRATCH_BUDGET = 4ll << 30;        // bytes of high-degree scratch (CTA prefix rebuilds)
-// CTA width of the retry pass of cached hubs: 128 << class threads.  128:
-// one warp resolves an item's slots while the others wait for the short
-// incremental rebuild passes, so narrow CTAs keep more items in flight
-// (measured: scale-25 step 26.2 ms at 256 threads, 25.5 ms at 128).
-#ifndef CSAW_RETRY_CTA_CLASS
-#define CSAW_RETRY_CTA_CLASS 0
+// CTA width of the retry pass of cached hubs.  128: one warp resolves an
+// item's slots while the others wait for the short incremental rebuild
+// passes, so narrow CTAs keep more items in flight (measured: scale-25 step
+// 26.2 ms at 256 threads, 25.5 ms at 128, 25.6 ms at 64).
+#ifndef CSAW_RETRY_THREADS
+#define CSAW_RETRY_THREADS 128
 #endif
 constexpr int MDRW_MAX_F = 4096;
 constexpr int MAX_HOST_PARTS = 8;                   // parts of a host-buffer job (copy-out pipelining)
@@ -567,6 +567,7 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
     int hblocks = 0;
     int64_t hstride = 0;
     int cta_grid[4] = {0, 0, 0, 0};
+    int rgrid = 0;   // the retry pass's grid (CSAW_RETRY_THREADS per CTA)
     if (BIASED && (g->maxdeg > smem_cap || sched)) {
         TRY(ensure(c->heavy, sizeof(uint32_t) * qcap, st));
         hstride = g->maxdeg + 2 * ((g->maxdeg >> 5) + 1) + (g->maxdeg >> 10) + 1 + 8;
@@ -577,6 +578,8 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
             cta_grid[k] = (int)std::min<int64_t>(grid_for(k_expand_heavy<I, BIAS>, 128 << k, 0, g->sm_count), cap_blocks);
             hblocks = std::max(hblocks, cta_grid[k]);
         }
+        rgrid = (int)std::min<int64_t>(grid_for(k_expand_heavy<I, BIAS>, CSAW_RETRY_THREADS, 0, g->sm_count), cap_blocks);
+        hblocks = std::max(hblocks, rgrid);
         hblocks = (int)std::min<int64_t>(hblocks, cap_blocks);
         TRY(ensure(c->hscratch, sizeof(float) * hstride * hblocks, st));
     }
@@ -822,11 +825,10 @@ int run_neighbor_t(csaw_graph_s *g, JobCtx *c, const csaw_params *p, const int f
                 LevelArgs ar = a;
                 ar.heavy_list = (SelEntry *)c->retry.p;
                 ar.n_heavy = &c->ctr->n_retry;
-                ar.cta_class = CSAW_RETRY_CTA_CLASS;
+                ar.cta_class = 0;   // recorded as the narrowest CTA class
                 ar.heavy_smem = g->retry_smem / 4;   // rows whose rebuild fits use shared memory
                 LaunchScope ls(g, KK_HEAVY, st);
-                k_expand_heavy<I, BIAS><<<cta_grid[CSAW_RETRY_CTA_CLASS], 128 << CSAW_RETRY_CTA_CLASS, g->retry_smem,
-                                          st>>>(dg, ar);
+                k_expand_heavy<I, BIAS><<<rgrid, CSAW_RETRY_THREADS, g->retry_smem, st>>>(dg, ar);
             }
             if (side) CK(cudaStreamWaitEvent(st, c->join, 0));
             if (dedup && l + 1 < D) TRY(dedup_level(nxt, l + 1));
