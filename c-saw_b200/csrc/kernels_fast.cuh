@@ -966,59 +966,73 @@ __device__ __forceinline__ void pair_body(const DevGraph &g, const LevelArgs &a,
         }
         return w.off;
     };
-    int off = 0;
+    // The item loop is uniform across the warp (half h takes item base + h;
+    // on the warp's last item the second half may idle), so the two halves
+    // meet at a full-warp barrier after their draws and run the copy
+    // request, the emission and the bookkeeping as one instruction stream.
+    const uint32_t hw = lane >> 4;
+    const uint32_t wstep = nh;   // two halves per warp
     uint32_t i = gh;
+    bool dead = false;           // a copy wait expired: this half stops
+    int off = 0;
     if (i < n) off = request(i, __ldcg(&a.pair_list[i].beg), __ldcg(&a.pair_list[i].d));
-    for (; i < n; i += nh) {
-        const uint32_t inext = i + nh;
+    for (uint32_t base = gh - hw; base < n; base += wstep, i += wstep) {
+        const bool act = i < n && !dead;
+        const uint32_t inext = i + wstep;
         long long nbeg = 0;
         int nd = 0;
-        if (inext < n) {   // the next item's range: its load overlaps this item
+        if (act && inext < n) {   // the next item's range: its load overlaps this item
             nbeg = __ldcg(&a.pair_list[inext].beg);
             nd = __ldcg(&a.pair_list[inext].d);
         }
-        if (!mbar_wait(bar, parity)) {   // bounded: report instead of spinning on
-            if (h.sl == 0) atomicOr(a.err, ERR_COPY_WAIT);
-            mbar_wait(bar, parity);        // let the copies in flight land first
-            break;
-        }
-        parity ^= 1u;
-        const SelEntry en = load_sel_smem(reinterpret_cast<const SelEntry *>(ebuf));
-        const int64_t beg = en.beg, d = en.d;
-        const float T = ebuf[12 + ((beg + d - 1) & 3)];
-        const DrawCtx dc{a.k0, a.k1, en.p, (uint32_t)en.s, (uint32_t)a.depth};
-        const bool rec = a.sched && a.sched->mode == SCHED_RECORD;
+        bool ok = true;
+        SelEntry en{};
+        StagePlan sp{STAGE_NONE, nullptr, 0};
+        int sel = 0;
         long long t0 = 0;
-        if (rec) t0 = clock64();
-        const StagePlan sp = stage_plan(g, beg, (int)d);
-        const float *S = buf + off;   // the staged row or index entries
-        int sel;
-        const bool ok = half_select(h, N, dc, T, [&](uint32_t x) -> int {
-            const float t = its_target(x, T);
-            if (sp.mode == STAGE_NONE) return (int)cdf_search(g, beg, d, t);
-            const int r = search_upper_lift<9>(S, sp.count, t);
-            return sp.mode == STAGE_ROW ? r : (int)staged_refine(g, sp.mode, r, beg, d, t);
-        }, sel);
-        __syncwarp(h.mask);   // every read of the buffers is done: they are free
-        if (inext < n) off = request(inext, nbeg, nd);
-        if (!ok) {   // rebuild needed: a whole warp redoes the item (in shared memory up to WF)
-            if (h.sl == 0) {
-                if (d <= WF) a.refill_list[atomicAdd(a.n_refill, 1u)] = en;
-                else a.retry_list[atomicAdd(a.n_retry, 1u)] = en;
+        const bool rec = a.sched && a.sched->mode == SCHED_RECORD;
+        if (act) {
+            if (!mbar_wait(bar, parity)) {   // bounded: report instead of spinning on
+                if (h.sl == 0) atomicOr(a.err, ERR_COPY_WAIT);
+                mbar_wait(bar, parity);        // let the copies in flight land first
+                dead = true;
+            } else {
+                parity ^= 1u;
             }
-            continue;
         }
-        if (h.sl < N)
-            emit_edge<I>(g, a, beg + sel, en.v, en.s, en.p * (uint32_t)N + (uint32_t)h.sl, (int64_t)en.ob + h.sl,
+        const bool run = act && !dead;
+        if (run) {
+            en = load_sel_smem(reinterpret_cast<const SelEntry *>(ebuf));
+            const int64_t beg = en.beg, d = en.d;
+            const float T = ebuf[12 + ((beg + d - 1) & 3)];
+            const DrawCtx dc{a.k0, a.k1, en.p, (uint32_t)en.s, (uint32_t)a.depth};
+            if (rec) t0 = clock64();
+            sp = stage_plan(g, beg, (int)d);
+            const float *S = buf + off;   // the staged row or index entries
+            ok = half_select(h, N, dc, T, [&](uint32_t x) -> int {
+                const float t = its_target(x, T);
+                if (sp.mode == STAGE_NONE) return (int)cdf_search(g, beg, d, t);
+                const int r = search_upper_lift<9>(S, sp.count, t);
+                return sp.mode == STAGE_ROW ? r : (int)staged_refine(g, sp.mode, r, beg, d, t);
+            }, sel);
+        }
+        __syncwarp();   // both halves: every read of the buffers is done, they are free
+        if (run && inext < n) off = request(inext, nbeg, nd);
+        if (run && !ok && h.sl == 0) {   // rebuild needed: a whole warp redoes the item
+            if (en.d <= WF) a.refill_list[atomicAdd(a.n_refill, 1u)] = en;
+            else a.retry_list[atomicAdd(a.n_retry, 1u)] = en;
+        }
+        if (run && ok && h.sl < N)
+            emit_edge<I>(g, a, en.beg + sel, en.v, en.s, en.p * (uint32_t)N + (uint32_t)h.sl, (int64_t)en.ob + h.sl,
                          en.q + (uint32_t)h.sl);
-        if (rec) {
+        if (run && ok && rec) {
             __syncwarp(h.mask);
             if (h.sl == 0)
-                record_profile(a.sched, d, N, a.sched->vstats[en.v], n_level, a.depth, en.cls, clock64() - t0);
+                record_profile(a.sched, en.d, N, a.sched->vstats[en.v], n_level, a.depth, en.cls, clock64() - t0);
         }
-        if (h.sl == 0) {
+        if (run && ok && h.sl == 0) {
             my_items++;
-            const unsigned long long row = staged_bytes(sp, d, N);
+            const unsigned long long row = staged_bytes(sp, en.d, N);
             my_bytes += 16 + row + (unsigned long long)N * (4ull + 4ull * nout +
                                                             (a.push ? 12ull + 2 * (sizeof(I) + 4) : 0ull));
         }
