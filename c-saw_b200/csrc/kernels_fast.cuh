@@ -484,64 +484,55 @@ __device__ __forceinline__ void coop_body(const DevGraph &g, const LevelArgs &a)
         const int incl = warp_incl_scan(k, lane);
         const int excl = incl - k;
         const int K = __shfl_sync(FULL, incl, 31);
+        // Items that need draws go to one list each, with their reserved
+        // slots.  Lane 0 reserves the batch's output and queue slots and its
+        // range in every list at once: the atomics are independent, so their
+        // round trips overlap instead of following one another.
+        const bool to_sel = drawn && !heavy && !hub && !pair && !thr;
+        const unsigned sm = __ballot_sync(FULL, to_sel);
+        const unsigned tm = __ballot_sync(FULL, thr);
+        const unsigned pbm = __ballot_sync(FULL, pair);
+        const unsigned hbm = __ballot_sync(FULL, hub);
+        unsigned cm[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) cm[c] = __ballot_sync(FULL, heavy && cls == 2 + c);
         unsigned long long ob = 0;
-        uint32_t qb = 0;
-        if (K) {
-            if (lane == 0) {
+        uint32_t qb = 0, ps = 0, pt = 0, pp = 0, ph = 0, pc[4] = {0u, 0u, 0u, 0u};
+        if (lane == 0) {
+            if (K) {
                 ob = atomicAdd(a.o_count, (unsigned long long)K);
                 if (a.push) qb = atomicAdd(a.n_out, (uint32_t)K);
             }
-            ob = __shfl_sync(FULL, ob, 0);
-            qb = __shfl_sync(FULL, qb, 0);
-        }
-        // hand off items that need draws, with their reserved slots
-        const unsigned sm = __ballot_sync(FULL, drawn && !heavy && !hub && !pair && !thr);
-        if (sm) {
-            uint32_t pos = 0;
-            if (lane == 0) pos = atomicAdd(a.n_sel, (uint32_t)__popc(sm));
-            pos = __shfl_sync(FULL, pos, 0);
-            if (drawn && !heavy && !hub && !pair && !thr)
-                a.sel_list[pos + __popc(sm & ((1u << lane) - 1u))] =
-                    SelEntry{it, qb + (uint32_t)excl, ob + excl, v, s, p, (int32_t)d, (long long)beg, cls, 0};
-        }
-        const unsigned tm = __ballot_sync(FULL, thr);
-        if (tm) {
-            uint32_t pos = 0;
-            if (lane == 0) pos = atomicAdd(a.n_thread, (uint32_t)__popc(tm));
-            pos = __shfl_sync(FULL, pos, 0);
-            if (thr)
-                a.thread_list[pos + __popc(tm & ((1u << lane) - 1u))] =
-                    SelEntry{it, qb + (uint32_t)excl, ob + excl, v, s, p, (int32_t)d, (long long)beg, cls, 0};
-        }
-        const unsigned pbm = __ballot_sync(FULL, pair);
-        if (pbm) {
-            uint32_t pos = 0;
-            if (lane == 0) pos = atomicAdd(a.n_pair, (uint32_t)__popc(pbm));
-            pos = __shfl_sync(FULL, pos, 0);
-            if (pair)
-                a.pair_list[pos + __popc(pbm & ((1u << lane) - 1u))] =
-                    SelEntry{it, qb + (uint32_t)excl, ob + excl, v, s, p, (int32_t)d, (long long)beg, cls, 0};
-        }
-        const unsigned hbm = __ballot_sync(FULL, hub);
-        if (hbm) {
-            uint32_t pos = 0;
-            if (lane == 0) pos = atomicAdd(a.n_hub, (uint32_t)__popc(hbm));
-            pos = __shfl_sync(FULL, pos, 0);
-            if (hub)
-                a.hub_list[pos + __popc(hbm & ((1u << lane) - 1u))] =
-                    SelEntry{it, qb + (uint32_t)excl, ob + excl, v, s, p, (int32_t)d, (long long)beg, cls, 0};
-        }
+            if (sm) ps = atomicAdd(a.n_sel, (uint32_t)__popc(sm));
+            if (tm) pt = atomicAdd(a.n_thread, (uint32_t)__popc(tm));
+            if (pbm) pp = atomicAdd(a.n_pair, (uint32_t)__popc(pbm));
+            if (hbm) ph = atomicAdd(a.n_hub, (uint32_t)__popc(hbm));
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const bool mine = heavy && cls == 2 + c;
-            const unsigned hm = __ballot_sync(FULL, mine);
-            if (hm) {
-                uint32_t pos = 0;
-                if (lane == 0) pos = atomicAdd(&a.n_cta[c], (uint32_t)__popc(hm));
-                pos = __shfl_sync(FULL, pos, 0);
-                if (mine)
-                    a.cta_list[c][pos + __popc(hm & ((1u << lane) - 1u))] =
-                        SelEntry{it, qb + (uint32_t)excl, ob + excl, v, s, p, (int32_t)d, (long long)beg, cls, 0};
+            for (int c = 0; c < 4; ++c)
+                if (cm[c]) pc[c] = atomicAdd(&a.n_cta[c], (uint32_t)__popc(cm[c]));
+        }
+        ob = __shfl_sync(FULL, ob, 0);
+        qb = __shfl_sync(FULL, qb, 0);
+        const unsigned below = (1u << lane) - 1u;
+        const SelEntry en{it, qb + (uint32_t)excl, ob + excl, v, s, p, (int32_t)d, (long long)beg, cls, 0};
+        {
+            const uint32_t pos_s = __shfl_sync(FULL, ps, 0), pos_t = __shfl_sync(FULL, pt, 0);
+            const uint32_t pos_p = __shfl_sync(FULL, pp, 0), pos_h = __shfl_sync(FULL, ph, 0);
+            uint32_t pos_c[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) pos_c[c] = __shfl_sync(FULL, pc[c], 0);
+            if (to_sel) {
+                a.sel_list[pos_s + __popc(sm & below)] = en;
+            } else if (thr) {
+                a.thread_list[pos_t + __popc(tm & below)] = en;
+            } else if (pair) {
+                a.pair_list[pos_p + __popc(pbm & below)] = en;
+            } else if (hub) {
+                a.hub_list[pos_h + __popc(hbm & below)] = en;
+            } else if (heavy) {
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                    if (cls == 2 + c) a.cta_list[c][pos_c[c] + __popc(cm[c] & below)] = en;
             }
         }
         if (valid) {
