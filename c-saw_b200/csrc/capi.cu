@@ -1404,10 +1404,13 @@ extern "C" int csaw_sample(csaw_graph g, const csaw_params *p, const int32_t *se
 // Parts a host-buffer job runs in: with P > 1 the output copy of part k
 // overlaps the sampling of parts k+1.. (hop posts already overlap the copy
 // of a hop's edges with the later hops; parts add overlap for single-kernel
-// walks and for the last hop).  A part costs the job's fixed per-kernel
-// latency again, so by default 4 parts only when the job can emit at least
-// 4 MB of (src, dst) and each part stays throughput-bound (16384 samples;
-// walks: 256 per SM), else 1.  Never during a timed scheduler trial.
+// walks and for the last hop, whose copy of the final part is the tail).  A
+// part costs the job's fixed per-kernel latency again, so by default 8 parts
+// when the job can emit at least 4 M edges, 4 from 512 K, else 1, and only
+// as many as keep each part throughput-bound (8192 samples; walks: 256 per
+// SM).  Measured on the scale-25 batch through host buffers: 57.0 ms per
+// step with 4 parts, 55.7 ms with 8 (the 3.05 GB copy-back then runs at the
+// link's rate).  Never during a timed scheduler trial.
 static int host_parts(const csaw_graph_s *g, const csaw_params *p, int64_t cap) {
     const int64_t S = p->n_samples;
     if (g->trial || S < 2 || p->depth < 1) return 1;
@@ -1416,8 +1419,9 @@ static int host_parts(const csaw_graph_s *g, const csaw_params *p, int64_t cap) 
     if (P == 0) {
         int64_t bound = 0, ns = 0;
         if (csaw_host_edge_bound((csaw_graph)g, p, &bound, &ns)) return 1;
-        const int64_t min_part = p->mode == CSAW_MODE_WALK ? 256ll * g->sm_count : 16384;
-        P = std::min(bound, cap) >= (512ll << 10) ? 4 : 1;
+        const int64_t min_part = p->mode == CSAW_MODE_WALK ? 256ll * g->sm_count : 8192;
+        const int64_t out = std::min(bound, cap);
+        P = out >= (4ll << 20) ? 8 : (out >= (512ll << 10) ? 4 : 1);
         while (P > 1 && S / P < min_part) --P;
     }
     return (int)std::max<int64_t>(1, std::min<int64_t>(P, S));

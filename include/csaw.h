@@ -219,8 +219,9 @@ enum {
     /* Host-buffer jobs (csaw_sample_host, host_buffers != 0) copy edges
      * back while they still sample: the edges of every finished hop, and of
      * every finished part when the job runs as P consecutive sample ranges
-     * (1..8); 0 (default): 4 ranges when the job can emit at least 512 Ki
-     * edges and each range has 16384 samples (walks: 256 per SM), else 1;
+     * (1..8); 0 (default): 8 ranges when the job can emit at least 4 Mi
+     * edges, 4 from 512 Ki, else 1, and no more than keep 8192 samples in
+     * a range (walks: 256 per SM);
      * -1: one range, copied back after all of its sampling.  Never changes
      * the edge multiset. */
     CSAW_OPT_HOST_PARTS = 5,
