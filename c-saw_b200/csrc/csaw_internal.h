@@ -85,7 +85,7 @@ struct LevelArgs {
     const uint8_t *sched_tab; // learned (trained): the level's decision table
     SelEntry *hub_list;       // batched: items above WF searching a cached prefix
     uint32_t *n_hub;
-    SelEntry *pair_list;      // batched: cached items run two per warp (N <= 16, d >= 4N)
+    SelEntry *pair_list;      // batched: cached items run two per warp (N <= 16, d >= 3N)
     uint32_t *n_pair;
     SelEntry *refill_list;    // batched: paired items redone by a whole warp (the warp list's buffer)
     uint32_t *n_refill;
