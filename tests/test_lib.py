@@ -149,3 +149,11 @@ def test_python_constants_match_header():
     for name, value in consts:
         assert hasattr(_lib, name), name
         assert getattr(_lib, name) == int(value), name
+
+
+def test_stream_option_rejects_null_graph():
+    """csaw_stream_graph_set_option checks its handle before any CUDA call."""
+    import csaw
+    from csaw import _lib
+    L = csaw.lib()
+    assert L.csaw_stream_graph_set_option(None, _lib.STREAM_OPT_READ_IN_PLACE, 1) == _lib.ERR_INVALID
