@@ -52,7 +52,9 @@ enum {
 
 enum {
     CSAW_SCHED_PLAIN = 0,    /* one launch per level, degree-threshold rule */
-    CSAW_SCHED_BATCHED = 1,  /* persistent work-queue kernel */
+    CSAW_SCHED_BATCHED = 1,  /* per-level passes by item class, CUDA-graph
+                                replayed; the one-launch persistent job
+                                kernel is CSAW_OPT_PERSISTENT */
     CSAW_SCHED_LEARNED = 2   /* batched + learned granularity */
 };
 
