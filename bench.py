@@ -30,7 +30,8 @@ Every form's edge multiset is hashed; differing hashes abort the run.
 5,105,039 edges, out-degree exponent 2.1 capped at 460, int32 CSR,
 lognormal(0,1) weights), (a) 4000 degree-biased samples F4 N20 D3 and (b)
 4000 degree-biased walks of 64.  The default run reports it, the request
-loop (serving) and MDRW as extra keys.
+loop (serving), MDRW and a streaming run (R-MAT scale 24 through a 1 GiB
+partition budget; --stream for the larger shapes) as extra keys.
 
 --impl reference times the CPU oracle (a port of the reference's sampling
 semantics; the reference itself has no CPU implementation and its CUDA
@@ -830,6 +831,7 @@ def serving(args, n_slots=8):
 
 
 STREAM_GRAPH = dict(edge_factor=16, a=0.57, b=0.19, c=0.19, seed=29, weight="uniform")
+EXTRA_STREAM_SHAPE = (24, 1.0, 16)   # scale, device budget (GiB), partition bits of the default line's key
 
 
 def streaming(args):
@@ -1067,7 +1069,7 @@ def main():
     ap.add_argument("--scale", type=int, default=25,
                     help="R-MAT scale of the rmat25 workload (samples and walks scale with 2^scale)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-extras", action="store_true", help="skip the power-law and serving extra keys")
+    ap.add_argument("--no-extras", action="store_true", help="skip the power-law, serving and streaming extra keys")
     ap.add_argument("--plain-budget-s", type=float, default=20.0,
                     help="device time the plain form's timed steps may take (at least 2 steps)")
     ap.add_argument("--profile-step", action="store_true",
@@ -1143,6 +1145,12 @@ def main():
                                                           "e2e_detail", "roofline", "kernels", "forms", "mdrw",
                                                           "gpu_launches")}
             line["serving"] = serving(args)
+            # streaming at a size the default run affords (the full sizes
+            # are --stream options): R-MAT scale 24, 1 GiB of partition
+            # slots for about 2.2 GB of host adjacency, 2^16-vertex partitions
+            sa = argparse.Namespace(**vars(args))
+            sa.stream_scale, sa.stream_budget_gb, sa.stream_pbits = EXTRA_STREAM_SHAPE
+            line["streaming"] = streaming(sa)
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
