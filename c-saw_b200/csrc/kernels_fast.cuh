@@ -228,12 +228,24 @@ __device__ __forceinline__ int resolve4(Spec4 &st, int N, int lane, const DrawCt
 // Generic driver: cand_of(x, act) maps a draw word to a candidate (warp-
 // uniform call); rebuild(st, j) zeroes the selections of slots < j out of the
 // prefix and returns false when no positive mass is left.
+// j0 > 0 resumes an item whose first phase failed at slot j0 (lane m < j0
+// passes its accepted index in sel0): slot j0 has used its draws
+// 0..REJECT_ATTEMPTS-1, so the run goes on exactly as it would after that
+// phase -- rebuild without the j0 selections, slot j0 from draw
+// REJECT_ATTEMPTS, later slots from draw 0.
 template <typename CandFn, typename RebuildFn>
 __device__ __forceinline__ int select_spec(int N, int lane, const DrawCtx &dc, bool zero, CandFn cand_of,
-                                           RebuildFn rebuild, bool lazy = false) {
+                                           RebuildFn rebuild, bool lazy = false, int j0 = 0, int sel0 = -1) {
     SlotRng rng;
     Spec4 st;
-    if (!zero) spec_fill(st, 0, N, lane, dc, rng, cand_of, 0, lazy);
+    if (j0 > 0) {
+        st.j = j0;
+        st.sel = lane < j0 ? sel0 : -1;
+        if (!rebuild(st, j0)) zero = true;
+        else spec_fill(st, j0, N, lane, dc, rng, cand_of, REJECT_ATTEMPTS, lazy);
+    } else if (!zero) {
+        spec_fill(st, 0, N, lane, dc, rng, cand_of, 0, lazy);
+    }
     for (;;) {
         if (zero) {
             for (int jj = st.j; jj < N; ++jj) fill_smallest(st, jj, lane);
@@ -298,9 +310,10 @@ __device__ __forceinline__ int select_smem(const float *W, int d, int N, const D
 // since the cache holds exactly the prefix it would compute.
 template <typename I, int BIAS>
 __device__ __forceinline__ int select_cached(const DevGraph &g, int64_t beg, int d, int N, const DrawCtx &dc,
-                                             float *P, uint32_t *zb, int lane) {
+                                             float *P, uint32_t *zb, int lane, int j0 = 0, int sel0 = -1) {
     const float *cp = g.cdf + beg;
-    for (int i0 = 0; i0 < d; i0 += 256) {
+    // a resumed item (j0 > 0) starts with a rebuild, which writes all of P
+    for (int i0 = 0; i0 < (j0 > 0 ? 0 : d); i0 += 256) {
         float r[8];
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
@@ -314,7 +327,7 @@ __device__ __forceinline__ int select_cached(const DevGraph &g, int64_t beg, int
         }
     }
     __syncwarp();
-    float T = P[d - 1];
+    float T = j0 > 0 ? 1.f : P[d - 1];
     auto cand_of = [&](uint32_t x, bool act) -> int {
         return act ? search_upper32(P, d, its_target(x, T)) : -1;
     };
@@ -328,7 +341,7 @@ __device__ __forceinline__ int select_cached(const DevGraph &g, int64_t beg, int
         T = warp_canon_prefix(wfn, d, P, zb, lane);
         return T > 0.f;
     };
-    return select_spec(N, lane, dc, !(T > 0.f), cand_of, rebuild, d >= 4 * N);
+    return select_spec(N, lane, dc, !(T > 0.f), cand_of, rebuild, d >= 4 * N, j0, sel0);
 }
 
 // Unbiased selection (no prefix): index ranks over the non-excluded range.
@@ -617,7 +630,17 @@ __device__ __forceinline__ void select_fast_body(const DevGraph &g, const LevelA
                 sel = select_reg<I, BIAS>(g, beg, (int)d, N, dc, lane);
             } else if constexpr (CACHED) {
                 if (d <= WF) {
-                    sel = select_cached<I, BIAS>(g, beg, (int)d, N, dc, P, zb, lane);
+                    // a pair item whose first phase failed (en.pad = its pair
+                    // index + 1): its failing slot and accepted indices wait
+                    // in the consumed pair entry
+                    int j0 = 0, sel0 = -1;
+                    if (en.pad > 0 && a.pair_list) {
+                        const uint16_t *ps = reinterpret_cast<const uint16_t *>(a.pair_list + (en.pad - 1));
+                        j0 = __ldcg(ps);
+                        if (j0 >= N) j0 = 0;
+                        if (lane < j0) sel0 = __ldcg(ps + 1 + lane);
+                    }
+                    sel = select_cached<I, BIAS>(g, beg, (int)d, N, dc, P, zb, lane, j0, sel0);
                 } else {   // hubs are listed for k_select_hub; kept for completeness
                     sel = select_warp<I, BIAS>(g, beg, d, N, dc, P, zb, zs, lane, WF);
                     if (sel == -2) {   // needs a rebuild that does not fit: retried by the CTA pass
@@ -797,15 +820,16 @@ struct Half {
 
 // Draws of one item (N <= 16 slots) in a half-warp, slot j on lane j, the
 // same draws and acceptance order as resolve_slots; cand_of(x) is a per-lane
-// search.  Returns false when a slot exhausts its draws of the first phase
-// (the item then needs a rebuild of its prefix: the caller retries it whole
-// on the CTA path).  T <= 0: the slots take indices 0..N-1.
+// search.  Returns -1 when every slot is accepted, else the slot j whose
+// draws of the first phase ran out (slots below j then hold their accepted
+// indices in sel; the item needs a rebuild of its prefix, which a whole warp
+// or CTA goes on with).  T <= 0: the slots take indices 0..N-1.
 template <typename CandFn>
-__device__ __forceinline__ bool half_select(const Half &h, int N, const DrawCtx &dc, float T, CandFn cand_of,
-                                            int &sel) {
+__device__ __forceinline__ int half_select(const Half &h, int N, const DrawCtx &dc, float T, CandFn cand_of,
+                                           int &sel) {
     const int sl = h.sl;
     sel = sl;
-    if (!(T > 0.f)) return true;
+    if (!(T > 0.f)) return -1;
     SlotRng rng;
     int cand = -1, A = 0;
     if (sl < N) {
@@ -831,14 +855,14 @@ __device__ __forceinline__ bool half_select(const Half &h, int N, const DrawCtx 
             a = 1;
             continue;
         }
-        if (a == REJECT_ATTEMPTS) return false;
+        if (a == REJECT_ATTEMPTS) return j;
         if (sl == j) {
             cand = cand_of(rng.word(dc, sl, A));
             ++A;
         }
         ++a;
     }
-    return true;
+    return -1;
 }
 
 // What the pair kernel stages in shared memory for an item over a cached
@@ -942,7 +966,8 @@ __device__ __forceinline__ void pair_body(const DevGraph &g, const LevelArgs &a,
     const uint32_t n_level = __ldcg(a.n_in);
     const int N = a.N;
     const int nout = 2 + (a.o_smp != nullptr) + (a.o_dep != nullptr);
-    unsigned long long my_bytes = 0, my_items = 0;
+    unsigned long long my_bytes = 0;
+    uint32_t my_items = 0;   // at most n per lane
     // requests the staged copies of item idx (row range rbeg, rd); returns the
     // offset of its staged array in the buffer
     auto request = [&](uint32_t idx, long long rbeg, int rd) -> int {
@@ -976,7 +1001,7 @@ __device__ __forceinline__ void pair_body(const DevGraph &g, const LevelArgs &a,
             nbeg = __ldcg(&a.pair_list[inext].beg);
             nd = __ldcg(&a.pair_list[inext].d);
         }
-        bool ok = true;
+        int jfail = -1;   // -1: all slots accepted; else the slot whose first phase failed
         SelEntry en{};
         StagePlan sp{STAGE_NONE, nullptr, 0};
         int sel = 0;
@@ -1000,18 +1025,31 @@ __device__ __forceinline__ void pair_body(const DevGraph &g, const LevelArgs &a,
             if (rec) t0 = clock64();
             sp = stage_plan(g, beg, (int)d);
             const float *S = buf + off;   // the staged row or index entries
-            ok = half_select(h, N, dc, T, [&](uint32_t x) -> int {
+            jfail = half_select(h, N, dc, T, [&](uint32_t x) -> int {
                 const float t = its_target(x, T);
                 if (sp.mode == STAGE_NONE) return (int)cdf_search(g, beg, d, t);
                 const int r = search_upper_lift<9>(S, sp.count, t);
                 return sp.mode == STAGE_ROW ? r : (int)staged_refine(g, sp.mode, r, beg, d, t);
             }, sel);
         }
+        const bool ok = jfail < 0;
         __syncwarp();   // both halves: every read of the buffers is done, they are free
         if (run && inext < n) off = request(inext, nbeg, nd);
-        if (run && !ok && h.sl == 0) {   // rebuild needed: a whole warp redoes the item
-            if (en.d <= WF) a.refill_list[atomicAdd(a.n_refill, 1u)] = en;
-            else a.retry_list[atomicAdd(a.n_retry, 1u)] = en;
+        if (run && !ok && en.d <= WF && i < 0x7FFFFFFFu) {
+            // a whole warp goes on from the failed first phase: the failing
+            // slot and the accepted indices (< WF) go into this item's pair
+            // entry, which nothing reads after its copy has landed
+            uint16_t *ps = reinterpret_cast<uint16_t *>(a.pair_list + i);
+            if (h.sl < jfail) ps[1 + h.sl] = (uint16_t)sel;
+            if (h.sl == 0) ps[0] = (uint16_t)jfail;
+        }
+        if (run && !ok && h.sl == 0) {   // rebuild needed: a whole warp goes on with the item
+            if (en.d <= WF) {
+                if (i < 0x7FFFFFFFu) en.pad = (int32_t)(i + 1);   // where its first phase's state waits
+                a.refill_list[atomicAdd(a.n_refill, 1u)] = en;
+            } else {
+                a.retry_list[atomicAdd(a.n_retry, 1u)] = en;
+            }
         }
         if (run && ok && h.sl < N)
             emit_edge<I>(g, a, en.beg + sel, en.v, en.s, en.p * (uint32_t)N + (uint32_t)h.sl, (int64_t)en.ob + h.sl,
@@ -1035,7 +1073,7 @@ __device__ __forceinline__ void pair_body(const DevGraph &g, const LevelArgs &a,
     }
     if (lane == 0 && my_items) {
         atomicAdd(&a.bytes[7], my_bytes);
-        atomicAdd(&a.items[7], my_items);
+        atomicAdd(&a.items[7], (unsigned long long)my_items);
     }
 }
 
