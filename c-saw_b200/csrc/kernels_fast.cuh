@@ -953,7 +953,9 @@ __device__ __forceinline__ unsigned long long staged_bytes(const StagePlan &sp, 
 // rebuild are redone from scratch: rows up to WF edges by k_select_fast on
 // the refill list (written over the consumed warp list), larger ones by the
 // CTA pass.
-constexpr int PAIR_ENT = 16;   // floats of a half's entry slot: the 48-byte entry and the 16-byte T window
+constexpr int PAIR_ENT = 16;
+// Largest row whose failed first phase is resumed (16-bit indices).
+constexpr int RESUME_MAX_DEG = 65535;   // floats of a half's entry slot: the 48-byte entry and the 16-byte T window
 
 template <typename I, int BIAS>
 __device__ __forceinline__ void pair_body(const DevGraph &g, const LevelArgs &a, float *buf, float *ebuf,
@@ -1035,21 +1037,20 @@ __device__ __forceinline__ void pair_body(const DevGraph &g, const LevelArgs &a,
         const bool ok = jfail < 0;
         __syncwarp();   // both halves: every read of the buffers is done, they are free
         if (run && inext < n) off = request(inext, nbeg, nd);
-        if (run && !ok && en.d <= WF && i < 0x7FFFFFFFu) {
-            // a whole warp goes on from the failed first phase: the failing
-            // slot and the accepted indices (< WF) go into this item's pair
-            // entry, which nothing reads after its copy has landed
+        const bool keep = en.d <= RESUME_MAX_DEG && i < 0x7FFFFFFFu;
+        if (run && !ok && keep) {
+            // a whole warp (rows) or CTA (hubs) goes on from the failed first
+            // phase: the failing slot and the accepted indices (16-bit) go
+            // into this item's pair entry, which nothing reads after its copy
+            // has landed
             uint16_t *ps = reinterpret_cast<uint16_t *>(a.pair_list + i);
             if (h.sl < jfail) ps[1 + h.sl] = (uint16_t)sel;
             if (h.sl == 0) ps[0] = (uint16_t)jfail;
         }
-        if (run && !ok && h.sl == 0) {   // rebuild needed: a whole warp goes on with the item
-            if (en.d <= WF) {
-                if (i < 0x7FFFFFFFu) en.pad = (int32_t)(i + 1);   // where its first phase's state waits
-                a.refill_list[atomicAdd(a.n_refill, 1u)] = en;
-            } else {
-                a.retry_list[atomicAdd(a.n_retry, 1u)] = en;
-            }
+        if (run && !ok && h.sl == 0) {   // rebuild needed: a whole warp or CTA goes on with the item
+            if (keep) en.pad = (int32_t)(i + 1);   // where its first phase's state waits
+            if (en.d <= WF) a.refill_list[atomicAdd(a.n_refill, 1u)] = en;
+            else a.retry_list[atomicAdd(a.n_retry, 1u)] = en;
         }
         if (run && ok && h.sl < N)
             emit_edge<I>(g, a, en.beg + sel, en.v, en.s, en.p * (uint32_t)N + (uint32_t)h.sl, (int64_t)en.ob + h.sl,

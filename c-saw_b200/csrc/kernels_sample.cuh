@@ -538,11 +538,30 @@ __device__ __forceinline__ void heavy_body(const DevGraph &g0, const LevelArgs &
             return indexed ? (int)cdf_search(g, beg, d, t) : (int)search_upper(P, d, t);
         };
         bool zero = !(T > 0.f);
-        if (warp == 0 && !zero) draw_pending(st, 0, N, lane, dc, rng, cand_of);
-        for (;;) {
+        // a pair item whose first phase failed at slot j0 (the entry's pad =
+        // its pair index + 1; the slot and the accepted indices wait in the
+        // consumed pair entry): the run goes on from there -- a rebuild
+        // without the j0 selections, slot j0 from draw REJECT_ATTEMPTS
+        int j0 = 0;
+        if (a.heavy_list && a.pair_list && indexed && !zero) {
+            const int pad = __ldcg(&a.heavy_list[h].pad);
+            if (pad > 0) {
+                const uint16_t *ps = reinterpret_cast<const uint16_t *>(a.pair_list + (pad - 1));
+                j0 = __ldcg(ps);
+                if (j0 >= N) j0 = 0;
+                if (warp == 0 && j0 > 0) {
+                    st.j = j0;
+                    if (lane < j0) st.sel = __ldcg(ps + 1 + lane);
+                    if (lane == j0) st.A = REJECT_ATTEMPTS;
+                }
+            }
+        }
+        if (warp == 0 && !zero && j0 == 0) draw_pending(st, 0, N, lane, dc, rng, cand_of);
+        for (bool resumed = j0 > 0;; resumed = false) {
             if (warp == 0) {
                 int r = 0;
-                if (zero) zero_fill(st, N, lane);
+                if (resumed) r = 1;   // the rebuild after the failed first phase comes first
+                else if (zero) zero_fill(st, N, lane);
                 else r = resolve_slots(st, N, lane, dc, rng, cand_of);
                 if (lane == 0) {
                     s_flag = r;
