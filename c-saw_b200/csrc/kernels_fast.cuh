@@ -950,12 +950,10 @@ __device__ __forceinline__ unsigned long long staged_bytes(const StagePlan &sp, 
 // searches the staged array in shared memory by fixed-step lifting; index
 // entries then lead to one 32-entry line per remaining level in global
 // memory, so rows and hubs share one resolver loop.  Items that need a
-// rebuild are redone from scratch: rows up to WF edges by k_select_fast on
-// the refill list (written over the consumed warp list), larger ones by the
-// CTA pass.
-constexpr int PAIR_ENT = 16;
-// Largest row whose failed first phase is resumed (16-bit indices).
-constexpr int RESUME_MAX_DEG = 65535;   // floats of a half's entry slot: the 48-byte entry and the 16-byte T window
+// rebuild go on from their failed first phase (its state kept in the
+// consumed pair entry): rows up to WF edges by k_select_fast on the refill
+// list (written over the consumed warp list), larger ones by the CTA pass.
+constexpr int PAIR_ENT = 16;   // floats of a half's entry slot: the 48-byte entry and the 16-byte T window
 
 template <typename I, int BIAS>
 __device__ __forceinline__ void pair_body(const DevGraph &g, const LevelArgs &a, float *buf, float *ebuf,

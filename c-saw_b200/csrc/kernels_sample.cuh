@@ -545,7 +545,7 @@ __device__ __forceinline__ void heavy_body(const DevGraph &g0, const LevelArgs &
         int j0 = 0;
         if (a.heavy_list && a.pair_list && indexed && !zero) {
             const int pad = __ldcg(&a.heavy_list[h].pad);
-            if (pad > 0) {
+            if (pad > 0 && d <= RESUME_MAX_DEG) {
                 const uint16_t *ps = reinterpret_cast<const uint16_t *>(a.pair_list + (pad - 1));
                 j0 = __ldcg(ps);
                 if (j0 >= N) j0 = 0;
